@@ -1,0 +1,141 @@
+/*
+ * C ABI of the B200 block-Wiedemann sequence engine over GF(p).
+ *
+ * Plain C types only (pointers, sizes, integers).  Every function returns 0 on
+ * success and a nonzero status otherwise (1 = invalid argument or host error,
+ * 2 = CUDA error, 3 = failed precondition); bw_last_error() then returns the
+ * message (thread-local, valid until the next failing call on that thread).
+ * No exception crosses this boundary.  Pointers documented as "device" are
+ * CUDA device pointers of the context's device; "stream" is a cudaStream_t
+ * (NULL = the context's own stream).
+ *
+ * Residues are canonical uint32 values in [0, p); blocks are row-major
+ * (row * width + column), the layout of the reference's dense blocks
+ * (cuda/matrices.h:23-41, cuda/prym_cuda_helpers.h:67-85).
+ */
+#ifndef BW_ENGINE_H
+#define BW_ENGINE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BW_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define BW_API __attribute__((visibility("default")))
+#else
+#define BW_API
+#endif
+
+/* Arithmetic form of the hot path. */
+#define BW_FORM_PLAIN 0 /* uint32/int32 CUDA-core modular arithmetic */
+#define BW_FORM_INT8 1  /* signed 8-bit limbs on tcgen05 kind::i8 tensor cores */
+
+/* Message of the last failing call on this thread ("" if none). */
+BW_API const char* bw_last_error(void);
+
+/* ABI version (BW_ABI_VERSION). */
+BW_API int bw_abi_version(void);
+
+/* Fill count residues of the counter-based seeded stream (seed, tag) into a
+ * device buffer: value idx is uniform in [lo, p).  The same stream on the host
+ * is bw_seeded_fill_host.  No reference counterpart: the synthetic workloads'
+ * inputs are defined by this stream. */
+BW_API int bw_seeded_fill(uint32_t* d_out, uint64_t count, uint64_t seed, uint32_t tag,
+                   uint32_t p, uint32_t lo, int device, void* stream);
+BW_API int bw_seeded_fill_host(uint32_t* out, uint64_t count, uint64_t seed, uint32_t tag,
+                        uint32_t p, uint32_t lo);
+
+/* ------------------------------------------------------------------------
+ * Synthetic Koszul operator
+ *   d : Lambda^k(F^r) (x) R_q -> Lambda^(k-1)(F^r) (x) R_(q+1),
+ *   (d y)[T, c] = sum_{i not in T} (-1)^pos(i, T u {i}) sum_b M_i[c, b] y[T u {i}, b],
+ *   S = D d^T d, sequence a_i = X^T S^i Y.
+ * Row order follows the reference's explicit differential
+ * (tests/deformation_reference.py:75-89): lexicographic subsets, coefficient
+ * index fastest.  The reference's nearest kernel is
+ * cyclic_phi_forward_scaled_kernel / cyclic_phi_transpose_kernel
+ * (cuda/cyclic_cuda_helpers.h:145-266) with dense maps in place of the
+ * character-sparse mu.
+ * ---------------------------------------------------------------------- */
+
+typedef struct bw_koszul bw_koszul;
+
+typedef struct bw_koszul_desc {
+    uint32_t r;           /* generators (exterior rank), 2..31 */
+    uint32_t k;           /* source exterior degree, 1..r */
+    uint32_t dim_in;      /* dim R_q   (columns of each M_i) */
+    uint32_t dim_out;     /* dim R_q+1 (rows of each M_i) */
+    uint32_t prime;       /* odd prime < 2^15 */
+    uint32_t block_width; /* n: columns of Y (4, 8, 16 or 32) */
+    uint32_t proj_width;  /* m: columns of X (4, 8, 16 or 32) */
+    uint32_t form;        /* BW_FORM_PLAIN or BW_FORM_INT8 */
+    const uint32_t* maps; /* host, r * dim_out * dim_in canonical residues, M_i row-major */
+    const uint32_t* diag; /* N_src nonzero residues of D (host or device, see diag_on_device) */
+    uint32_t diag_on_device;
+} bw_koszul_desc;
+
+typedef struct bw_koszul_info {
+    uint64_t n_src;          /* C(r,k) * dim_in  : rows of Y, X and S */
+    uint64_t n_tgt;          /* C(r,k-1) * dim_out */
+    uint64_t device_bytes;   /* device memory held by the context */
+    uint64_t scratch_bytes;  /* of which projection scratch (partials + counters) */
+    uint32_t form;
+    uint32_t sm_count;
+} bw_koszul_info;
+
+/* Replaces the operator set-up of run_eliminated_sector
+ * (cuda/cuprym_cyclic.cu:2136-2324) for the synthetic operator: builds the
+ * incidence tables, uploads maps and diagonal, allocates the work blocks. */
+BW_API int bw_koszul_create(const bw_koszul_desc* desc, int device, bw_koszul** out);
+BW_API int bw_koszul_info_get(const bw_koszul* ctx, bw_koszul_info* out);
+BW_API void bw_koszul_destroy(bw_koszul* ctx);
+
+/* d_z = d d_y (device, canonical).  Replaces cyclic_phi_forward_scaled_kernel
+ * (cuda/cyclic_cuda_helpers.h:145-204). */
+BW_API int bw_koszul_forward(bw_koszul* ctx, const uint32_t* d_y, uint32_t* d_z, void* stream);
+/* d_w = d^T d_z, times D when scale_by_diag (device, canonical).  Replaces
+ * cyclic_phi_transpose_kernel (cuda/cyclic_cuda_helpers.h:206-266). */
+BW_API int bw_koszul_transpose(bw_koszul* ctx, const uint32_t* d_z, uint32_t* d_w, int scale_by_diag,
+                        void* stream);
+/* d_out = S d_y (device, canonical).  Replaces apply_square
+ * (cuda/cuprym_cyclic.cu:2408-2418). */
+BW_API int bw_koszul_apply(bw_koszul* ctx, const uint32_t* d_y, uint32_t* d_out, void* stream);
+
+/* Sequence session (replaces the hot loop of run_eliminated_sector,
+ * cuda/cuprym_cyclic.cu:2420-2450, and compute_and_push_bigsp2, :886-897):
+ *   start : loads X (n_src x m) and Y0 (n_src x n), writes a_0 = X^T Y0 into
+ *           d_seq[0] (d_seq holds seq_capacity entries of m x n residues);
+ *   step  : performs `steps` applications of S, appending a_i after each;
+ *   finish: writes the current block S^i Y0 to d_y_out (may be NULL) and the
+ *           number of entries written to *nlen_out (may be NULL). */
+BW_API int bw_koszul_seq_start(bw_koszul* ctx, const uint32_t* d_x, const uint32_t* d_y0,
+                        uint32_t* d_seq, uint64_t seq_capacity, void* stream);
+BW_API int bw_koszul_seq_step(bw_koszul* ctx, uint64_t steps, void* stream);
+BW_API int bw_koszul_seq_finish(bw_koszul* ctx, uint32_t* d_y_out, uint64_t* nlen_out, void* stream);
+
+/* One-shot sequence of nlen entries through HOST buffers: copies X and Y0 to
+ * the device, runs nlen-1 steps, copies the sequence (nlen x m x n) and the
+ * final block back (h_y_final may be NULL).  Synchronous. */
+BW_API int bw_koszul_sequence_host(bw_koszul* ctx, const uint32_t* h_x, const uint32_t* h_y0,
+                            uint64_t nlen, uint32_t* h_seq, uint32_t* h_y_final);
+
+/* Like bw_koszul_seq_step, but issues the steps one kernel at a time with
+ * CUDA events around each launch on the session stream and returns the
+ * average device time per launch (ms) of each kernel kind in ms_out[0..2]:
+ * [0] forward d, [1] transpose d^T (with D), [2] projection.  For measurement
+ * (roofline figures); the sequence it appends is the same. */
+BW_API int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* ms_out, void* stream);
+
+/* Number of engine kernel launches issued by this context since creation. */
+BW_API uint64_t bw_koszul_launch_count(const bw_koszul* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BW_ENGINE_H */

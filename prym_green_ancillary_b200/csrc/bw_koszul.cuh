@@ -1,0 +1,85 @@
+// Context of the synthetic Koszul engine (shared by the plain and INT8 forms).
+#pragma once
+
+#include "bw_common.cuh"
+#include "../../include/bw_engine.h"
+
+#include <memory>
+#include <vector>
+
+namespace bw {
+
+struct KoszulCtx {
+    // shape
+    int device = 0, sms = 0;
+    int r = 0, k = 0, ci = 0, co = 0, ci4 = 0, co4 = 0, nb = 0, m = 0;
+    uint32_t p = 0, form = BW_FORM_PLAIN;
+    Mod mod{};
+    uint64_t n_s = 0, n_t = 0, n_src = 0, n_tgt = 0;
+
+    // device state
+    cudaStream_t own_stream = nullptr;
+    std::vector<void*> allocations;
+    uint64_t device_bytes = 0, scratch_bytes = 0;
+    int32_t *d_coef_fwd = nullptr, *d_coef_bwd = nullptr;
+    uint32_t *d_fwd = nullptr, *d_bwd = nullptr;
+    int32_t* d_diag = nullptr;
+    int32_t *d_ya = nullptr, *d_yb = nullptr, *d_z = nullptr, *d_xb = nullptr;
+    std::vector<uint32_t> maps_canonical;
+
+    // projection scratch
+    unsigned proj_grid = 1;
+    int32_t* d_partials = nullptr;
+    unsigned int* d_counter = nullptr;
+    unsigned long long* d_seq_index = nullptr;
+
+    // sequence session
+    bool in_session = false, cur_is_a = true;
+    uint32_t* d_seq = nullptr;
+    uint64_t seq_capacity = 0, seq_len = 0;
+    static constexpr int kGraphPairs = 8;
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+    uint64_t graph_launch_kernels = 0;
+    uint64_t launches = 0;
+
+    // host-buffer staging
+    uint32_t *d_stage_x = nullptr, *d_stage_y = nullptr, *d_stage_seq = nullptr;
+    uint64_t stage_seq_cap = 0;
+
+    // INT8-limb form state (bw_koszul_i8.cu)
+    struct I8State;
+    I8State* i8 = nullptr;
+
+    static KoszulCtx* create(const bw_koszul_desc& d, int dev);
+    ~KoszulCtx();
+
+    template <class T>
+    T* alloc(uint64_t count);
+    void release(void* p);
+
+    void launch_to_balanced(const uint32_t* in, int32_t* out, uint64_t count, cudaStream_t st);
+    void launch_to_canonical(const int32_t* in, uint32_t* out, uint64_t count, cudaStream_t st);
+
+    void plain_forward(const int32_t* y, int32_t* z, cudaStream_t st);
+    void plain_transpose(const int32_t* z, int32_t* w, bool scale, cudaStream_t st);
+    void forward(const int32_t* y, int32_t* z, cudaStream_t st);
+    void transpose(const int32_t* z, int32_t* w, bool scale, cudaStream_t st);
+    void project(const int32_t* w, cudaStream_t st);
+    void step_once(cudaStream_t st);
+
+    void seq_start(const uint32_t* x, const uint32_t* y0, uint32_t* seq, uint64_t capacity, cudaStream_t st);
+    void seq_step(uint64_t steps, cudaStream_t st);
+    void seq_finish(uint32_t* y_out, uint64_t* nlen_out, cudaStream_t st);
+    uint64_t kernels_per_step() const;
+    uint64_t launches_in_pair_graph() const;
+    void ensure_host_staging(uint64_t nlen);
+
+    // INT8-limb form
+    void i8_setup();
+    void i8_destroy();
+    void i8_forward(const int32_t* y, int32_t* z, cudaStream_t st);
+    void i8_transpose(const int32_t* z, int32_t* w, bool scale, cudaStream_t st);
+    uint64_t i8_kernels_per_step() const;
+};
+
+}  // namespace bw

@@ -1,0 +1,215 @@
+"""ctypes binding of the engine's C ABI (include/bw_engine.h).
+
+The CUDA library ``libbw_b200.so`` is built in-tree by ``build.build()``.
+There is no CPU fallback: every entry point here calls the CUDA library and
+raises ``EngineError`` with the library's message on a nonzero status.
+
+Device buffers are torch tensors (int32 storage of canonical residues; every
+residue is below 2^15, so the int32 and uint32 bit patterns agree).  Host
+buffers are numpy uint32 arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libbw_b200.so"
+
+FORM_PLAIN = 0
+FORM_INT8 = 1
+FORMS = {"plain": FORM_PLAIN, "int8": FORM_INT8}
+
+_LIB = None
+
+
+class EngineError(RuntimeError):
+    """A nonzero status from the engine's C ABI."""
+
+    def __init__(self, status, message):
+        super().__init__(f"[status {status}] {message}")
+        self.status = status
+
+
+class KoszulDesc(ctypes.Structure):
+    _fields_ = [
+        ("r", ctypes.c_uint32), ("k", ctypes.c_uint32), ("dim_in", ctypes.c_uint32),
+        ("dim_out", ctypes.c_uint32), ("prime", ctypes.c_uint32), ("block_width", ctypes.c_uint32),
+        ("proj_width", ctypes.c_uint32), ("form", ctypes.c_uint32),
+        ("maps", ctypes.c_void_p), ("diag", ctypes.c_void_p), ("diag_on_device", ctypes.c_uint32),
+    ]
+
+
+class KoszulInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_src", ctypes.c_uint64), ("n_tgt", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64),
+        ("scratch_bytes", ctypes.c_uint64), ("form", ctypes.c_uint32), ("sm_count", ctypes.c_uint32),
+    ]
+
+
+# Every symbol the header declares, with (restype, argtypes).
+_VP, _U32, _U64, _INT = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+SIGNATURES = {
+    "bw_last_error": (ctypes.c_char_p, []),
+    "bw_abi_version": (_INT, []),
+    "bw_seeded_fill": (_INT, [_VP, _U64, _U64, _U32, _U32, _U32, _INT, _VP]),
+    "bw_seeded_fill_host": (_INT, [_VP, _U64, _U64, _U32, _U32, _U32]),
+    "bw_koszul_create": (_INT, [ctypes.POINTER(KoszulDesc), _INT, ctypes.POINTER(_VP)]),
+    "bw_koszul_info_get": (_INT, [_VP, ctypes.POINTER(KoszulInfo)]),
+    "bw_koszul_destroy": (None, [_VP]),
+    "bw_koszul_forward": (_INT, [_VP, _VP, _VP, _VP]),
+    "bw_koszul_transpose": (_INT, [_VP, _VP, _VP, _INT, _VP]),
+    "bw_koszul_apply": (_INT, [_VP, _VP, _VP, _VP]),
+    "bw_koszul_seq_start": (_INT, [_VP, _VP, _VP, _VP, _U64, _VP]),
+    "bw_koszul_seq_step": (_INT, [_VP, _U64, _VP]),
+    "bw_koszul_seq_finish": (_INT, [_VP, _VP, ctypes.POINTER(_U64), _VP]),
+    "bw_koszul_sequence_host": (_INT, [_VP, _VP, _VP, _U64, _VP, _VP]),
+    "bw_koszul_seq_step_timed": (_INT, [_VP, _U64, ctypes.POINTER(ctypes.c_float), _VP]),
+    "bw_koszul_launch_count": (_U64, [_VP]),
+}
+
+
+def load():
+    """Load libbw_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise EngineError(-1, f"{LIB_PATH} is missing: run prym_green_ancillary_b200.build.build()")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def _check(status):
+    if status != 0:
+        msg = load().bw_last_error()
+        raise EngineError(status, msg.decode() if msg else "")
+
+
+def _host_ptr(a: np.ndarray):
+    assert a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"], "host buffers must be C-contiguous uint32"
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _dev_ptr(t):
+    import torch
+    assert t.is_cuda and t.dtype in (torch.int32, torch.uint32) and t.is_contiguous()
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def seeded_fill_host(count, seed, tag, p, lo=0):
+    out = np.empty(count, dtype=np.uint32)
+    _check(load().bw_seeded_fill_host(_host_ptr(out), count, seed, tag, p, lo))
+    return out
+
+
+def seeded_fill_device(out, seed, tag, p, lo=0, stream=None):
+    """Fill a CUDA int32 tensor with the seeded stream (seed, tag) on [lo, p)."""
+    _check(load().bw_seeded_fill(_dev_ptr(out), out.numel(), seed, tag, p, lo,
+                                 out.device.index or 0, _stream_ptr(stream)))
+    return out
+
+
+class KoszulEngine:
+    """Synthetic Koszul operator S = D d^T d on one GPU (see include/bw_engine.h).
+
+    ``maps`` is an (r, dim_out, dim_in) uint32 array; ``diag`` is either a
+    host uint32 array or a CUDA int32 tensor of length n_src.
+    """
+
+    def __init__(self, r, k, dim_in, dim_out, prime, block_width, proj_width=None,
+                 maps=None, diag=None, form="plain", device=0):
+        lib = load()
+        self.r, self.k, self.dim_in, self.dim_out, self.p = r, k, dim_in, dim_out, prime
+        self.nb = block_width
+        self.m = block_width if proj_width is None else proj_width
+        self.form = form
+        self.device = device
+        maps = np.ascontiguousarray(maps, dtype=np.uint32).reshape(-1)
+        desc = KoszulDesc(r, k, dim_in, dim_out, prime, self.nb, self.m, FORMS[form],
+                          maps.ctypes.data, 0, 0)
+        if isinstance(diag, np.ndarray):
+            diag = np.ascontiguousarray(diag, dtype=np.uint32)
+            desc.diag = diag.ctypes.data
+        else:
+            desc.diag = diag.data_ptr()
+            desc.diag_on_device = 1
+        handle = ctypes.c_void_p()
+        _check(lib.bw_koszul_create(ctypes.byref(desc), device, ctypes.byref(handle)))
+        self._h = handle
+        info = KoszulInfo()
+        _check(lib.bw_koszul_info_get(self._h, ctypes.byref(info)))
+        self.n_src, self.n_tgt = int(info.n_src), int(info.n_tgt)
+        self.device_bytes, self.scratch_bytes = int(info.device_bytes), int(info.scratch_bytes)
+        self.sm_count = int(info.sm_count)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().bw_koszul_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- device-buffer API -------------------------------------------------
+    def forward(self, y, z, stream=None):
+        _check(load().bw_koszul_forward(self._h, _dev_ptr(y), _dev_ptr(z), _stream_ptr(stream)))
+
+    def transpose(self, z, w, scale_by_diag=True, stream=None):
+        _check(load().bw_koszul_transpose(self._h, _dev_ptr(z), _dev_ptr(w), int(scale_by_diag),
+                                          _stream_ptr(stream)))
+
+    def apply(self, y, out, stream=None):
+        _check(load().bw_koszul_apply(self._h, _dev_ptr(y), _dev_ptr(out), _stream_ptr(stream)))
+
+    def seq_start(self, x, y0, seq, stream=None):
+        cap = seq.numel() // (self.m * self.nb)
+        _check(load().bw_koszul_seq_start(self._h, _dev_ptr(x), _dev_ptr(y0), _dev_ptr(seq), cap,
+                                          _stream_ptr(stream)))
+
+    def seq_step(self, steps, stream=None):
+        _check(load().bw_koszul_seq_step(self._h, steps, _stream_ptr(stream)))
+
+    def seq_finish(self, y_out=None, stream=None):
+        n = ctypes.c_uint64()
+        _check(load().bw_koszul_seq_finish(self._h, _dev_ptr(y_out) if y_out is not None else None,
+                                           ctypes.byref(n), _stream_ptr(stream)))
+        return int(n.value)
+
+    def seq_step_timed(self, steps, stream=None):
+        """Steps with per-kernel CUDA events; returns average ms (forward, transpose, project)."""
+        ms = (ctypes.c_float * 3)()
+        _check(load().bw_koszul_seq_step_timed(self._h, steps, ms, _stream_ptr(stream)))
+        return tuple(float(v) for v in ms)
+
+    # -- host-buffer API ---------------------------------------------------
+    def sequence_host(self, X, Y0, nlen, want_final=True):
+        X = np.ascontiguousarray(X, dtype=np.uint32)
+        Y0 = np.ascontiguousarray(Y0, dtype=np.uint32)
+        seq = np.empty((nlen, self.m, self.nb), dtype=np.uint32)
+        yf = np.empty((self.n_src, self.nb), dtype=np.uint32) if want_final else None
+        _check(load().bw_koszul_sequence_host(self._h, _host_ptr(X), _host_ptr(Y0), nlen, _host_ptr(seq),
+                                              _host_ptr(yf) if yf is not None else None))
+        return seq, yf
+
+    @property
+    def launch_count(self):
+        return int(load().bw_koszul_launch_count(self._h))
