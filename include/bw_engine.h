@@ -134,6 +134,80 @@ BW_API int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* ms_ou
 /* Number of engine kernel launches issued by this context since creation. */
 BW_API uint64_t bw_koszul_launch_count(const bw_koszul* ctx);
 
+/* ------------------------------------------------------------------------
+ * Paper mode: the eliminated cyclic operator of one sector,
+ *   F(x, z) = D_(m-1)(B z - R D_m x),  S = Dc F^t T^t Dr T F Dc,
+ * and its symmetric moment sequence V^t S^k V (block width 4), exactly as the
+ * reference's cuprym_cyclic executable computes it (cuda/cuprym_cyclic.cu).
+ * ---------------------------------------------------------------------- */
+
+typedef struct bw_cyclic bw_cyclic;
+
+#define BW_CYCLIC_APPLY_SQUARE 0          /* S: cols x 4 -> cols x 4 */
+#define BW_CYCLIC_APPLY_FORWARD 1         /* F, no preconditioners: cols x 4 -> rows x 4 */
+#define BW_CYCLIC_APPLY_TRANSPOSE 2       /* F^t, no preconditioners: rows x 4 -> cols x 4 */
+#define BW_CYCLIC_APPLY_SQUARE_UNFOLDED 3 /* S with T, Dr, T^t applied round by round */
+
+typedef struct bw_cyclic_info {
+    uint64_t rows;          /* target rows of F in this sector (N_r) */
+    uint64_t cols;          /* source columns x + z (N_c) */
+    uint64_t x_cols, z_cols, t_rows, y_rows;
+    uint64_t dm_nnz, d2_nnz;
+    uint64_t default_nlen;  /* 2 N_c / 4 + 50 (cuda/cuprym_cyclic.cu:2316) */
+    uint64_t seq_len;       /* moments held after bw_cyclic_generate */
+    uint64_t rowmix_realized_seed, rowmix_hash;
+    uint64_t device_bytes;
+    uint32_t genus, prime, order, sector, y_sector, num_v;
+} bw_cyclic_info;
+
+/* Loads the instance JSON, assembles the sector, draws the seeded
+ * preconditioners and initial block, builds the row-mixing plan and uploads
+ * everything.  Replaces load_cyclic_instance, build_*_generic and the set-up
+ * half of run_eliminated_sector (cuda/cuprym_cyclic.cu:483-819, 2136-2324).
+ * op must be "eliminated"; num_v must be 4 (the paper recipe).  device < 0
+ * opens a host-only context (assembly, seeded data, plan, sidecar; every
+ * device call then fails with status 3). */
+BW_API int bw_cyclic_open(const char* instance_path, const char* op, uint32_t sector, uint32_t num_v,
+                          uint64_t seed, uint32_t rowmix_rounds, uint64_t rowmix_seed, int device,
+                          bw_cyclic** out);
+BW_API int bw_cyclic_info_get(const bw_cyclic* ctx, bw_cyclic_info* out);
+BW_API void bw_cyclic_close(bw_cyclic* ctx);
+
+/* One application (BW_CYCLIC_APPLY_*) through host buffers (row-major,
+ * canonical).  Replaces apply_square / apply_forward / apply_backward
+ * (cuda/cuprym_cyclic.cu:2330-2418). */
+BW_API int bw_cyclic_apply_host(bw_cyclic* ctx, int what, const uint32_t* in, uint32_t* out);
+
+/* Runs the symmetric sequence from the initial block: nlen moments (0 = the
+ * default 2 N_c / 4 + 50), rounded up to whole rounds of 4 moments like the
+ * reference's hot loop (cuda/cuprym_cyclic.cu:2420-2450). */
+BW_API int bw_cyclic_generate(bw_cyclic* ctx, uint64_t nlen);
+
+/* Copies the packed moments (seq_len x 10, upper triangles in WDM order) and
+ * the current block (cols x 4, row-major) to host buffers (either may be NULL). */
+BW_API int bw_cyclic_download(bw_cyclic* ctx, uint32_t* packed_seq, uint64_t seq_capacity, uint32_t* current);
+
+/* Output names and files (cuda/cuprym_cyclic.cu:1295-1400, 965-1007):
+ * output_path creates out_dir and writes the WDM path into buf;
+ * check_outputs_absent fails if the WDM or its sidecar exists;
+ * write_sidecar writes the .rowmix.json; write_wdm writes WDM.tmp, then renames. */
+BW_API int bw_cyclic_output_path(const bw_cyclic* ctx, const char* out_dir, char* buf, size_t cap);
+BW_API int bw_cyclic_check_outputs_absent(const char* wdm_path);
+BW_API int bw_cyclic_write_sidecar(const bw_cyclic* ctx, const char* wdm_path);
+BW_API int bw_cyclic_write_wdm(bw_cyclic* ctx, const char* wdm_path);
+
+/* --validate-rowmix (cuda/cuprym_cyclic.cu:1970-2132): the rowmix transpose
+ * identity on the host, the folded target preconditioner against the
+ * round-by-round one on three deterministic blocks, and the symmetry
+ * <S x, y> = <x, S y>, all on the device. */
+BW_API int bw_cyclic_validate(bw_cyclic* ctx, uint32_t columns);
+
+BW_API uint64_t bw_cyclic_launch_count(const bw_cyclic* ctx);
+
+/* Reads a text file, decompressing it when it carries the zstd magic
+ * (cuda/zstd_compat.h:67-77).  With buf == NULL only *len is set. */
+BW_API int bw_file_read_text(const char* path, char* buf, size_t cap, size_t* len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,6 +10,8 @@ from .engine import (  # noqa: F401
     FORM_INT8,
     FORM_PLAIN,
     KoszulEngine,
+    CyclicEngine,
+    read_text,
     load,
     seeded_fill_device,
     seeded_fill_host,

@@ -1,0 +1,747 @@
+// Paper-mode engine: the eliminated cyclic Koszul operator of one sector,
+//   F(x, z) = D_(m-1) (B z - R D_m x),   S = Dc F^t T^t Dr T F Dc,
+// and its symmetric block-Wiedemann sequence V^t S^k V (block width 4).
+//
+// Replaces the device work of cuda/cuprym_cyclic.cu (run_eliminated_sector,
+// :2136-2496) and cuda/cyclic_cuda_helpers.h.  Differences in structure, not
+// in results (every output is the canonical residue the reference produces):
+//   * one thread per block row holding the 4 columns as one 16-byte vector;
+//   * t = D_m x, y = B z - R t fused into one kernel, and t_adj = R^t h,
+//     x_adj = D_m^t t_adj, z_adj = B^t h, the adjoint assembly fused into one;
+//   * the target preconditioner T^t Dr T (two paired-SL2 rounds, a diagonal
+//     and the two transposed rounds) folded on the host into one exact sparse
+//     matrix with at most 16 entries per row, applied in one pass;
+//   * both Gram moments of a half-round in one reduction kernel whose last CTA
+//     packs the upper triangles (no atomics, deterministic);
+//   * one half-round pair captured as a CUDA graph and replayed.
+#include "bw_cyclic.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <iostream>
+
+namespace bw {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ int32_t red64(long long x, const Mod& m) {
+    long long r = x % m.p;
+    if (r > m.half) r -= m.p;
+    if (r < -m.half) r += m.p;
+    return static_cast<int32_t>(r);
+}
+
+struct Acc4 {
+    long long x = 0, y = 0, z = 0, w = 0;
+    __device__ __forceinline__ void mac(int32_t c, const int4& v) {
+        x += static_cast<long long>(c) * v.x;
+        y += static_cast<long long>(c) * v.y;
+        z += static_cast<long long>(c) * v.z;
+        w += static_cast<long long>(c) * v.w;
+    }
+    __device__ __forceinline__ int4 reduce(const Mod& m) const {
+        return make_int4(red64(x, m), red64(y, m), red64(z, m), red64(w, m));
+    }
+};
+
+__device__ __forceinline__ int4 ld4(const int32_t* base, long long row) {
+    return __ldg(reinterpret_cast<const int4*>(base) + row);
+}
+__device__ __forceinline__ void st4(int32_t* base, long long row, const int4& v) {
+    reinterpret_cast<int4*>(base)[row] = v;
+}
+__device__ __forceinline__ int4 scale4(const int4& v, int32_t s, const Mod& m) {
+    return make_int4(reduce_balanced(v.x * s, m), reduce_balanced(v.y * s, m), reduce_balanced(v.z * s, m),
+                     reduce_balanced(v.w * s, m));
+}
+
+__device__ __forceinline__ void decode_inc(uint32_t e, uint32_t& sub, int& i, bool& neg) {
+    sub = e & 0x3FFFFFFu;
+    i = static_cast<int>((e >> 26) & 31u);
+    neg = (e >> 31) != 0;
+}
+__device__ __forceinline__ void decode_coef(int32_t e, int& local, int32_t& coef) {
+    local = static_cast<int>(static_cast<uint32_t>(e) >> 16);
+    coef = static_cast<int16_t>(e & 0xFFFF);
+}
+
+// out[row] = dc[row] * in[row]  (dc == nullptr: copy)
+__global__ void cyc_scale_kernel(const int32_t* __restrict__ in, const int32_t* __restrict__ dc,
+                                 int32_t* __restrict__ out, long long rows, Mod mod) {
+    for (long long row = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; row < rows;
+         row += static_cast<long long>(gridDim.x) * blockDim.x) {
+        int4 v = ld4(in, row);
+        st4(out, row, dc ? scale4(v, __ldg(dc + row), mod) : v);
+    }
+}
+
+// t(S, beta) = sum_{i not in S} +-sum_a mu[i,beta,a] xs[(S u i, a)]   (D_m forward row)
+__device__ __forceinline__ int4 dm_row(const ElimDev& E, const int32_t* __restrict__ xs, uint32_t S, int beta) {
+    Acc4 acc;
+    const uint32_t* inc = E.dm_row_inc + static_cast<size_t>(S) * E.dm_row_width;
+    for (uint32_t pos = 0; pos < E.dm_row_width; ++pos) {
+        uint32_t cs;
+        int i;
+        bool neg;
+        decode_inc(__ldg(inc + pos), cs, i, neg);
+        const uint32_t base = __ldg(E.x_off + cs);
+        const int li = i * E.n + beta;
+        for (uint32_t k = __ldg(E.fl_off + li); k < __ldg(E.fl_off + li + 1); ++k) {
+            int la;
+            int32_t c;
+            decode_coef(__ldg(E.fl + k), la, c);
+            acc.mac(neg ? -c : c, ld4(xs, base + la));
+        }
+    }
+    return acc.reduce(E.mod);
+}
+
+// y(S, a) = sum_kappa B[a,kappa] zs(S,kappa) - sum_beta R[a,beta] t(S,beta)
+__global__ void cyc_elim_forward_kernel(ElimDev E, const int32_t* __restrict__ xs, int32_t* __restrict__ y) {
+    for (long long yr = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; yr < E.y_rows;
+         yr += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const uint32_t S = __ldg(E.y_sub + yr);
+        const int a = __ldg(E.y_a + yr);
+        Acc4 acc;
+        for (uint32_t zr = __ldg(E.z_off + S); zr < __ldg(E.z_off + S + 1); ++zr) {
+            const int32_t c = __ldg(E.Bk + a * E.kdim + __ldg(E.z_k + zr));
+            if (c) acc.mac(c, ld4(xs, static_cast<long long>(E.x_cols) + zr));
+        }
+        for (uint32_t tr = __ldg(E.t_off + S); tr < __ldg(E.t_off + S + 1); ++tr) {
+            const int beta = __ldg(E.t_beta + tr);
+            const int32_t c = __ldg(E.R + a * E.n + beta);
+            if (!c) continue;
+            acc.mac(-c, dm_row(E, xs, S, beta));
+        }
+        st4(y, yr, acc.reduce(E.mod));
+    }
+}
+
+// u(T2, beta) = sum_{i not in T2} +-sum_a mu[i,beta,a] y(T2 u i, a)   (D_(m-1) forward)
+__global__ void cyc_d2_forward_kernel(ElimDev E, const int32_t* __restrict__ y, int32_t* __restrict__ u) {
+    for (long long ur = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; ur < E.n_r;
+         ur += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const uint32_t S2 = __ldg(E.u_sub + ur);
+        const int beta = __ldg(E.u_beta + ur);
+        Acc4 acc;
+        const uint32_t* inc = E.d2_row_inc + static_cast<size_t>(S2) * E.d2_row_width;
+        for (uint32_t pos = 0; pos < E.d2_row_width; ++pos) {
+            uint32_t cs;
+            int i;
+            bool neg;
+            decode_inc(__ldg(inc + pos), cs, i, neg);
+            const uint32_t base = __ldg(E.y_off + cs);
+            const int li = i * E.n + beta;
+            for (uint32_t k = __ldg(E.fl_off + li); k < __ldg(E.fl_off + li + 1); ++k) {
+                int la;
+                int32_t c;
+                decode_coef(__ldg(E.fl + k), la, c);
+                acc.mac(neg ? -c : c, ld4(y, base + la));
+            }
+        }
+        st4(u, ur, acc.reduce(E.mod));
+    }
+}
+
+// out = P u  (P = T^t Dr T in CSR)
+__global__ void cyc_spmv_kernel(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                                const int32_t* __restrict__ val, const int32_t* __restrict__ u,
+                                int32_t* __restrict__ out, long long rows, Mod mod) {
+    for (long long row = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; row < rows;
+         row += static_cast<long long>(gridDim.x) * blockDim.x) {
+        Acc4 acc;
+        for (uint32_t e = __ldg(ptr + row); e < __ldg(ptr + row + 1); ++e) acc.mac(__ldg(val + e), ld4(u, __ldg(col + e)));
+        st4(out, row, acc.reduce(mod));
+    }
+}
+
+// h(S, a) = sum_{j in S} +-sum_beta mu[j,beta,a] u2(S \ j, beta)   (D_(m-1) transpose)
+__global__ void cyc_d2_transpose_kernel(ElimDev E, const int32_t* __restrict__ u2, int32_t* __restrict__ h) {
+    for (long long yr = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; yr < E.y_rows;
+         yr += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const uint32_t S = __ldg(E.y_sub + yr);
+        const int a = __ldg(E.y_a + yr);
+        Acc4 acc;
+        const uint32_t* inc = E.d2_col_inc + static_cast<size_t>(S) * E.d2_col_width;
+        for (uint32_t pos = 0; pos < E.d2_col_width; ++pos) {
+            uint32_t rs;
+            int j;
+            bool neg;
+            decode_inc(__ldg(inc + pos), rs, j, neg);
+            const uint32_t base = __ldg(E.u_off + rs);
+            const int lj = j * E.g + a;
+            for (uint32_t k = __ldg(E.tl_off + lj); k < __ldg(E.tl_off + lj + 1); ++k) {
+                int lb;
+                int32_t c;
+                decode_coef(__ldg(E.tl + k), lb, c);
+                acc.mac(neg ? -c : c, ld4(u2, base + lb));
+            }
+        }
+        st4(h, yr, acc.reduce(E.mod));
+    }
+}
+
+// t_adj(T, beta) = sum_{a} R[a,beta] h(T, a)
+__device__ __forceinline__ int4 rt_h(const ElimDev& E, const int32_t* __restrict__ h, uint32_t T, int beta) {
+    Acc4 acc;
+    for (uint32_t yr = __ldg(E.y_off + T); yr < __ldg(E.y_off + T + 1); ++yr) {
+        const int32_t c = __ldg(E.R + __ldg(E.y_a + yr) * E.n + beta);
+        if (c) acc.mac(c, ld4(h, yr));
+    }
+    return acc.reduce(E.mod);
+}
+
+// out = Dc [ -D_m^t R^t h ; B^t h ]
+__global__ void cyc_elim_backward_kernel(ElimDev E, const int32_t* __restrict__ h, const int32_t* __restrict__ dc,
+                                         int32_t* __restrict__ out) {
+    const long long total = static_cast<long long>(E.x_cols) + E.z_cols;
+    for (long long row = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; row < total;
+         row += static_cast<long long>(gridDim.x) * blockDim.x) {
+        Acc4 acc;
+        if (row < E.x_cols) {
+            const uint32_t S = __ldg(E.x_sub + row);
+            const int a = __ldg(E.x_a + row);
+            const uint32_t* inc = E.dm_col_inc + static_cast<size_t>(S) * E.dm_col_width;
+            for (uint32_t pos = 0; pos < E.dm_col_width; ++pos) {
+                uint32_t T;
+                int j;
+                bool neg;
+                decode_inc(__ldg(inc + pos), T, j, neg);
+                const uint32_t base = __ldg(E.t_off + T);
+                const int lj = j * E.g + a;
+                for (uint32_t k = __ldg(E.tl_off + lj); k < __ldg(E.tl_off + lj + 1); ++k) {
+                    int lb;
+                    int32_t c;
+                    decode_coef(__ldg(E.tl + k), lb, c);
+                    const int beta = __ldg(E.t_beta + base + lb);
+                    // assembled adjoint negates the x part
+                    acc.mac(neg ? c : -c, rt_h(E, h, T, beta));
+                }
+            }
+        } else {
+            const long long zr = row - E.x_cols;
+            const uint32_t S = __ldg(E.z_sub + zr);
+            const int kap = __ldg(E.z_k + zr);
+            for (uint32_t yr = __ldg(E.y_off + S); yr < __ldg(E.y_off + S + 1); ++yr) {
+                const int32_t c = __ldg(E.Bk + __ldg(E.y_a + yr) * E.kdim + kap);
+                if (c) acc.mac(c, ld4(h, yr));
+            }
+        }
+        int4 v = acc.reduce(E.mod);
+        st4(out, row, dc ? scale4(v, __ldg(dc + row), E.mod) : v);
+    }
+}
+
+// F^t alone (no preconditioners): out = [ -D_m^t R^t h ; B^t h ] with h = D_(m-1)^t in.
+// (cyc_d2_transpose_kernel followed by cyc_elim_backward_kernel with dc = nullptr.)
+
+// One paired-SL2 round on the target block (validation path).
+__global__ void cyc_rowmix_kernel(const uint32_t* __restrict__ pairs, long long count, int32_t* __restrict__ block,
+                                  bool transpose, Mod mod) {
+    for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < count;
+         q += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const uint32_t f = __ldg(pairs + 3 * q), s = __ldg(pairs + 3 * q + 1), ab = __ldg(pairs + 3 * q + 2);
+        const long long a = ab & 0xFFFF, b = ab >> 16, oab = 1 + a * b;
+        const int4 x = ld4(block, f), y = ld4(block, s);
+        int4 nf, ns;
+        if (transpose) {
+            nf = make_int4(red64(x.x + b * y.x, mod), red64(x.y + b * y.y, mod), red64(x.z + b * y.z, mod),
+                           red64(x.w + b * y.w, mod));
+            ns = make_int4(red64(a * x.x + oab * y.x, mod), red64(a * x.y + oab * y.y, mod),
+                           red64(a * x.z + oab * y.z, mod), red64(a * x.w + oab * y.w, mod));
+        } else {
+            nf = make_int4(red64(x.x + a * y.x, mod), red64(x.y + a * y.y, mod), red64(x.z + a * y.z, mod),
+                           red64(x.w + a * y.w, mod));
+            ns = make_int4(red64(b * x.x + oab * y.x, mod), red64(b * x.y + oab * y.y, mod),
+                           red64(b * x.z + oab * y.z, mod), red64(b * x.w + oab * y.w, mod));
+        }
+        st4(block, f, nf);
+        st4(block, s, ns);
+    }
+}
+
+__device__ __forceinline__ int tri_index(int row, int col) { return row * (2 * 4 - row + 1) / 2 + (col - row); }
+
+// Gram moments of one half-round: G1 = A1^t C1 and (count == 2) G2 = A2^t C2,
+// upper triangles packed into seq at positions *seq_index (+1), canonical.
+// partials: gridDim.x x 20 int32; counter left at 0.
+__global__ void __launch_bounds__(kThreads) cyc_gram_kernel(
+    const int32_t* __restrict__ A1, const int32_t* __restrict__ C1, const int32_t* __restrict__ A2,
+    const int32_t* __restrict__ C2, int count, long long rows, int32_t* __restrict__ partials,
+    unsigned int* __restrict__ counter, uint32_t* __restrict__ seq, unsigned long long* __restrict__ seq_index,
+    Mod mod) {
+    int32_t acc[20];
+#pragma unroll
+    for (int e = 0; e < 20; ++e) acc[e] = 0;
+    int cnt = 0;
+    for (long long row = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; row < rows;
+         row += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int4 a1 = ld4(A1, row), c1 = ld4(C1, row);
+        const int av[4] = {a1.x, a1.y, a1.z, a1.w}, cv[4] = {c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+        for (int r0 = 0; r0 < 4; ++r0)
+#pragma unroll
+            for (int c0 = r0; c0 < 4; ++c0) acc[tri_index(r0, c0)] += av[r0] * cv[c0];
+        if (count == 2) {
+            const int4 a2 = ld4(A2, row), c2 = ld4(C2, row);
+            const int bv[4] = {a2.x, a2.y, a2.z, a2.w}, dv[4] = {c2.x, c2.y, c2.z, c2.w};
+#pragma unroll
+            for (int r0 = 0; r0 < 4; ++r0)
+#pragma unroll
+                for (int c0 = r0; c0 < 4; ++c0) acc[10 + tri_index(r0, c0)] += bv[r0] * dv[c0];
+        }
+        if (++cnt == 8) {
+            cnt = 0;
+#pragma unroll
+            for (int e = 0; e < 20; ++e) acc[e] = reduce_partial(acc[e], mod);
+        }
+    }
+    __shared__ int32_t red[kThreads / 32][20];
+    __shared__ bool am_last;
+    // warp reduction (values below 2p; 32 of them stay far inside int32)
+#pragma unroll
+    for (int e = 0; e < 20; ++e) {
+        int32_t v = reduce_balanced(acc[e], mod);
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        acc[e] = v;
+    }
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (lane == 0)
+#pragma unroll
+        for (int e = 0; e < 20; ++e) red[warp][e] = reduce_balanced(acc[e], mod);
+    __syncthreads();
+    if (threadIdx.x < 20) {
+        int32_t s = 0;
+        for (int w = 0; w < kThreads / 32; ++w) s += red[w][threadIdx.x];
+        partials[static_cast<size_t>(blockIdx.x) * 20 + threadIdx.x] = reduce_balanced(s, mod);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    const unsigned long long pos = *reinterpret_cast<volatile unsigned long long*>(seq_index);
+    if (threadIdx.x < 10 * count) {
+        int32_t s = 0;
+        for (unsigned b = 0; b < gridDim.x; ++b) {
+            s += reinterpret_cast<volatile int32_t*>(partials)[static_cast<size_t>(b) * 20 + threadIdx.x];
+            if ((b & 7) == 7) s = reduce_partial(s, mod);
+        }
+        const int which = threadIdx.x / 10, e = threadIdx.x % 10;
+        seq[(pos + which) * 10 + e] = to_canonical(reduce_balanced(s, mod), mod);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *seq_index = pos + count;
+        *counter = 0;
+        __threadfence();
+    }
+}
+
+__global__ void cyc_to_balanced_kernel(const uint32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
+                                       Mod mod) {
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+        out[i] = to_balanced(in[i] % static_cast<uint32_t>(mod.p), mod);
+}
+__global__ void cyc_to_canonical_kernel(const int32_t* __restrict__ in, uint32_t* __restrict__ out, long long n,
+                                        Mod mod) {
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+        out[i] = to_canonical(in[i], mod);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host
+
+CyclicCtx::~CyclicCtx() {
+    if (host_only) return;
+    cudaSetDevice(device);
+    for (auto& g : graphs)
+        if (g) cudaGraphExecDestroy(g);
+    for (void* p : allocations) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+template <class T>
+T* CyclicCtx::upload(const std::vector<T>& host) {
+    void* p = nullptr;
+    const size_t bytes = std::max<size_t>(host.size(), 1) * sizeof(T);
+    BW_CUDA(cudaMalloc(&p, bytes));
+    allocations.push_back(p);
+    device_bytes += bytes;
+    if (!host.empty()) BW_CUDA(cudaMemcpyAsync(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    return static_cast<T*>(p);
+}
+
+template <class T>
+T* CyclicCtx::alloc(size_t count) {
+    void* p = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    BW_CUDA(cudaMalloc(&p, bytes));
+    allocations.push_back(p);
+    device_bytes += bytes;
+    return static_cast<T*>(p);
+}
+
+unsigned CyclicCtx::grid_for(size_t rows) const {
+    const size_t blocks = (rows + kThreads - 1) / kThreads;
+    return static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(blocks, static_cast<size_t>(sms) * 8)));
+}
+
+namespace {
+std::vector<uint32_t> pack_incidence(const std::vector<uint32_t>& sub, const std::vector<uint32_t>& idx,
+                                     const std::vector<uint8_t>& neg) {
+    std::vector<uint32_t> out(sub.size());
+    for (size_t e = 0; e < sub.size(); ++e) {
+        if (sub[e] >= (1u << 26) || idx[e] >= 32) throw Error("incidence does not fit the packed device format", 3);
+        out[e] = sub[e] | (idx[e] << 26) | (neg[e] ? 0x80000000u : 0u);
+    }
+    return out;
+}
+std::vector<int32_t> balanced(const std::vector<uint32_t>& v, const Mod& m) {
+    std::vector<int32_t> out(v.size());
+    for (size_t i = 0; i < v.size(); ++i) out[i] = to_balanced(v[i] % static_cast<uint32_t>(m.p), m);
+    return out;
+}
+}  // namespace
+
+CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& op, size_t sector, size_t num_v,
+                           uint64_t seed, size_t rowmix_rounds, uint64_t rowmix_seed, int dev) {
+    BW_REQUIRE(op == "eliminated", "--operator must be eliminated");
+    BW_REQUIRE(num_v == 4, "the paper pipeline requires exactly 4 block vectors");
+    std::unique_ptr<CyclicCtx> c(new CyclicCtx());
+    c->op = op;
+    c->num_v = num_v;
+    c->seed = seed;
+    c->inst = cyclic::load_instance(instance_path);
+    BW_REQUIRE(sector < c->inst.r, "--sector must be in 0.." + std::to_string(c->inst.r - 1));
+    BW_REQUIRE(cyclic::is_prime(c->inst.modulus), "Modulus " + std::to_string(c->inst.modulus) + " is not prime.");
+    BW_REQUIRE(c->inst.modulus >= 3 && c->inst.modulus < 32768, "the engine supports odd primes below 2^15");
+    c->p = c->inst.modulus;
+    c->mod = make_mod(c->p);
+    c->es = cyclic::assemble_eliminated_sector(c->inst, sector);
+    const auto& es = c->es;
+    const auto& inst = c->inst;
+
+    // Seeded data in the reference's draw order (cuda/cuprym_cyclic.cu:2196-2199).
+    std::mt19937_64 gen(cyclic::seeded_sector_value(seed, sector));
+    c->row_precond = cyclic::random_vector(es.target_rows, c->p, gen, true);
+    c->col_precond = cyclic::random_vector(es.total_cols(), c->p, gen, true);
+    c->initial_block = cyclic::random_vector(es.total_cols() * num_v, c->p, gen, false);
+    c->plan = cyclic::generate_rowmix_plan(es.target_rows, op, sector, c->p, rowmix_rounds, rowmix_seed);
+    if (rowmix_rounds > 0) {
+        c->precond = cyclic::composite_target_preconditioner(c->plan, c->row_precond, c->p);
+    } else {
+        c->precond.row_ptr.resize(es.target_rows + 1);
+        for (size_t i = 0; i <= es.target_rows; ++i) c->precond.row_ptr[i] = static_cast<uint32_t>(i);
+        c->precond.col.resize(es.target_rows);
+        for (size_t i = 0; i < es.target_rows; ++i) c->precond.col[i] = static_cast<uint32_t>(i);
+        c->precond.val = c->row_precond;
+    }
+
+    c->device = dev;
+    if (dev < 0) {   // host-only context: assembly, seeded data, plan and sidecar, no device work
+        c->host_only = true;
+        return c.release();
+    }
+    BW_CUDA(cudaSetDevice(dev));
+    c->sms = sm_count(dev);
+    BW_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+
+    // Coefficient lists: forward (i, beta) -> (local a, mu[i,beta,a]); transpose (j, a) -> (local beta, mu[j,beta,a]).
+    const cyclic::CharMap a0 = cyclic::build_char_map(inst.weight_a0, inst.r);
+    const cyclic::CharMap a1 = cyclic::build_char_map(inst.weight_a1, inst.r);
+    std::vector<uint32_t> fl_off(inst.n * inst.n + 1), tl_off(inst.n * inst.genus + 1);
+    std::vector<int32_t> fl, tl;
+    auto pack = [&](int local, uint32_t mu) {
+        const int32_t b = ::bw::to_balanced(mu, c->mod);
+        return static_cast<int32_t>((static_cast<uint32_t>(local) << 16) | (static_cast<uint32_t>(b) & 0xFFFFu));
+    };
+    for (size_t i = 0; i < inst.n; ++i)
+        for (size_t beta = 0; beta < inst.n; ++beta) {
+            fl_off[i * inst.n + beta] = static_cast<uint32_t>(fl.size());
+            const uint32_t q = static_cast<uint32_t>((inst.weight_a1[beta] + inst.r - inst.weight_v[i] % inst.r) % inst.r);
+            for (uint32_t idx = a0.offsets[q]; idx < a0.offsets[q + 1]; ++idx) {
+                const uint32_t mu = inst.mu_at(i, beta, a0.indices[idx]);
+                if (mu) fl.push_back(pack(static_cast<int>(idx - a0.offsets[q]), mu));
+            }
+        }
+    fl_off[inst.n * inst.n] = static_cast<uint32_t>(fl.size());
+    for (size_t j = 0; j < inst.n; ++j)
+        for (size_t a = 0; a < inst.genus; ++a) {
+            tl_off[j * inst.genus + a] = static_cast<uint32_t>(tl.size());
+            const uint32_t q = static_cast<uint32_t>((inst.weight_a0[a] + inst.weight_v[j]) % inst.r);
+            for (uint32_t idx = a1.offsets[q]; idx < a1.offsets[q + 1]; ++idx) {
+                const uint32_t mu = inst.mu_at(j, a1.indices[idx], a);
+                if (mu) tl.push_back(pack(static_cast<int>(idx - a1.offsets[q]), mu));
+            }
+        }
+    tl_off[inst.n * inst.genus] = static_cast<uint32_t>(tl.size());
+
+    ElimDev& E = c->E;
+    E.mod = c->mod;
+    E.n = static_cast<int>(inst.n);
+    E.g = static_cast<int>(inst.genus);
+    E.kdim = static_cast<int>(inst.kernel_dim());
+    E.x_cols = es.x_cols;
+    E.z_cols = es.z_cols;
+    E.t_rows = es.t_rows;
+    E.y_rows = es.y_rows;
+    E.n_r = es.target_rows;
+    E.dm_row_width = static_cast<uint32_t>(es.dm.row_width);
+    E.dm_col_width = static_cast<uint32_t>(es.dm.column_width);
+    E.d2_row_width = static_cast<uint32_t>(es.d2.row_width);
+    E.d2_col_width = static_cast<uint32_t>(es.d2.column_width);
+    E.t_off = c->upload(es.dm_layout.row_offsets);
+    E.t_beta = c->upload(es.dm_layout.row_beta);
+    E.x_off = c->upload(es.dm_layout.col_offsets);
+    E.x_sub = c->upload(es.dm_layout.col_subset);
+    E.x_a = c->upload(es.dm_layout.col_a);
+    E.dm_row_inc = c->upload(pack_incidence(es.dm.row_col, es.dm.row_i, es.dm.row_neg));
+    E.dm_col_inc = c->upload(pack_incidence(es.dm.col_row, es.dm.col_i, es.dm.col_neg));
+    E.y_off = c->upload(es.d2_layout.col_offsets);
+    E.y_sub = c->upload(es.d2_layout.col_subset);
+    E.y_a = c->upload(es.d2_layout.col_a);
+    E.u_off = c->upload(es.d2_layout.row_offsets);
+    E.u_sub = c->upload(es.d2_layout.row_subset);
+    E.u_beta = c->upload(es.d2_layout.row_beta);
+    E.d2_row_inc = c->upload(pack_incidence(es.d2.row_col, es.d2.row_i, es.d2.row_neg));
+    E.d2_col_inc = c->upload(pack_incidence(es.d2.col_row, es.d2.col_i, es.d2.col_neg));
+    E.z_off = c->upload(es.z_layout.offsets);
+    E.z_sub = c->upload(es.z_layout.subset);
+    E.z_k = c->upload(es.z_layout.index);
+    E.fl_off = c->upload(fl_off);
+    E.fl = c->upload(fl);
+    E.tl_off = c->upload(tl_off);
+    E.tl = c->upload(tl);
+    E.R = c->upload(balanced(inst.right_inverse, c->mod));
+    E.Bk = c->upload(balanced(inst.kernel_basis, c->mod));
+    c->d_dc = c->upload(balanced(c->col_precond, c->mod));
+    c->d_p_ptr = c->upload(c->precond.row_ptr);
+    c->d_p_col = c->upload(c->precond.col);
+    c->d_p_val = c->upload(balanced(c->precond.val, c->mod));
+
+    const size_t nc = es.total_cols(), v = num_v;
+    c->d_b = c->alloc<int32_t>(nc * v);
+    c->d_d = c->alloc<int32_t>(nc * v);
+    c->d_xs = c->alloc<int32_t>(nc * v);
+    c->d_y = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
+    c->d_h = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
+    c->d_u = c->alloc<int32_t>(std::max<size_t>(es.target_rows, 1) * v);
+    c->d_u2 = c->alloc<int32_t>(std::max<size_t>(es.target_rows, 1) * v);
+    c->gram_grid = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>((nc + kThreads - 1) / kThreads,
+                                                                                static_cast<size_t>(c->sms) * 2)));
+    c->d_partials = c->alloc<int32_t>(static_cast<size_t>(c->gram_grid) * 20);
+    c->d_counter = c->alloc<unsigned int>(1);
+    c->d_seq_index = c->alloc<unsigned long long>(1);
+    BW_CUDA(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int), c->stream));
+    BW_CUDA(cudaMemsetAsync(c->d_seq_index, 0, sizeof(unsigned long long), c->stream));
+    // the initial block (canonical -> balanced)
+    uint32_t* tmp = c->upload(c->initial_block);
+    c->to_balanced(tmp, c->d_b, nc * v);
+    BW_CUDA(cudaStreamSynchronize(c->stream));
+    return c.release();
+}
+
+void CyclicCtx::to_balanced(const uint32_t* in, int32_t* out, size_t count) {
+    cyc_to_balanced_kernel<<<grid_for(count), kThreads, 0, stream>>>(in, out, static_cast<long long>(count), mod);
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+void CyclicCtx::to_canonical(const int32_t* in, uint32_t* out, size_t count) {
+    cyc_to_canonical_kernel<<<grid_for(count), kThreads, 0, stream>>>(in, out, static_cast<long long>(count), mod);
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+void CyclicCtx::forward(const int32_t* in, int32_t* u, bool precondition) {
+    const size_t nc = es.total_cols();
+    cyc_scale_kernel<<<grid_for(nc), kThreads, 0, stream>>>(in, precondition ? d_dc : nullptr, d_xs,
+                                                            static_cast<long long>(nc), mod);
+    BW_CHECK_LAUNCH();
+    cyc_elim_forward_kernel<<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, d_xs, d_y);
+    BW_CHECK_LAUNCH();
+    cyc_d2_forward_kernel<<<grid_for(es.target_rows), kThreads, 0, stream>>>(E, d_y, u);
+    BW_CHECK_LAUNCH();
+    launches += 3;
+}
+
+void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
+    cyc_d2_transpose_kernel<<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, u2, d_h);
+    BW_CHECK_LAUNCH();
+    cyc_elim_backward_kernel<<<grid_for(es.total_cols()), kThreads, 0, stream>>>(E, d_h, precondition ? d_dc : nullptr,
+                                                                                 out);
+    BW_CHECK_LAUNCH();
+    launches += 2;
+}
+
+void CyclicCtx::target_precondition(const int32_t* u, int32_t* u2) {
+    cyc_spmv_kernel<<<grid_for(es.target_rows), kThreads, 0, stream>>>(d_p_ptr, d_p_col, d_p_val, u, u2,
+                                                                       static_cast<long long>(es.target_rows), mod);
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+void CyclicCtx::apply_square(const int32_t* in, int32_t* out) {
+    forward(in, d_u, true);
+    target_precondition(d_u, d_u2);
+    backward(d_u2, out, true);
+}
+
+void CyclicCtx::gram(const int32_t* a1, const int32_t* c1, const int32_t* a2, const int32_t* c2, int count) {
+    cyc_gram_kernel<<<gram_grid, kThreads, 0, stream>>>(a1, c1, a2 ? a2 : a1, c2 ? c2 : c1, count,
+                                                        static_cast<long long>(es.total_cols()), d_partials,
+                                                        d_counter, d_seq, d_seq_index, mod);
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+// One round of the reference's loop (cuda/cuprym_cyclic.cu:2443-2449):
+// D = S B; push B^t D, D^t D; B = S D; push B^t D, B^t B.
+void CyclicCtx::round() {
+    apply_square(d_b, d_d);
+    gram(d_b, d_d, d_d, d_d, 2);
+    apply_square(d_d, d_b);
+    gram(d_b, d_d, d_b, d_b, 2);
+}
+
+void CyclicCtx::generate(size_t nlen_target) {
+    const size_t nc = es.total_cols();
+    const size_t default_nlen = (2 * nc) / num_v + 50;
+    const size_t max_nlen = nlen_target == 0 ? default_nlen : nlen_target;
+    const size_t rounds = (max_nlen - 1 + 3) / 4;
+    seq_capacity = max_nlen + 5;
+    if (!d_seq || seq_alloc < seq_capacity) {
+        d_seq = alloc<uint32_t>(seq_capacity * 10);
+        seq_alloc = seq_capacity;
+        for (auto& g : graphs)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    }
+    BW_CUDA(cudaMemsetAsync(d_seq_index, 0, sizeof(unsigned long long), stream));
+    BW_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), stream));
+    // restart from the initial block
+    uint32_t* tmp = scratch_canonical();
+    BW_CUDA(cudaMemcpyAsync(tmp, initial_block.data(), nc * num_v * 4, cudaMemcpyHostToDevice, stream));
+    to_balanced(tmp, d_b, nc * num_v);
+    gram(d_b, d_b, nullptr, nullptr, 1);
+    if (rounds > 0) {
+        if (!graphs[0]) {
+            const uint64_t l0 = launches;
+            cudaGraph_t graph;
+            BW_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                round();
+            } catch (...) {
+                cudaStreamEndCapture(stream, &graph);
+                throw;
+            }
+            BW_CUDA(cudaStreamEndCapture(stream, &graph));
+            graph_kernels = launches - l0;
+            launches = l0;
+            BW_CUDA(cudaGraphInstantiate(&graphs[0], graph, 0));
+            cudaGraphDestroy(graph);
+        }
+        for (size_t r = 0; r < rounds; ++r) {
+            BW_CUDA(cudaGraphLaunch(graphs[0], stream));
+            launches += graph_kernels;
+        }
+    }
+    seq_len = 1 + 4 * rounds;
+    BW_CUDA(cudaStreamSynchronize(stream));
+}
+
+uint32_t* CyclicCtx::scratch_canonical() {
+    if (!d_canon) d_canon = alloc<uint32_t>(std::max<size_t>(es.total_cols(), es.target_rows) * num_v);
+    return d_canon;
+}
+
+void CyclicCtx::download_state(std::vector<uint32_t>& current, std::vector<uint32_t>& packed) {
+    const size_t nc = es.total_cols();
+    uint32_t* tmp = scratch_canonical();
+    to_canonical(d_b, tmp, nc * num_v);
+    current.resize(nc * num_v);
+    packed.resize(seq_len * 10);
+    BW_CUDA(cudaMemcpyAsync(current.data(), tmp, current.size() * 4, cudaMemcpyDeviceToHost, stream));
+    BW_CUDA(cudaMemcpyAsync(packed.data(), d_seq, packed.size() * 4, cudaMemcpyDeviceToHost, stream));
+    BW_CUDA(cudaStreamSynchronize(stream));
+}
+
+// Host-buffer operator applications (validation and tests).
+void CyclicCtx::apply_host(int what, const uint32_t* in, uint32_t* out) {
+    const size_t nc = es.total_cols(), nr = es.target_rows, v = num_v;
+    uint32_t* tmp = scratch_canonical();
+    if (what == BW_CYCLIC_APPLY_SQUARE || what == BW_CYCLIC_APPLY_FORWARD) {
+        BW_CUDA(cudaMemcpyAsync(tmp, in, nc * v * 4, cudaMemcpyHostToDevice, stream));
+        to_balanced(tmp, d_d, nc * v);
+        if (what == BW_CYCLIC_APPLY_SQUARE) {
+            apply_square(d_d, d_d);   // in place is safe: the first kernel copies into d_xs
+            to_canonical(d_d, tmp, nc * v);
+            BW_CUDA(cudaMemcpyAsync(out, tmp, nc * v * 4, cudaMemcpyDeviceToHost, stream));
+        } else {
+            forward(d_d, d_u, false);
+            to_canonical(d_u, tmp, nr * v);
+            BW_CUDA(cudaMemcpyAsync(out, tmp, nr * v * 4, cudaMemcpyDeviceToHost, stream));
+        }
+    } else if (what == BW_CYCLIC_APPLY_TRANSPOSE) {
+        BW_CUDA(cudaMemcpyAsync(tmp, in, nr * v * 4, cudaMemcpyHostToDevice, stream));
+        to_balanced(tmp, d_u2, nr * v);
+        backward(d_u2, d_d, false);
+        to_canonical(d_d, tmp, nc * v);
+        BW_CUDA(cudaMemcpyAsync(out, tmp, nc * v * 4, cudaMemcpyDeviceToHost, stream));
+    } else if (what == BW_CYCLIC_APPLY_SQUARE_UNFOLDED) {
+        // The reference's order of operations for the target preconditioner:
+        // rowmix rounds, Dr, transposed rounds in reverse (validation of the folded P).
+        BW_CUDA(cudaMemcpyAsync(tmp, in, nc * v * 4, cudaMemcpyHostToDevice, stream));
+        to_balanced(tmp, d_d, nc * v);
+        forward(d_d, d_u, true);
+        if (plan.rounds > 0) {
+            if (!d_pairs) {
+                std::vector<uint32_t> flat;
+                for (const auto& round : plan.round_pairs) {
+                    pair_offsets.push_back(flat.size() / 3);
+                    for (const auto& pr : round) {
+                        flat.push_back(pr.first);
+                        flat.push_back(pr.second);
+                        flat.push_back(static_cast<uint32_t>(pr.a) | (static_cast<uint32_t>(pr.b) << 16));
+                    }
+                }
+                pair_offsets.push_back(flat.size() / 3);
+                d_pairs = upload(flat);
+                d_dr = upload(balanced(row_precond, mod));
+            }
+            for (size_t r = 0; r < plan.rounds; ++r) {
+                const long long cnt = static_cast<long long>(pair_offsets[r + 1] - pair_offsets[r]);
+                cyc_rowmix_kernel<<<grid_for(cnt), kThreads, 0, stream>>>(d_pairs + 3 * pair_offsets[r], cnt, d_u,
+                                                                          false, mod);
+                BW_CHECK_LAUNCH();
+            }
+            cyc_scale_kernel<<<grid_for(nr), kThreads, 0, stream>>>(d_u, d_dr, d_u2, static_cast<long long>(nr), mod);
+            BW_CHECK_LAUNCH();
+            for (size_t r = plan.rounds; r > 0; --r) {
+                const long long cnt = static_cast<long long>(pair_offsets[r] - pair_offsets[r - 1]);
+                cyc_rowmix_kernel<<<grid_for(cnt), kThreads, 0, stream>>>(d_pairs + 3 * pair_offsets[r - 1], cnt,
+                                                                          d_u2, true, mod);
+                BW_CHECK_LAUNCH();
+            }
+        } else {
+            target_precondition(d_u, d_u2);
+        }
+        backward(d_u2, d_d, true);
+        to_canonical(d_d, tmp, nc * v);
+        BW_CUDA(cudaMemcpyAsync(out, tmp, nc * v * 4, cudaMemcpyDeviceToHost, stream));
+    } else {
+        throw Error("unknown application kind", 1);
+    }
+    BW_CUDA(cudaStreamSynchronize(stream));
+}
+
+}  // namespace bw

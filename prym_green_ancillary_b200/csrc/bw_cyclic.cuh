@@ -1,0 +1,100 @@
+// Paper-mode (eliminated cyclic operator) engine context.
+#pragma once
+
+#include "bw_common.cuh"
+#include "cyclic_host.hpp"
+#include "../../include/bw_engine.h"
+
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace bw {
+
+// Device view of one eliminated sector (all pointers device, read-only).
+struct ElimDev {
+    Mod mod;
+    int n, g, kdim;
+    uint64_t x_cols, z_cols, t_rows, y_rows, n_r;
+    uint32_t dm_row_width, dm_col_width, d2_row_width, d2_col_width;
+    // D_m: rows t = (S, beta) over (m-1)-subsets, columns x = (S', a) over m-subsets
+    const uint32_t *t_off, *x_off, *x_sub;
+    const uint16_t *t_beta, *x_a;
+    const uint32_t *dm_row_inc, *dm_col_inc;   // packed: subset | i << 26 | negative << 31
+    // D_(m-1): columns y = (S, a) over (m-1)-subsets, rows u = (S2, beta) over (m-2)-subsets
+    const uint32_t *y_off, *y_sub, *u_off, *u_sub;
+    const uint16_t *y_a, *u_beta;
+    const uint32_t *d2_row_inc, *d2_col_inc;
+    // z = (S, kappa) over (m-1)-subsets
+    const uint32_t *z_off, *z_sub;
+    const uint16_t* z_k;
+    // coefficient lists: local index << 16 | balanced mu (int16)
+    const uint32_t *fl_off, *tl_off;
+    const int32_t *fl, *tl;
+    const int32_t *R, *Bk;   // g x n, g x kdim (balanced)
+};
+
+struct CyclicCtx {
+    int device = 0, sms = 0;
+    bool host_only = false;
+    uint32_t p = 0;
+    Mod mod{};
+    std::string op = "eliminated";
+    size_t num_v = 4;
+    uint64_t seed = 1;
+    cyclic::Instance inst;
+    cyclic::EliminatedSector es;
+    std::vector<uint32_t> row_precond, col_precond, initial_block;
+    cyclic::RowMixPlan plan;
+    cyclic::Csr precond;
+
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocations;
+    uint64_t device_bytes = 0, launches = 0, graph_kernels = 0;
+    ElimDev E{};
+    int32_t* d_dc = nullptr;
+    uint32_t *d_p_ptr = nullptr, *d_p_col = nullptr;
+    int32_t* d_p_val = nullptr;
+    int32_t *d_b = nullptr, *d_d = nullptr, *d_xs = nullptr, *d_y = nullptr, *d_h = nullptr, *d_u = nullptr,
+            *d_u2 = nullptr;
+    uint32_t* d_canon = nullptr;
+    unsigned gram_grid = 1;
+    int32_t* d_partials = nullptr;
+    unsigned int* d_counter = nullptr;
+    unsigned long long* d_seq_index = nullptr;
+    uint32_t* d_seq = nullptr;
+    size_t seq_alloc = 0, seq_capacity = 0, seq_len = 0;
+    cudaGraphExec_t graphs[1] = {nullptr};
+    // validation path (explicit rowmix rounds)
+    uint32_t* d_pairs = nullptr;
+    int32_t* d_dr = nullptr;
+    std::vector<size_t> pair_offsets;
+
+    static CyclicCtx* open(const std::string& instance_path, const std::string& op, size_t sector, size_t num_v,
+                           uint64_t seed, size_t rowmix_rounds, uint64_t rowmix_seed, int dev);
+    ~CyclicCtx();
+
+    template <class T>
+    T* upload(const std::vector<T>& host);
+    template <class T>
+    T* alloc(size_t count);
+    unsigned grid_for(size_t rows) const;
+    uint32_t* scratch_canonical();
+
+    void to_balanced(const uint32_t* in, int32_t* out, size_t count);
+    void to_canonical(const int32_t* in, uint32_t* out, size_t count);
+    void forward(const int32_t* in, int32_t* u, bool precondition);
+    void target_precondition(const int32_t* u, int32_t* u2);
+    void backward(const int32_t* u2, int32_t* out, bool precondition);
+    void apply_square(const int32_t* in, int32_t* out);
+    void gram(const int32_t* a1, const int32_t* c1, const int32_t* a2, const int32_t* c2, int count);
+    void round();
+    void generate(size_t nlen_target);
+    void download_state(std::vector<uint32_t>& current, std::vector<uint32_t>& packed);
+    void apply_host(int what, const uint32_t* in, uint32_t* out);
+    void require_device() const {
+        if (host_only) throw Error("this context was opened host-only (device < 0)", 3);
+    }
+};
+
+}  // namespace bw

@@ -1,0 +1,693 @@
+// Host-side assembly of the eliminated cyclic operator (see cyclic_host.hpp).
+#include "cyclic_host.hpp"
+
+#include "json_lite.hpp"
+
+#include <algorithm>
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
+#include <limits>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+
+namespace bw {
+namespace cyclic {
+
+namespace {
+
+constexpr uint64_t kFnvOffset = 14695981039346656037ULL;
+constexpr uint64_t kFnvPrime = 1099511628211ULL;
+
+uint64_t binom64(size_t n, size_t k) {
+    if (k > n) return 0;
+    k = std::min(k, n - k);
+    unsigned __int128 out = 1;
+    for (size_t i = 0; i < k; ++i) {
+        out = out * (n - i) / (i + 1);
+        if (out > std::numeric_limits<uint64_t>::max()) throw std::runtime_error("binomial coefficient overflows u64");
+    }
+    return static_cast<uint64_t>(out);
+}
+
+uint32_t sub_mod(size_t a, size_t b, size_t r) { return static_cast<uint32_t>((a + r - (b % r)) % r); }
+
+uint32_t checked_u32(size_t v, const std::string& label) {
+    if (v > std::numeric_limits<uint32_t>::max()) throw std::runtime_error(label + " does not fit in uint32_t");
+    return static_cast<uint32_t>(v);
+}
+
+std::string read_file(const std::string& path) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in) throw std::runtime_error("failed to open " + path);
+    std::ostringstream ss;
+    ss << in.rdbuf();
+    return ss.str();
+}
+
+std::vector<uint16_t> weight_array(const json::Value& obj, const std::string& key, size_t r) {
+    std::vector<int64_t> raw = obj.at(key).ints(key);
+    std::vector<uint16_t> out;
+    out.reserve(raw.size());
+    for (int64_t v : raw) {
+        if (v < 0 || static_cast<uint64_t>(v) >= r || v > 65535)
+            throw std::runtime_error("weight " + std::to_string(v) + " in " + key + " is outside 0..r-1");
+        out.push_back(static_cast<uint16_t>(v));
+    }
+    return out;
+}
+
+std::vector<uint32_t> mod_array(const json::Value& obj, const std::string& key, size_t expected, uint32_t modulus) {
+    std::vector<int64_t> raw = obj.at(key).ints(key);
+    if (expected != 0 && raw.size() != expected)
+        throw std::runtime_error(key + " has " + std::to_string(raw.size()) + " entries; expected " +
+                                 std::to_string(expected));
+    std::vector<uint32_t> out;
+    out.reserve(raw.size());
+    for (int64_t v : raw) {
+        if (v < 0 || static_cast<uint64_t>(v) >= modulus)
+            throw std::runtime_error(key + " entry is not reduced modulo the instance modulus");
+        out.push_back(static_cast<uint32_t>(v));
+    }
+    return out;
+}
+
+std::vector<uint64_t> u64_array(const json::Value& obj, const std::string& key) {
+    std::vector<int64_t> raw = obj.at(key).ints(key);
+    std::vector<uint64_t> out(raw.size());
+    for (size_t i = 0; i < raw.size(); ++i) {
+        if (raw[i] < 0) throw std::runtime_error(key + " has a negative entry");
+        out[i] = static_cast<uint64_t>(raw[i]);
+    }
+    return out;
+}
+
+// mu_w R = I and mu_w B = 0 (cuda/cuprym_cyclic.cu:423-481).
+void validate_elimination(const Instance& inst) {
+    if (!inst.has_elimination) return;
+    if (inst.w_index >= inst.n) throw std::runtime_error("elimination w_V_index is outside V");
+    if (inst.w_weight != inst.weight_v[inst.w_index])
+        throw std::runtime_error("elimination w_weight does not match V weight");
+    if (inst.right_inverse.size() != inst.genus * inst.n)
+        throw std::runtime_error("elimination right inverse has wrong shape");
+    const size_t kd = inst.kernel_dim();
+    if (kd == 0) throw std::runtime_error("elimination kernel basis is empty");
+    if (inst.kernel_basis.size() != inst.genus * kd) throw std::runtime_error("elimination kernel basis has wrong shape");
+    const uint64_t p = inst.modulus;
+    for (size_t beta = 0; beta < inst.n; ++beta) {
+        for (size_t gamma = 0; gamma < inst.n; ++gamma) {
+            uint64_t acc = 0;
+            for (size_t a = 0; a < inst.genus; ++a)
+                acc = (acc + static_cast<uint64_t>(inst.mu_at(inst.w_index, beta, a)) *
+                                 inst.right_inverse[a * inst.n + gamma]) % p;
+            if (acc != (beta == gamma ? 1u : 0u))
+                throw std::runtime_error("elimination right inverse check mu_w*R=I failed");
+        }
+        for (size_t k = 0; k < kd; ++k) {
+            uint64_t acc = 0;
+            for (size_t a = 0; a < inst.genus; ++a)
+                acc = (acc + static_cast<uint64_t>(inst.mu_at(inst.w_index, beta, a)) *
+                                 inst.kernel_basis[a * kd + k]) % p;
+            if (acc != 0) throw std::runtime_error("elimination kernel check mu_w*B=0 failed");
+        }
+    }
+}
+
+uint64_t fnv_u8(uint64_t h, uint8_t v) { return (h ^ v) * kFnvPrime; }
+uint64_t fnv_u64(uint64_t h, uint64_t v) {
+    for (int b = 0; b < 8; ++b) h = fnv_u8(h, static_cast<uint8_t>((v >> (8 * b)) & 0xffu));
+    return h;
+}
+uint64_t fnv_str(uint64_t h, const std::string& s) {
+    for (unsigned char c : s) h = fnv_u8(h, c);
+    return h;
+}
+
+uint64_t lex_rank_mask(uint64_t mask, size_t n, size_t k) {
+    // rank = C(n,k) - 1 - sum_pos C(n-1-s_pos, k-pos)
+    uint64_t acc = 0;
+    size_t pos = 0;
+    for (size_t v = 0; v < n && pos < k; ++v)
+        if (mask & (1ULL << v)) acc += binom64(n - 1 - v, k - pos++);
+    return binom64(n, k) - 1 - acc;
+}
+
+}  // namespace
+
+bool is_prime(uint32_t n) {
+    if (n <= 1) return false;
+    for (uint32_t i = 2; i <= n / i; ++i)
+        if (n % i == 0) return false;
+    return true;
+}
+
+// load_cyclic_instance (cuda/cuprym_cyclic.cu:483-609).
+Instance load_instance(const std::string& path) {
+    const std::string text = read_file(path);
+    const json::Value root = json::parse(text);
+    Instance inst;
+    const uint64_t genus = root.at("genus").as_u64("genus");
+    const uint64_t modulus = root.at("modulus").as_u64("modulus");
+    const uint64_t r = root.at("cyclic").at("order").as_u64("cyclic.order");
+    if (modulus == 0 || modulus > 65535) throw std::runtime_error("instance modulus must fit uint16_t CUDA storage");
+    if (genus < 6 || genus % 2 != 0) throw std::runtime_error("cyclic Prym CUDA path expects an even genus >= 6");
+    inst.genus = genus;
+    inst.modulus = static_cast<uint32_t>(modulus);
+    inst.r = r;
+    inst.n = genus - 3;
+    inst.m = genus / 2;
+    if (r == 0 || inst.m > inst.n) throw std::runtime_error("invalid cyclic Prym dimensions");
+    const json::Value& w = root.at("weights");
+    inst.weight_v = weight_array(w, "V", r);
+    inst.weight_a0 = weight_array(w, "A0", r);
+    inst.weight_a1 = weight_array(w, "A1", r);
+    if (inst.weight_v.size() != inst.n || inst.weight_a0.size() != inst.genus || inst.weight_a1.size() != inst.n)
+        throw std::runtime_error("cyclic weight vector lengths do not match genus metadata");
+    const json::Value& mu = root.at("artinian").at("mu");
+    const uint64_t mu_n = mu.at("n").as_u64("mu.n"), mu_g = mu.at("g").as_u64("mu.g");
+    inst.mu = mod_array(mu, "values", 0, inst.modulus);
+    if (mu_n != inst.n || mu_g != inst.genus || inst.mu.size() != inst.n * inst.n * inst.genus)
+        throw std::runtime_error("artinian.mu dimensions do not match cyclic genus metadata");
+    if (const json::Value* k = root.find("koszul")) {
+        try {
+            inst.expected_sector_columns = u64_array(*k, "sector_columns");
+            inst.expected_sector_rows = u64_array(*k, "sector_rows");
+            inst.expected_sector_nnz = u64_array(*k, "sector_nnz");
+        } catch (const std::exception&) {
+            inst.expected_sector_columns.clear();
+            inst.expected_sector_rows.clear();
+            inst.expected_sector_nnz.clear();
+        }
+    }
+    if (const json::Value* e = root.find("third_section_elimination")) {
+        inst.has_elimination = true;
+        const uint64_t wi = e->at("w_V_index").as_u64("w_V_index");
+        const uint64_t ww = e->at("w_weight").as_u64("w_weight");
+        if (ww >= r) throw std::runtime_error("third_section_elimination scalar metadata is invalid");
+        inst.w_index = wi;
+        inst.w_weight = static_cast<uint16_t>(ww);
+        inst.kernel_weights = weight_array(*e, "kernel_weights", r);
+        inst.right_inverse = mod_array(*e, "right_inverse_A0_by_A1", inst.genus * inst.n, inst.modulus);
+        inst.kernel_basis = mod_array(*e, "kernel_basis_A0_by_3", inst.genus * inst.kernel_dim(), inst.modulus);
+        inst.expected_elim_columns = u64_array(*e, "sector_columns");
+        inst.expected_elim_rows = u64_array(*e, "sector_rows");
+    }
+    validate_elimination(inst);
+    return inst;
+}
+
+size_t CharMap::max_block() const {
+    size_t best = 0;
+    for (size_t c = 0; c + 1 < offsets.size(); ++c) best = std::max<size_t>(best, offsets[c + 1] - offsets[c]);
+    return best;
+}
+
+// build_character_map (cuda/cuprym_cyclic.cu:611-627).
+CharMap build_char_map(const std::vector<uint16_t>& weights, size_t r) {
+    CharMap map;
+    map.offsets.resize(r + 1);
+    for (size_t ch = 0; ch < r; ++ch) {
+        map.offsets[ch] = checked_u32(map.indices.size(), "character offset");
+        for (size_t idx = 0; idx < weights.size(); ++idx)
+            if (weights[idx] == ch) map.indices.push_back(static_cast<uint16_t>(idx));
+    }
+    map.offsets[r] = checked_u32(map.indices.size(), "character offset");
+    return map;
+}
+
+// build_common_incidences_generic (cuda/cuprym_cyclic.cu:631-727), with the
+// subset ranks computed by the lexicographic ranking formula instead of a hash
+// map (same ranks: the lexicographic order of itertools.combinations).
+Incidence build_incidences(size_t local_n, size_t degree, size_t r, const std::vector<size_t>& original,
+                           const std::vector<uint16_t>& local_weights) {
+    if (local_n >= 64) throw std::runtime_error("implicit operator supports local_n < 64");
+    if (degree == 0 || degree > local_n) throw std::runtime_error("source exterior degree is invalid");
+    if (original.size() != local_n || local_weights.size() != local_n)
+        throw std::runtime_error("local index metadata has the wrong length");
+    Incidence inc;
+    inc.local_n = local_n;
+    inc.degree = degree;
+    const size_t td = degree - 1;
+    inc.row_subsets = binom64(local_n, td);
+    inc.column_subsets = binom64(local_n, degree);
+    inc.row_width = local_n - td;
+    inc.column_width = degree;
+    inc.row_subset_weights.resize(inc.row_subsets);
+    inc.column_subset_weights.resize(inc.column_subsets);
+    inc.row_i.reserve(inc.row_subsets * inc.row_width);
+    inc.row_col.reserve(inc.row_subsets * inc.row_width);
+    inc.row_neg.reserve(inc.row_subsets * inc.row_width);
+    inc.col_i.reserve(inc.column_subsets * degree);
+    inc.col_row.reserve(inc.column_subsets * degree);
+    inc.col_neg.reserve(inc.column_subsets * degree);
+
+    // Enumerate (d-1)-subsets in lexicographic order.
+    std::vector<size_t> s(td);
+    for (size_t i = 0; i < td; ++i) s[i] = i;
+    for (uint64_t rank = 0; rank < inc.row_subsets; ++rank) {
+        uint64_t mask = 0;
+        size_t wsum = 0;
+        for (size_t v : s) {
+            mask |= 1ULL << v;
+            wsum += local_weights[v];
+        }
+        inc.row_subset_weights[rank] = static_cast<uint16_t>(wsum % r);
+        size_t position = 0;
+        for (size_t li = 0; li < local_n; ++li) {
+            if (mask & (1ULL << li)) {
+                ++position;
+                continue;
+            }
+            inc.row_i.push_back(checked_u32(original[li], "row incidence i"));
+            inc.row_col.push_back(checked_u32(lex_rank_mask(mask | (1ULL << li), local_n, degree), "column rank"));
+            inc.row_neg.push_back(static_cast<uint8_t>(position % 2 == 1));
+        }
+        // next combination
+        if (td > 0) {
+            size_t i = td;
+            while (i > 0 && s[i - 1] == local_n - td + i - 1) --i;
+            if (i == 0) break;
+            ++s[i - 1];
+            for (size_t j = i; j < td; ++j) s[j] = s[j - 1] + 1;
+        }
+    }
+    std::vector<size_t> c(degree);
+    for (size_t i = 0; i < degree; ++i) c[i] = i;
+    for (uint64_t rank = 0; rank < inc.column_subsets; ++rank) {
+        uint64_t mask = 0;
+        size_t wsum = 0;
+        for (size_t v : c) {
+            mask |= 1ULL << v;
+            wsum += local_weights[v];
+        }
+        inc.column_subset_weights[rank] = static_cast<uint16_t>(wsum % r);
+        for (size_t position = 0; position < degree; ++position) {
+            const size_t li = c[position];
+            inc.col_i.push_back(checked_u32(original[li], "column incidence i"));
+            inc.col_row.push_back(checked_u32(lex_rank_mask(mask & ~(1ULL << li), local_n, td), "row rank"));
+            inc.col_neg.push_back(static_cast<uint8_t>(position % 2 == 1));
+        }
+        size_t i = degree;
+        while (i > 0 && c[i - 1] == local_n - degree + i - 1) --i;
+        if (i == 0) break;
+        ++c[i - 1];
+        for (size_t j = i; j < degree; ++j) c[j] = c[j - 1] + 1;
+    }
+    return inc;
+}
+
+// build_sector_layout_generic (cuda/cuprym_cyclic.cu:733-790).
+SectorLayout build_sector_layout(const Instance& inst, const Incidence& inc, const CharMap& a0, const CharMap& a1,
+                                 size_t sector) {
+    SectorLayout L;
+    L.sector = sector;
+    L.row_offsets.resize(inc.row_subsets + 1);
+    L.col_offsets.resize(inc.column_subsets + 1);
+    for (size_t rr = 0; rr < inc.row_subsets; ++rr) {
+        L.row_offsets[rr] = checked_u32(L.row_subset.size(), "row offset");
+        const uint32_t ch = sub_mod(sector, inc.row_subset_weights[rr], inst.r);
+        for (uint32_t idx = a1.offsets[ch]; idx < a1.offsets[ch + 1]; ++idx) {
+            L.row_subset.push_back(static_cast<uint32_t>(rr));
+            L.row_beta.push_back(a1.indices[idx]);
+        }
+    }
+    L.row_offsets[inc.row_subsets] = checked_u32(L.row_subset.size(), "row offset");
+    for (size_t cr = 0; cr < inc.column_subsets; ++cr) {
+        L.col_offsets[cr] = checked_u32(L.col_subset.size(), "column offset");
+        const uint32_t ch = sub_mod(sector, inc.column_subset_weights[cr], inst.r);
+        for (uint32_t idx = a0.offsets[ch]; idx < a0.offsets[ch + 1]; ++idx) {
+            L.col_subset.push_back(static_cast<uint32_t>(cr));
+            L.col_a.push_back(a0.indices[idx]);
+        }
+    }
+    L.col_offsets[inc.column_subsets] = checked_u32(L.col_subset.size(), "column offset");
+    uint64_t nnz = 0;
+    for (size_t row = 0; row < L.row_subset.size(); ++row) {
+        const size_t rr = L.row_subset[row];
+        const uint32_t beta = L.row_beta[row];
+        for (size_t pos = 0; pos < inc.row_width; ++pos) {
+            const uint32_t i = inc.row_i[rr * inc.row_width + pos];
+            const uint32_t q = sub_mod(inst.weight_a1[beta], inst.weight_v[i], inst.r);
+            for (uint32_t idx = a0.offsets[q]; idx < a0.offsets[q + 1]; ++idx)
+                if (inst.mu_at(i, beta, a0.indices[idx]) != 0) ++nnz;
+        }
+    }
+    L.nnz = nnz;
+    return L;
+}
+
+// build_tensor_layout (cuda/cuprym_cyclic.cu:796-819).
+TensorLayout build_tensor_layout(const std::vector<uint16_t>& subset_weights, const CharMap& map, size_t r,
+                                 size_t sector) {
+    TensorLayout L;
+    L.offsets.resize(subset_weights.size() + 1);
+    for (size_t s = 0; s < subset_weights.size(); ++s) {
+        L.offsets[s] = checked_u32(L.subset.size(), "tensor offset");
+        const uint32_t ch = sub_mod(sector, subset_weights[s], r);
+        for (uint32_t idx = map.offsets[ch]; idx < map.offsets[ch + 1]; ++idx) {
+            L.subset.push_back(static_cast<uint32_t>(s));
+            L.index.push_back(map.indices[idx]);
+        }
+    }
+    L.offsets[subset_weights.size()] = checked_u32(L.subset.size(), "tensor offset");
+    return L;
+}
+
+// seeded_sector_value (cuda/cuprym_cyclic.cu:1143-1151).
+uint64_t seeded_sector_value(uint64_t seed, size_t sector) {
+    uint64_t x = seed ^ (0x9E3779B97F4A7C15ULL + (static_cast<uint64_t>(sector) << 6) + (static_cast<uint64_t>(sector) >> 2));
+    x ^= x >> 30;
+    x *= 0xBF58476D1CE4E5B9ULL;
+    x ^= x >> 27;
+    x *= 0x94D049BB133111EBULL;
+    x ^= x >> 31;
+    return x;
+}
+
+uint64_t splitmix64_next(uint64_t& state) {
+    uint64_t z = (state += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// generate_random_vector (cuda/matrices.h:44-56): the libstdc++ uniform
+// distribution over mt19937_64, drawn in the caller's order.
+std::vector<uint32_t> random_vector(size_t size, uint32_t prime, std::mt19937_64& gen, bool nonzero) {
+    std::vector<uint32_t> out(size);
+    std::uniform_int_distribution<uint64_t> dis(nonzero ? 1 : 0, static_cast<uint64_t>(prime) - 1);
+    for (size_t i = 0; i < size; ++i) out[i] = static_cast<uint32_t>(static_cast<uint16_t>(dis(gen)));
+    return out;
+}
+
+namespace {
+uint64_t rowmix_bounded(uint64_t& state, uint64_t bound) {
+    if (bound == 0) throw std::runtime_error("rowmix bounded RNG called with zero bound");
+    const uint64_t threshold = (0ULL - bound) % bound;
+    while (true) {
+        const uint64_t v = splitmix64_next(state);
+        if (v >= threshold) return v % bound;
+    }
+}
+uint16_t rowmix_nonzero(uint64_t& state, uint32_t prime) {
+    if (prime <= 1 || prime > 65535) throw std::runtime_error("rowmix prime must be in 2..65535");
+    return static_cast<uint16_t>(1 + rowmix_bounded(state, prime - 1));
+}
+uint64_t rowmix_realized_seed(uint64_t seed, const std::string& op, size_t sector, size_t rows, uint32_t prime) {
+    uint64_t h = kFnvOffset;
+    h = fnv_str(h, kRowmixAlgorithm);
+    h = fnv_str(h, op);
+    h = fnv_u64(h, seed);
+    h = fnv_u64(h, sector);
+    h = fnv_u64(h, rows);
+    h = fnv_u64(h, prime);
+    return seeded_sector_value(h, sector);
+}
+}  // namespace
+
+// generate_rowmix_plan (cuda/cuprym_cyclic.cu:1227-1268).
+RowMixPlan generate_rowmix_plan(size_t target_rows, const std::string& op, size_t sector, uint32_t prime,
+                                size_t rounds, uint64_t seed) {
+    RowMixPlan plan;
+    plan.target_rows = target_rows;
+    plan.rounds = rounds;
+    plan.seed = seed;
+    plan.realized_seed = rowmix_realized_seed(seed, op, sector, target_rows, prime);
+    plan.round_pairs.resize(rounds);
+    if (rounds == 0) return plan;
+    std::vector<uint32_t> perm(target_rows);
+    for (size_t i = 0; i < target_rows; ++i) perm[i] = checked_u32(i, "rowmix target coordinate");
+    uint64_t state = plan.realized_seed;
+    const size_t pairs = target_rows / 2;
+    for (size_t round = 0; round < rounds; ++round) {
+        for (size_t i = target_rows; i > 1; --i) {
+            const size_t j = static_cast<size_t>(rowmix_bounded(state, i));
+            std::swap(perm[i - 1], perm[j]);
+        }
+        auto& out = plan.round_pairs[round];
+        out.reserve(pairs);
+        for (size_t q = 0; q < pairs; ++q) {
+            RowMixPair pr;
+            pr.first = perm[2 * q];
+            pr.second = perm[2 * q + 1];
+            pr.a = rowmix_nonzero(state, prime);
+            pr.b = rowmix_nonzero(state, prime);
+            out.push_back(pr);
+        }
+    }
+    return plan;
+}
+
+uint64_t rowmix_plan_hash(const RowMixPlan& plan) {
+    uint64_t h = kFnvOffset;
+    h = fnv_str(h, kRowmixAlgorithm);
+    h = fnv_u64(h, plan.target_rows);
+    h = fnv_u64(h, plan.rounds);
+    h = fnv_u64(h, plan.seed);
+    h = fnv_u64(h, plan.realized_seed);
+    for (const auto& round : plan.round_pairs) {
+        h = fnv_u64(h, round.size());
+        for (const auto& pr : round) {
+            h = fnv_u64(h, pr.first);
+            h = fnv_u64(h, pr.second);
+            h = fnv_u64(h, pr.a);
+            h = fnv_u64(h, pr.b);
+        }
+    }
+    return h;
+}
+
+uint64_t fnv1a64_vector_hash(const std::vector<uint32_t>& values) {
+    uint64_t h = fnv_u64(kFnvOffset, values.size());
+    for (uint32_t v : values) h = fnv_u64(h, v);
+    return h;
+}
+
+std::string hex_u64(uint64_t v) {
+    std::ostringstream out;
+    out << "0x" << std::hex << std::setw(16) << std::setfill('0') << v;
+    return out.str();
+}
+
+// deterministic_dense_block (cuda/cuprym_cyclic.cu:1413-1424).
+std::vector<uint32_t> deterministic_block(size_t rows, size_t cols, uint32_t prime, uint64_t salt) {
+    std::vector<uint32_t> out(rows * cols);
+    uint64_t state = salt ^ (0xD6E8FEB86659FD93ULL + rows * 1315423911ULL + cols * 2654435761ULL);
+    for (size_t i = 0; i < rows * cols; ++i) out[i] = static_cast<uint32_t>(splitmix64_next(state) % prime);
+    return out;
+}
+
+namespace {
+void rowmix_apply(const RowMixPlan& plan, std::vector<uint32_t>& block, size_t cols, uint32_t prime, bool transpose) {
+    auto one = [&](const std::vector<RowMixPair>& round) {
+        for (const auto& pr : round)
+            for (size_t c = 0; c < cols; ++c) {
+                uint64_t x = block[pr.first * cols + c], y = block[pr.second * cols + c];
+                uint64_t a = pr.a, b = pr.b, oab = 1 + a * b;
+                if (transpose) {
+                    block[pr.first * cols + c] = static_cast<uint32_t>((x + b * y) % prime);
+                    block[pr.second * cols + c] = static_cast<uint32_t>((a * x + oab * y) % prime);
+                } else {
+                    block[pr.first * cols + c] = static_cast<uint32_t>((x + a * y) % prime);
+                    block[pr.second * cols + c] = static_cast<uint32_t>((b * x + oab * y) % prime);
+                }
+            }
+    };
+    if (transpose)
+        for (size_t r = plan.round_pairs.size(); r > 0; --r) one(plan.round_pairs[r - 1]);
+    else
+        for (const auto& round : plan.round_pairs) one(round);
+}
+}  // namespace
+
+uint32_t dot_mod(const std::vector<uint32_t>& a, const std::vector<uint32_t>& b, uint32_t p) {
+    if (a.size() != b.size()) throw std::runtime_error("dense dot input size mismatch");
+    uint64_t s = 0;
+    for (size_t i = 0; i < a.size(); ++i) {
+        s += static_cast<uint64_t>(a[i]) * b[i];
+        if (s > (1ULL << 62)) s %= p;
+    }
+    return static_cast<uint32_t>(s % p);
+}
+
+void validate_rowmix_transpose_identity(const RowMixPlan& plan, size_t cols, uint32_t prime) {
+    std::vector<uint32_t> x = deterministic_block(plan.target_rows, cols, prime, 0xA11CE001ULL);
+    std::vector<uint32_t> y = deterministic_block(plan.target_rows, cols, prime, 0xB0B5EED2ULL);
+    std::vector<uint32_t> tx = x, tty = y;
+    rowmix_apply(plan, tx, cols, prime, false);
+    rowmix_apply(plan, tty, cols, prime, true);
+    const uint32_t left = dot_mod(tx, y, prime), right = dot_mod(x, tty, prime);
+    if (left != right)
+        throw std::runtime_error("rowmix transpose identity failed: <Tx,y>=" + std::to_string(left) +
+                                 ", <x,T^t y>=" + std::to_string(right));
+}
+
+// P = T^t Dr T with T = T_R ... T_1 (the rounds of generate_rowmix_plan).
+Csr composite_target_preconditioner(const RowMixPlan& plan, const std::vector<uint32_t>& dr, uint32_t prime) {
+    const size_t n = plan.target_rows;
+    if (dr.size() != n) throw std::runtime_error("row preconditioner length does not match the rowmix plan");
+    // Sparse rows of T, built round by round: T <- T_k T.
+    std::vector<std::vector<std::pair<uint32_t, uint64_t>>> t(n);
+    for (size_t i = 0; i < n; ++i) t[i] = {{static_cast<uint32_t>(i), 1}};
+    auto combine = [&](const std::vector<std::pair<uint32_t, uint64_t>>& u, uint64_t cu,
+                       const std::vector<std::pair<uint32_t, uint64_t>>& v, uint64_t cv) {
+        std::map<uint32_t, uint64_t> acc;
+        for (auto& e : u) acc[e.first] = (acc[e.first] + cu * e.second) % prime;
+        for (auto& e : v) acc[e.first] = (acc[e.first] + cv * e.second) % prime;
+        std::vector<std::pair<uint32_t, uint64_t>> out;
+        for (auto& e : acc)
+            if (e.second) out.push_back(e);
+        return out;
+    };
+    for (const auto& round : plan.round_pairs) {
+        for (const auto& pr : round) {
+            const uint64_t a = pr.a, b = pr.b, oab = (1 + a * b) % prime;
+            auto f = combine(t[pr.first], 1, t[pr.second], a);
+            auto s = combine(t[pr.first], b, t[pr.second], oab);
+            t[pr.first] = std::move(f);
+            t[pr.second] = std::move(s);
+        }
+    }
+    // P[i][j] = sum_k T[k][i] Dr[k] T[k][j]
+    std::vector<std::map<uint32_t, uint64_t>> rows(n);
+    for (size_t k = 0; k < n; ++k)
+        for (auto& ei : t[k])
+            for (auto& ej : t[k]) {
+                uint64_t v = ei.second * dr[k] % prime * ej.second % prime;
+                auto& slot = rows[ei.first][ej.first];
+                slot = (slot + v) % prime;
+            }
+    Csr out;
+    out.row_ptr.resize(n + 1);
+    for (size_t i = 0; i < n; ++i) {
+        out.row_ptr[i] = checked_u32(out.col.size(), "preconditioner nnz");
+        for (auto& e : rows[i])
+            if (e.second) {
+                out.col.push_back(e.first);
+                out.val.push_back(static_cast<uint32_t>(e.second));
+            }
+    }
+    out.row_ptr[n] = checked_u32(out.col.size(), "preconditioner nnz");
+    return out;
+}
+
+std::string rowmix_label(size_t rounds, uint64_t seed) {
+    std::ostringstream out;
+    out << "rowmix-r" << rounds << "-s" << seed;
+    return out.str();
+}
+
+// sector_filename (cuda/cuprym_cyclic.cu:1295-1312).
+std::string sector_filename(const std::string& out_dir, const std::string& op, size_t sector, size_t num_v,
+                            size_t rowmix_rounds, uint64_t rowmix_seed) {
+    std::filesystem::path dir(out_dir.empty() ? "." : out_dir);
+    std::filesystem::create_directories(dir);
+    std::ostringstream name;
+    name << op << "-sector" << std::setw(2) << std::setfill('0') << sector << "-v" << num_v;
+    if (rowmix_rounds > 0) name << "-rowmix-r" << rowmix_rounds << "-s" << rowmix_seed;
+    name << ".wdm.zst";
+    return (dir / name.str()).string();
+}
+
+std::string rowmix_sidecar_filename(const std::string& wdm) {
+    const std::string suffix = ".wdm.zst";
+    if (wdm.size() >= suffix.size() && wdm.compare(wdm.size() - suffix.size(), suffix.size(), suffix) == 0)
+        return wdm.substr(0, wdm.size() - suffix.size()) + ".rowmix.json";
+    return wdm + ".rowmix.json";
+}
+
+void ensure_output_absent(const std::string& wdm) {
+    if (std::filesystem::exists(wdm)) throw std::runtime_error("refusing to overwrite existing WDM file " + wdm);
+    const std::string side = rowmix_sidecar_filename(wdm);
+    if (std::filesystem::exists(side)) throw std::runtime_error("refusing to reuse existing rowmix sidecar " + side);
+}
+
+// write_rowmix_sidecar (cuda/cuprym_cyclic.cu:1336-1400): the same keys, order and text.
+void write_rowmix_sidecar(const std::string& wdm, const std::string& op, size_t sector, size_t rows, size_t cols,
+                          size_t num_v, uint32_t prime, uint64_t random_seed, const RowMixPlan& plan,
+                          const std::vector<uint32_t>& row_precond, const std::vector<uint32_t>& col_precond,
+                          const std::vector<uint32_t>& initial_block) {
+    const std::string side = rowmix_sidecar_filename(wdm);
+    const std::string tmp = side + ".tmp";
+    std::ofstream out(tmp, std::ios::binary);
+    if (!out) throw std::runtime_error("failed to open rowmix sidecar " + tmp);
+    out << "{\n";
+    out << "  \"type\": \"prym_cyclic_rowmix_sidecar\",\n";
+    out << "  \"version\": 1,\n";
+    out << "  \"algorithm_version\": \"" << kRowmixAlgorithm << "\",\n";
+    out << "  \"wdm_file\": \"" << wdm << "\",\n";
+    out << "  \"operator\": \"" << op << "\",\n";
+    out << "  \"sector\": " << sector << ",\n";
+    out << "  \"rows\": " << rows << ",\n";
+    out << "  \"columns\": " << cols << ",\n";
+    out << "  \"vector_count\": " << num_v << ",\n";
+    out << "  \"prime\": " << prime << ",\n";
+    out << "  \"numerical_seed\": " << random_seed << ",\n";
+    out << "  \"rowmix\": {\n";
+    out << "    \"rounds\": " << plan.rounds << ",\n";
+    out << "    \"seed\": " << plan.seed << ",\n";
+    out << "    \"realized_seed\": " << plan.realized_seed << ",\n";
+    out << "    \"rng\": \"splitmix64-v1\",\n";
+    out << "    \"target_rows\": " << plan.target_rows << ",\n";
+    out << "    \"pair_count_per_round\": [";
+    for (size_t i = 0; i < plan.round_pairs.size(); ++i) out << (i ? ", " : "") << plan.round_pairs[i].size();
+    out << "],\n";
+    out << "    \"recipe\": \"Starting from realized_seed, for each round reset permutation to the previous round's "
+           "final order, run descending Fisher-Yates using splitmix64 rejection-bounded draws, pair consecutive "
+           "coordinates, then draw nonzero a,b in F_p by rejection-bounded draws in 1..p-1.\",\n";
+    out << "    \"hash_fnv1a64\": \"" << hex_u64(rowmix_plan_hash(plan)) << "\"\n";
+    out << "  },\n";
+    out << "  \"hashes\": {\n";
+    out << "    \"row_preconditioner_fnv1a64\": \"" << hex_u64(fnv1a64_vector_hash(row_precond)) << "\",\n";
+    out << "    \"column_preconditioner_fnv1a64\": \"" << hex_u64(fnv1a64_vector_hash(col_precond)) << "\",\n";
+    out << "    \"initial_block_fnv1a64\": \"" << hex_u64(fnv1a64_vector_hash(initial_block)) << "\"\n";
+    out << "  }\n";
+    out << "}\n";
+    out.close();
+    if (!out) throw std::runtime_error("failed to write rowmix sidecar " + tmp);
+    std::filesystem::rename(tmp, side);
+}
+
+// The sector assembly of run_eliminated_sector (cuda/cuprym_cyclic.cu:2155-2176)
+// with the U basis and incidences of main (:2605-2657).
+EliminatedSector assemble_eliminated_sector(const Instance& inst, size_t sector) {
+    if (!inst.has_elimination) throw std::runtime_error("instance does not contain third_section_elimination data");
+    if (sector >= inst.r) throw std::runtime_error("--sector must be in 0.." + std::to_string(inst.r - 1));
+    EliminatedSector es;
+    es.sector = sector;
+    std::vector<size_t> u_idx;
+    std::vector<uint16_t> u_w;
+    for (size_t i = 0; i < inst.n; ++i) {
+        if (i == inst.w_index) continue;
+        u_idx.push_back(i);
+        u_w.push_back(inst.weight_v[i]);
+    }
+    const CharMap a0 = build_char_map(inst.weight_a0, inst.r);
+    const CharMap a1 = build_char_map(inst.weight_a1, inst.r);
+    const CharMap km = build_char_map(inst.kernel_weights, inst.r);
+    es.dm = build_incidences(u_idx.size(), inst.m, inst.r, u_idx, u_w);
+    es.d2 = build_incidences(u_idx.size(), inst.m - 1, inst.r, u_idx, u_w);
+    es.y_sector = sub_mod(sector, inst.w_weight, inst.r);
+    es.dm_layout = build_sector_layout(inst, es.dm, a0, a1, sector);
+    es.d2_layout = build_sector_layout(inst, es.d2, a0, a1, es.y_sector);
+    es.z_layout = build_tensor_layout(es.dm.row_subset_weights, km, inst.r, es.y_sector);
+    es.x_cols = es.dm_layout.col_subset.size();
+    es.t_rows = es.dm_layout.row_subset.size();
+    es.y_rows = es.d2_layout.col_subset.size();
+    es.z_cols = es.z_layout.subset.size();
+    es.target_rows = es.d2_layout.row_subset.size();
+    es.dm_nnz = es.dm_layout.nnz;
+    es.d2_nnz = es.d2_layout.nnz;
+    // validate_eliminated_sector_against_fixture (cuda/cuprym_cyclic.cu:1124-1141)
+    if (!inst.expected_elim_columns.empty() && sector < inst.expected_elim_columns.size() &&
+        inst.expected_elim_columns[sector] != es.total_cols())
+        throw std::runtime_error("eliminated sector column count does not match fixture metadata");
+    if (!inst.expected_elim_rows.empty() && sector < inst.expected_elim_rows.size() &&
+        inst.expected_elim_rows[sector] != es.target_rows)
+        throw std::runtime_error("eliminated sector row count does not match fixture metadata");
+    return es;
+}
+
+}  // namespace cyclic
+}  // namespace bw

@@ -68,7 +68,31 @@ SIGNATURES = {
     "bw_koszul_sequence_host": (_INT, [_VP, _VP, _VP, _U64, _VP, _VP]),
     "bw_koszul_seq_step_timed": (_INT, [_VP, _U64, ctypes.POINTER(ctypes.c_float), _VP]),
     "bw_koszul_launch_count": (_U64, [_VP]),
+    "bw_cyclic_open": (_INT, [ctypes.c_char_p, ctypes.c_char_p, _U32, _U32, _U64, _U32, _U64, _INT,
+                              ctypes.POINTER(_VP)]),
+    "bw_cyclic_info_get": (_INT, [_VP, _VP]),
+    "bw_cyclic_close": (None, [_VP]),
+    "bw_cyclic_apply_host": (_INT, [_VP, _INT, _VP, _VP]),
+    "bw_cyclic_generate": (_INT, [_VP, _U64]),
+    "bw_cyclic_download": (_INT, [_VP, _VP, _U64, _VP]),
+    "bw_cyclic_output_path": (_INT, [_VP, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "bw_cyclic_check_outputs_absent": (_INT, [ctypes.c_char_p]),
+    "bw_cyclic_write_sidecar": (_INT, [_VP, ctypes.c_char_p]),
+    "bw_cyclic_write_wdm": (_INT, [_VP, ctypes.c_char_p]),
+    "bw_cyclic_validate": (_INT, [_VP, _U32]),
+    "bw_cyclic_launch_count": (_U64, [_VP]),
+    "bw_file_read_text": (_INT, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
 }
+
+
+class CyclicInfo(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in (
+        "rows", "cols", "x_cols", "z_cols", "t_rows", "y_rows", "dm_nnz", "d2_nnz", "default_nlen", "seq_len",
+        "rowmix_realized_seed", "rowmix_hash", "device_bytes")] + [
+        (name, ctypes.c_uint32) for name in ("genus", "prime", "order", "sector", "y_sector", "num_v")]
+
+
+APPLY_SQUARE, APPLY_FORWARD, APPLY_TRANSPOSE, APPLY_SQUARE_UNFOLDED = 0, 1, 2, 3
 
 
 def load():
@@ -213,3 +237,85 @@ class KoszulEngine:
     @property
     def launch_count(self):
         return int(load().bw_koszul_launch_count(self._h))
+
+
+def read_text(path):
+    """A text file, decompressed when it carries the zstd magic (the WDM reader's framing)."""
+    lib = load()
+    n = ctypes.c_size_t()
+    _check(lib.bw_file_read_text(str(path).encode(), None, 0, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(max(1, n.value))
+    _check(lib.bw_file_read_text(str(path).encode(), buf, n.value, ctypes.byref(n)))
+    return buf.raw[:n.value].decode()
+
+
+class CyclicEngine:
+    """Eliminated cyclic operator of one sector (paper mode, include/bw_engine.h).
+
+    ``device=-1`` opens a host-only context (assembly, seeded data, row-mixing
+    plan and sidecar; no device calls).
+    """
+
+    def __init__(self, instance, sector, op="eliminated", num_v=4, seed=1, rowmix_rounds=2, rowmix_seed=10001,
+                 device=0):
+        lib = load()
+        handle = ctypes.c_void_p()
+        _check(lib.bw_cyclic_open(str(instance).encode(), op.encode(), sector, num_v, seed, rowmix_rounds,
+                                  rowmix_seed, device, ctypes.byref(handle)))
+        self._h = handle
+        self.refresh()
+
+    def refresh(self):
+        info = CyclicInfo()
+        _check(load().bw_cyclic_info_get(self._h, ctypes.byref(info)))
+        self.info = {name: getattr(info, name) for name, _ in CyclicInfo._fields_}
+        return self.info
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().bw_cyclic_close(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def apply(self, what, block):
+        block = np.ascontiguousarray(block, dtype=np.uint32)
+        rows = self.info["rows"] if what == APPLY_FORWARD else self.info["cols"]
+        out = np.empty((rows, 4), dtype=np.uint32)
+        _check(load().bw_cyclic_apply_host(self._h, what, _host_ptr(block), _host_ptr(out)))
+        return out
+
+    def generate(self, nlen=0):
+        _check(load().bw_cyclic_generate(self._h, nlen))
+        return self.refresh()["seq_len"]
+
+    def download(self):
+        n = self.info["seq_len"]
+        seq = np.empty((n, 10), dtype=np.uint32)
+        cur = np.empty((self.info["cols"], 4), dtype=np.uint32)
+        _check(load().bw_cyclic_download(self._h, _host_ptr(seq), n, _host_ptr(cur)))
+        return seq, cur
+
+    def output_path(self, out_dir):
+        buf = ctypes.create_string_buffer(4096)
+        _check(load().bw_cyclic_output_path(self._h, str(out_dir).encode(), buf, 4096))
+        return buf.value.decode()
+
+    def write_sidecar(self, wdm_path):
+        _check(load().bw_cyclic_write_sidecar(self._h, str(wdm_path).encode()))
+
+    def write_wdm(self, wdm_path):
+        _check(load().bw_cyclic_write_wdm(self._h, str(wdm_path).encode()))
+
+    def validate(self, columns=4):
+        _check(load().bw_cyclic_validate(self._h, columns))
+
+    @property
+    def launch_count(self):
+        return int(load().bw_cyclic_launch_count(self._h))

@@ -126,11 +126,13 @@ def _check_sampled_rows(shape, maps, diag, y, out, count, seed):
 
 
 def _projection(x, w, p):
-    # exact int64 X^T W on the GPU (|products| < 2^30, at most 2^21 rows per chunk)
-    acc = torch.zeros((x.shape[1], w.shape[1]), dtype=torch.int64, device=x.device)
-    for s in range(0, x.shape[0], 1 << 20):
-        acc += (x[s:s + (1 << 20)].to(torch.int64).T @ w[s:s + (1 << 20)].to(torch.int64)) % p
-    return (acc % p).cpu().numpy().astype(np.uint32)
+    # exact int64 X^T W on the host (products < 2^30, 2^20 rows per chunk < 2^50)
+    xn = x.cpu().numpy().astype(np.int64)
+    wn = w.cpu().numpy().astype(np.int64)
+    acc = np.zeros((xn.shape[1], wn.shape[1]), dtype=np.int64)
+    for s in range(0, xn.shape[0], 1 << 20):
+        acc = (acc + xn[s:s + (1 << 20)].T @ wn[s:s + (1 << 20)]) % p
+    return acc.astype(np.uint32)
 
 
 @pytest.mark.parametrize("form", FORMS)
