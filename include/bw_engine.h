@@ -204,6 +204,21 @@ BW_API int bw_cyclic_validate(bw_cyclic* ctx, uint32_t columns);
 
 BW_API uint64_t bw_cyclic_launch_count(const bw_cyclic* ctx);
 
+/* Block projection d_out = X^T W (m x n canonical residues; X is rows x m and
+ * W rows x n, canonical, device, W 16-byte aligned) that allocates nothing:
+ * the cross-CTA scratch is a fixed 1 MiB + 256 B array inside the library.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * a framework whose allocator owns all device memory, or code that must not
+ * trigger the device-wide synchronisation of cudaMalloc / cudaFree.
+ * Limits: m, n in {4, 8, 16, 32}; odd prime below 2^15; rows below 2^40;
+ * larger sizes are rejected with status 1.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) and should come before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race and give wrong results; each call clears the arrival counter it
+ * needs at zero. */
+BW_API int bw_project_noalloc(const uint32_t* d_x, const uint32_t* d_w, uint64_t rows, uint32_t m, uint32_t n,
+                              uint32_t prime, uint32_t* d_out, int device, void* stream);
+
 /* Reads a text file, decompressing it when it carries the zstd magic
  * (cuda/zstd_compat.h:67-77).  With buf == NULL only *len is set. */
 BW_API int bw_file_read_text(const char* path, char* buf, size_t cap, size_t* len);

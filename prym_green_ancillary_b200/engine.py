@@ -82,6 +82,7 @@ SIGNATURES = {
     "bw_cyclic_validate": (_INT, [_VP, _U32]),
     "bw_cyclic_launch_count": (_U64, [_VP]),
     "bw_file_read_text": (_INT, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "bw_project_noalloc": (_INT, [_VP, _VP, _U64, _U32, _U32, _U32, _VP, _INT, _VP]),
 }
 
 
