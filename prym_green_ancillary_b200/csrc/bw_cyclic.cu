@@ -33,7 +33,28 @@ __device__ __forceinline__ int32_t red64(long long x, const Mod& m) {
     return static_cast<int32_t>(r);
 }
 
-struct Acc4 {
+// Four-column accumulator.  SMALL: int32 sums, exact because the host checked
+// that (terms per output) * ((p-1)/2)^2 + 2p < 2^31 for every kernel of this
+// sector (always true at the paper primes); otherwise int64 sums.
+template <bool SMALL>
+struct Acc4;
+
+template <>
+struct Acc4<true> {
+    int32_t x = 0, y = 0, z = 0, w = 0;
+    __device__ __forceinline__ void mac(int32_t c, const int4& v) {
+        x += c * v.x;
+        y += c * v.y;
+        z += c * v.z;
+        w += c * v.w;
+    }
+    __device__ __forceinline__ int4 reduce(const Mod& m) const {
+        return make_int4(reduce_balanced(x, m), reduce_balanced(y, m), reduce_balanced(z, m), reduce_balanced(w, m));
+    }
+};
+
+template <>
+struct Acc4<false> {
     long long x = 0, y = 0, z = 0, w = 0;
     __device__ __forceinline__ void mac(int32_t c, const int4& v) {
         x += static_cast<long long>(c) * v.x;
@@ -56,6 +77,7 @@ __device__ __forceinline__ int4 scale4(const int4& v, int32_t s, const Mod& m) {
     return make_int4(reduce_balanced(v.x * s, m), reduce_balanced(v.y * s, m), reduce_balanced(v.z * s, m),
                      reduce_balanced(v.w * s, m));
 }
+__device__ __forceinline__ int4 neg4(const int4& v) { return make_int4(-v.x, -v.y, -v.z, -v.w); }
 
 __device__ __forceinline__ void decode_inc(uint32_t e, uint32_t& sub, int& i, bool& neg) {
     sub = e & 0x3FFFFFFu;
@@ -67,175 +89,177 @@ __device__ __forceinline__ void decode_coef(int32_t e, int& local, int32_t& coef
     coef = static_cast<int16_t>(e & 0xFFFF);
 }
 
+#define BW_ROWS(var, count)                                                                     \
+    for (long long var = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; var < (count); \
+         var += static_cast<long long>(gridDim.x) * blockDim.x)
+
 // out[row] = dc[row] * in[row]  (dc == nullptr: copy)
 __global__ void cyc_scale_kernel(const int32_t* __restrict__ in, const int32_t* __restrict__ dc,
                                  int32_t* __restrict__ out, long long rows, Mod mod) {
-    for (long long row = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; row < rows;
-         row += static_cast<long long>(gridDim.x) * blockDim.x) {
+    BW_ROWS(row, rows) {
         int4 v = ld4(in, row);
         st4(out, row, dc ? scale4(v, __ldg(dc + row), mod) : v);
     }
 }
 
-// t(S, beta) = sum_{i not in S} +-sum_a mu[i,beta,a] xs[(S u i, a)]   (D_m forward row)
-__device__ __forceinline__ int4 dm_row(const ElimDev& E, const int32_t* __restrict__ xs, uint32_t S, int beta) {
-    Acc4 acc;
-    const uint32_t* inc = E.dm_row_inc + static_cast<size_t>(S) * E.dm_row_width;
-    for (uint32_t pos = 0; pos < E.dm_row_width; ++pos) {
+// Koszul forward row of D on a block `in` whose column blocks start at col_off:
+//   sum_{i not in S} +-sum_a mu[i,beta,a] in[(S u i, a)]
+template <bool SMALL>
+__device__ __forceinline__ int4 koszul_row(const ElimDev& E, const uint32_t* __restrict__ inc, uint32_t width,
+                                           const uint32_t* __restrict__ col_off, const int32_t* __restrict__ in,
+                                           int beta) {
+    Acc4<SMALL> acc;
+    for (uint32_t pos = 0; pos < width; ++pos) {
         uint32_t cs;
         int i;
         bool neg;
         decode_inc(__ldg(inc + pos), cs, i, neg);
-        const uint32_t base = __ldg(E.x_off + cs);
+        const uint32_t base = __ldg(col_off + cs);
         const int li = i * E.n + beta;
-        for (uint32_t k = __ldg(E.fl_off + li); k < __ldg(E.fl_off + li + 1); ++k) {
+        const uint32_t k1 = __ldg(E.fl_off + li + 1);
+        for (uint32_t k = __ldg(E.fl_off + li); k < k1; ++k) {
             int la;
             int32_t c;
             decode_coef(__ldg(E.fl + k), la, c);
-            acc.mac(neg ? -c : c, ld4(xs, base + la));
+            acc.mac(neg ? -c : c, ld4(in, base + la));
         }
     }
     return acc.reduce(E.mod);
 }
 
+// Koszul transpose column of D on a block `in` whose row blocks start at row_off:
+//   sum_{j in S} +-sum_beta mu[j,beta,a] in[(S \ j, beta)]
+template <bool SMALL>
+__device__ __forceinline__ int4 koszul_col(const ElimDev& E, const uint32_t* __restrict__ inc, uint32_t width,
+                                           const uint32_t* __restrict__ row_off, const int32_t* __restrict__ in,
+                                           int a) {
+    Acc4<SMALL> acc;
+    for (uint32_t pos = 0; pos < width; ++pos) {
+        uint32_t rs;
+        int j;
+        bool neg;
+        decode_inc(__ldg(inc + pos), rs, j, neg);
+        const uint32_t base = __ldg(row_off + rs);
+        const int lj = j * E.g + a;
+        const uint32_t k1 = __ldg(E.tl_off + lj + 1);
+        for (uint32_t k = __ldg(E.tl_off + lj); k < k1; ++k) {
+            int lb;
+            int32_t c;
+            decode_coef(__ldg(E.tl + k), lb, c);
+            acc.mac(neg ? -c : c, ld4(in, base + lb));
+        }
+    }
+    return acc.reduce(E.mod);
+}
+
+// t = D_m xs  (rows (S, beta) over (m-1)-subsets)
+template <bool SMALL>
+__global__ void cyc_dm_forward_kernel(ElimDev E, const int32_t* __restrict__ xs, int32_t* __restrict__ t) {
+    BW_ROWS(tr, E.t_rows) {
+        const uint32_t S = __ldg(E.t_sub + tr);
+        st4(t, tr, koszul_row<SMALL>(E, E.dm_row_inc + static_cast<size_t>(S) * E.dm_row_width, E.dm_row_width,
+                                     E.x_off, xs, __ldg(E.t_beta + tr)));
+    }
+}
+
 // y(S, a) = sum_kappa B[a,kappa] zs(S,kappa) - sum_beta R[a,beta] t(S,beta)
-__global__ void cyc_elim_forward_kernel(ElimDev E, const int32_t* __restrict__ xs, int32_t* __restrict__ y) {
-    for (long long yr = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; yr < E.y_rows;
-         yr += static_cast<long long>(gridDim.x) * blockDim.x) {
+template <bool SMALL>
+__global__ void cyc_elim_y_kernel(ElimDev E, const int32_t* __restrict__ xs, const int32_t* __restrict__ t,
+                                  int32_t* __restrict__ y) {
+    BW_ROWS(yr, E.y_rows) {
         const uint32_t S = __ldg(E.y_sub + yr);
         const int a = __ldg(E.y_a + yr);
-        Acc4 acc;
-        for (uint32_t zr = __ldg(E.z_off + S); zr < __ldg(E.z_off + S + 1); ++zr) {
+        Acc4<SMALL> acc;
+        const uint32_t z1 = __ldg(E.z_off + S + 1);
+        for (uint32_t zr = __ldg(E.z_off + S); zr < z1; ++zr) {
             const int32_t c = __ldg(E.Bk + a * E.kdim + __ldg(E.z_k + zr));
             if (c) acc.mac(c, ld4(xs, static_cast<long long>(E.x_cols) + zr));
         }
-        for (uint32_t tr = __ldg(E.t_off + S); tr < __ldg(E.t_off + S + 1); ++tr) {
-            const int beta = __ldg(E.t_beta + tr);
-            const int32_t c = __ldg(E.R + a * E.n + beta);
-            if (!c) continue;
-            acc.mac(-c, dm_row(E, xs, S, beta));
+        const uint32_t t1 = __ldg(E.t_off + S + 1);
+        for (uint32_t tr = __ldg(E.t_off + S); tr < t1; ++tr) {
+            const int32_t c = __ldg(E.R + a * E.n + __ldg(E.t_beta + tr));
+            if (c) acc.mac(-c, ld4(t, tr));
         }
         st4(y, yr, acc.reduce(E.mod));
     }
 }
 
-// u(T2, beta) = sum_{i not in T2} +-sum_a mu[i,beta,a] y(T2 u i, a)   (D_(m-1) forward)
+// u = D_(m-1) y  (rows (S2, beta) over (m-2)-subsets)
+template <bool SMALL>
 __global__ void cyc_d2_forward_kernel(ElimDev E, const int32_t* __restrict__ y, int32_t* __restrict__ u) {
-    for (long long ur = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; ur < E.n_r;
-         ur += static_cast<long long>(gridDim.x) * blockDim.x) {
+    BW_ROWS(ur, E.n_r) {
         const uint32_t S2 = __ldg(E.u_sub + ur);
-        const int beta = __ldg(E.u_beta + ur);
-        Acc4 acc;
-        const uint32_t* inc = E.d2_row_inc + static_cast<size_t>(S2) * E.d2_row_width;
-        for (uint32_t pos = 0; pos < E.d2_row_width; ++pos) {
-            uint32_t cs;
-            int i;
-            bool neg;
-            decode_inc(__ldg(inc + pos), cs, i, neg);
-            const uint32_t base = __ldg(E.y_off + cs);
-            const int li = i * E.n + beta;
-            for (uint32_t k = __ldg(E.fl_off + li); k < __ldg(E.fl_off + li + 1); ++k) {
-                int la;
-                int32_t c;
-                decode_coef(__ldg(E.fl + k), la, c);
-                acc.mac(neg ? -c : c, ld4(y, base + la));
-            }
-        }
-        st4(u, ur, acc.reduce(E.mod));
+        st4(u, ur, koszul_row<SMALL>(E, E.d2_row_inc + static_cast<size_t>(S2) * E.d2_row_width, E.d2_row_width,
+                                     E.y_off, y, __ldg(E.u_beta + ur)));
     }
 }
 
 // out = P u  (P = T^t Dr T in CSR)
+template <bool SMALL>
 __global__ void cyc_spmv_kernel(const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
                                 const int32_t* __restrict__ val, const int32_t* __restrict__ u,
                                 int32_t* __restrict__ out, long long rows, Mod mod) {
-    for (long long row = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; row < rows;
-         row += static_cast<long long>(gridDim.x) * blockDim.x) {
-        Acc4 acc;
-        for (uint32_t e = __ldg(ptr + row); e < __ldg(ptr + row + 1); ++e) acc.mac(__ldg(val + e), ld4(u, __ldg(col + e)));
+    BW_ROWS(row, rows) {
+        Acc4<SMALL> acc;
+        const uint32_t e1 = __ldg(ptr + row + 1);
+        for (uint32_t e = __ldg(ptr + row); e < e1; ++e) acc.mac(__ldg(val + e), ld4(u, __ldg(col + e)));
         st4(out, row, acc.reduce(mod));
     }
 }
 
-// h(S, a) = sum_{j in S} +-sum_beta mu[j,beta,a] u2(S \ j, beta)   (D_(m-1) transpose)
+// h = D_(m-1)^t u2  (rows (S, a) over (m-1)-subsets)
+template <bool SMALL>
 __global__ void cyc_d2_transpose_kernel(ElimDev E, const int32_t* __restrict__ u2, int32_t* __restrict__ h) {
-    for (long long yr = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; yr < E.y_rows;
-         yr += static_cast<long long>(gridDim.x) * blockDim.x) {
+    BW_ROWS(yr, E.y_rows) {
         const uint32_t S = __ldg(E.y_sub + yr);
-        const int a = __ldg(E.y_a + yr);
-        Acc4 acc;
-        const uint32_t* inc = E.d2_col_inc + static_cast<size_t>(S) * E.d2_col_width;
-        for (uint32_t pos = 0; pos < E.d2_col_width; ++pos) {
-            uint32_t rs;
-            int j;
-            bool neg;
-            decode_inc(__ldg(inc + pos), rs, j, neg);
-            const uint32_t base = __ldg(E.u_off + rs);
-            const int lj = j * E.g + a;
-            for (uint32_t k = __ldg(E.tl_off + lj); k < __ldg(E.tl_off + lj + 1); ++k) {
-                int lb;
-                int32_t c;
-                decode_coef(__ldg(E.tl + k), lb, c);
-                acc.mac(neg ? -c : c, ld4(u2, base + lb));
-            }
-        }
-        st4(h, yr, acc.reduce(E.mod));
+        st4(h, yr, koszul_col<SMALL>(E, E.d2_col_inc + static_cast<size_t>(S) * E.d2_col_width, E.d2_col_width,
+                                     E.u_off, u2, __ldg(E.y_a + yr)));
     }
 }
 
-// t_adj(T, beta) = sum_{a} R[a,beta] h(T, a)
-__device__ __forceinline__ int4 rt_h(const ElimDev& E, const int32_t* __restrict__ h, uint32_t T, int beta) {
-    Acc4 acc;
-    for (uint32_t yr = __ldg(E.y_off + T); yr < __ldg(E.y_off + T + 1); ++yr) {
-        const int32_t c = __ldg(E.R + __ldg(E.y_a + yr) * E.n + beta);
-        if (c) acc.mac(c, ld4(h, yr));
-    }
-    return acc.reduce(E.mod);
-}
-
-// out = Dc [ -D_m^t R^t h ; B^t h ]
-__global__ void cyc_elim_backward_kernel(ElimDev E, const int32_t* __restrict__ h, const int32_t* __restrict__ dc,
-                                         int32_t* __restrict__ out) {
-    const long long total = static_cast<long long>(E.x_cols) + E.z_cols;
-    for (long long row = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; row < total;
-         row += static_cast<long long>(gridDim.x) * blockDim.x) {
-        Acc4 acc;
-        if (row < E.x_cols) {
-            const uint32_t S = __ldg(E.x_sub + row);
-            const int a = __ldg(E.x_a + row);
-            const uint32_t* inc = E.dm_col_inc + static_cast<size_t>(S) * E.dm_col_width;
-            for (uint32_t pos = 0; pos < E.dm_col_width; ++pos) {
-                uint32_t T;
-                int j;
-                bool neg;
-                decode_inc(__ldg(inc + pos), T, j, neg);
-                const uint32_t base = __ldg(E.t_off + T);
-                const int lj = j * E.g + a;
-                for (uint32_t k = __ldg(E.tl_off + lj); k < __ldg(E.tl_off + lj + 1); ++k) {
-                    int lb;
-                    int32_t c;
-                    decode_coef(__ldg(E.tl + k), lb, c);
-                    const int beta = __ldg(E.t_beta + base + lb);
-                    // assembled adjoint negates the x part
-                    acc.mac(neg ? c : -c, rt_h(E, h, T, beta));
-                }
+// rows [0, t_rows):            t_adj(S, beta) = sum_a R[a,beta] h(S, a)
+// rows [t_rows, t_rows+z_cols): out_z(S, kappa) = dc * sum_a B[a,kappa] h(S, a)
+template <bool SMALL>
+__global__ void cyc_adjoint_t_z_kernel(ElimDev E, const int32_t* __restrict__ h, const int32_t* __restrict__ dc,
+                                       int32_t* __restrict__ t_adj, int32_t* __restrict__ out) {
+    BW_ROWS(row, static_cast<long long>(E.t_rows) + E.z_cols) {
+        Acc4<SMALL> acc;
+        if (row < E.t_rows) {
+            const uint32_t S = __ldg(E.t_sub + row);
+            const int beta = __ldg(E.t_beta + row);
+            const uint32_t y1 = __ldg(E.y_off + S + 1);
+            for (uint32_t yr = __ldg(E.y_off + S); yr < y1; ++yr) {
+                const int32_t c = __ldg(E.R + __ldg(E.y_a + yr) * E.n + beta);
+                if (c) acc.mac(c, ld4(h, yr));
             }
+            st4(t_adj, row, acc.reduce(E.mod));
         } else {
-            const long long zr = row - E.x_cols;
+            const long long zr = row - E.t_rows;
             const uint32_t S = __ldg(E.z_sub + zr);
             const int kap = __ldg(E.z_k + zr);
-            for (uint32_t yr = __ldg(E.y_off + S); yr < __ldg(E.y_off + S + 1); ++yr) {
+            const uint32_t y1 = __ldg(E.y_off + S + 1);
+            for (uint32_t yr = __ldg(E.y_off + S); yr < y1; ++yr) {
                 const int32_t c = __ldg(E.Bk + __ldg(E.y_a + yr) * E.kdim + kap);
                 if (c) acc.mac(c, ld4(h, yr));
             }
+            const long long orow = static_cast<long long>(E.x_cols) + zr;
+            const int4 v = acc.reduce(E.mod);
+            st4(out, orow, dc ? scale4(v, __ldg(dc + orow), E.mod) : v);
         }
-        int4 v = acc.reduce(E.mod);
-        st4(out, row, dc ? scale4(v, __ldg(dc + row), E.mod) : v);
     }
 }
 
-// F^t alone (no preconditioners): out = [ -D_m^t R^t h ; B^t h ] with h = D_(m-1)^t in.
-// (cyc_d2_transpose_kernel followed by cyc_elim_backward_kernel with dc = nullptr.)
+// out_x(S', a) = -dc * (D_m^t t_adj)(S', a)
+template <bool SMALL>
+__global__ void cyc_dm_transpose_kernel(ElimDev E, const int32_t* __restrict__ t_adj, const int32_t* __restrict__ dc,
+                                        int32_t* __restrict__ out) {
+    BW_ROWS(xr, E.x_cols) {
+        const uint32_t S = __ldg(E.x_sub + xr);
+        const int4 v = neg4(koszul_col<SMALL>(E, E.dm_col_inc + static_cast<size_t>(S) * E.dm_col_width,
+                                              E.dm_col_width, E.t_off, t_adj, __ldg(E.x_a + xr)));
+        st4(out, xr, dc ? scale4(v, __ldg(dc + xr), E.mod) : v);
+    }
+}
 
 // One paired-SL2 round on the target block (validation path).
 __global__ void cyc_rowmix_kernel(const uint32_t* __restrict__ pairs, long long count, int32_t* __restrict__ block,
@@ -483,6 +507,22 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
         }
     tl_off[inst.n * inst.genus] = static_cast<uint32_t>(tl.size());
 
+    // Most products any kernel sums into one output (the reference's
+    // eliminated_accumulation_terms, cuda/cuprym_cyclic.cu:1080-1121, extended
+    // to the folded target preconditioner); int32 sums are exact when
+    // terms * ((p-1)/2)^2 + 2p < 2^31.
+    {
+        const cyclic::CharMap km = cyclic::build_char_map(inst.kernel_weights, inst.r);
+        const uint64_t ma0 = a0.max_block(), ma1 = a1.max_block(), mk = km.max_block();
+        uint64_t spmv = 0;
+        for (size_t i = 0; i + 1 < c->precond.row_ptr.size(); ++i)
+            spmv = std::max<uint64_t>(spmv, c->precond.row_ptr[i + 1] - c->precond.row_ptr[i]);
+        c->max_terms = std::max({es.dm.row_width * ma0, es.d2.row_width * ma0, mk + ma1, spmv,
+                                 es.d2.column_width * ma1, ma0, es.dm.column_width * ma1, uint64_t{1}});
+        const uint64_t half = (c->p - 1) / 2;
+        c->small = c->max_terms * half * half + 2ull * c->p < (1ull << 31);
+    }
+
     ElimDev& E = c->E;
     E.mod = c->mod;
     E.n = static_cast<int>(inst.n);
@@ -499,6 +539,7 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
     E.d2_col_width = static_cast<uint32_t>(es.d2.column_width);
     E.t_off = c->upload(es.dm_layout.row_offsets);
     E.t_beta = c->upload(es.dm_layout.row_beta);
+    E.t_sub = c->upload(es.dm_layout.row_subset);
     E.x_off = c->upload(es.dm_layout.col_offsets);
     E.x_sub = c->upload(es.dm_layout.col_subset);
     E.x_a = c->upload(es.dm_layout.col_a);
@@ -531,6 +572,7 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
     c->d_d = c->alloc<int32_t>(nc * v);
     c->d_xs = c->alloc<int32_t>(nc * v);
     c->d_y = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
+    c->d_t = c->alloc<int32_t>(std::max<size_t>(es.t_rows, 1) * v);
     c->d_h = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
     c->d_u = c->alloc<int32_t>(std::max<size_t>(es.target_rows, 1) * v);
     c->d_u2 = c->alloc<int32_t>(std::max<size_t>(es.target_rows, 1) * v);
@@ -565,25 +607,42 @@ void CyclicCtx::forward(const int32_t* in, int32_t* u, bool precondition) {
     cyc_scale_kernel<<<grid_for(nc), kThreads, 0, stream>>>(in, precondition ? d_dc : nullptr, d_xs,
                                                             static_cast<long long>(nc), mod);
     BW_CHECK_LAUNCH();
-    cyc_elim_forward_kernel<<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, d_xs, d_y);
+    if (small) {
+        cyc_dm_forward_kernel<true><<<grid_for(es.t_rows), kThreads, 0, stream>>>(E, d_xs, d_t);
+        cyc_elim_y_kernel<true><<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, d_xs, d_t, d_y);
+        cyc_d2_forward_kernel<true><<<grid_for(es.target_rows), kThreads, 0, stream>>>(E, d_y, u);
+    } else {
+        cyc_dm_forward_kernel<false><<<grid_for(es.t_rows), kThreads, 0, stream>>>(E, d_xs, d_t);
+        cyc_elim_y_kernel<false><<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, d_xs, d_t, d_y);
+        cyc_d2_forward_kernel<false><<<grid_for(es.target_rows), kThreads, 0, stream>>>(E, d_y, u);
+    }
     BW_CHECK_LAUNCH();
-    cyc_d2_forward_kernel<<<grid_for(es.target_rows), kThreads, 0, stream>>>(E, d_y, u);
+    launches += 4;
+}
+
+void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
+    const int32_t* dc = precondition ? d_dc : nullptr;
+    const size_t tz = es.t_rows + es.z_cols;
+    if (small) {
+        cyc_d2_transpose_kernel<true><<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, u2, d_h);
+        cyc_adjoint_t_z_kernel<true><<<grid_for(tz), kThreads, 0, stream>>>(E, d_h, dc, d_t, out);
+        cyc_dm_transpose_kernel<true><<<grid_for(es.x_cols), kThreads, 0, stream>>>(E, d_t, dc, out);
+    } else {
+        cyc_d2_transpose_kernel<false><<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, u2, d_h);
+        cyc_adjoint_t_z_kernel<false><<<grid_for(tz), kThreads, 0, stream>>>(E, d_h, dc, d_t, out);
+        cyc_dm_transpose_kernel<false><<<grid_for(es.x_cols), kThreads, 0, stream>>>(E, d_t, dc, out);
+    }
     BW_CHECK_LAUNCH();
     launches += 3;
 }
 
-void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
-    cyc_d2_transpose_kernel<<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, u2, d_h);
-    BW_CHECK_LAUNCH();
-    cyc_elim_backward_kernel<<<grid_for(es.total_cols()), kThreads, 0, stream>>>(E, d_h, precondition ? d_dc : nullptr,
-                                                                                 out);
-    BW_CHECK_LAUNCH();
-    launches += 2;
-}
-
 void CyclicCtx::target_precondition(const int32_t* u, int32_t* u2) {
-    cyc_spmv_kernel<<<grid_for(es.target_rows), kThreads, 0, stream>>>(d_p_ptr, d_p_col, d_p_val, u, u2,
-                                                                       static_cast<long long>(es.target_rows), mod);
+    if (small)
+        cyc_spmv_kernel<true><<<grid_for(es.target_rows), kThreads, 0, stream>>>(
+            d_p_ptr, d_p_col, d_p_val, u, u2, static_cast<long long>(es.target_rows), mod);
+    else
+        cyc_spmv_kernel<false><<<grid_for(es.target_rows), kThreads, 0, stream>>>(
+            d_p_ptr, d_p_col, d_p_val, u, u2, static_cast<long long>(es.target_rows), mod);
     BW_CHECK_LAUNCH();
     ++launches;
 }

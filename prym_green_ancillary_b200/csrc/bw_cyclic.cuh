@@ -18,7 +18,7 @@ struct ElimDev {
     uint64_t x_cols, z_cols, t_rows, y_rows, n_r;
     uint32_t dm_row_width, dm_col_width, d2_row_width, d2_col_width;
     // D_m: rows t = (S, beta) over (m-1)-subsets, columns x = (S', a) over m-subsets
-    const uint32_t *t_off, *x_off, *x_sub;
+    const uint32_t *t_off, *t_sub, *x_off, *x_sub;
     const uint16_t *t_beta, *x_a;
     const uint32_t *dm_row_inc, *dm_col_inc;   // packed: subset | i << 26 | negative << 31
     // D_(m-1): columns y = (S, a) over (m-1)-subsets, rows u = (S2, beta) over (m-2)-subsets
@@ -56,7 +56,9 @@ struct CyclicCtx {
     uint32_t *d_p_ptr = nullptr, *d_p_col = nullptr;
     int32_t* d_p_val = nullptr;
     int32_t *d_b = nullptr, *d_d = nullptr, *d_xs = nullptr, *d_y = nullptr, *d_h = nullptr, *d_u = nullptr,
-            *d_u2 = nullptr;
+            *d_u2 = nullptr, *d_t = nullptr;
+    bool small = false;          // int32 accumulation is exact for this sector
+    uint64_t max_terms = 0;      // most products summed into one output by any kernel
     uint32_t* d_canon = nullptr;
     unsigned gram_grid = 1;
     int32_t* d_partials = nullptr;
