@@ -325,6 +325,10 @@ void KoszulCtx::transpose(const int32_t* z, int32_t* w, bool scale, cudaStream_t
 
 // One step: cur -> other, append a_i.
 void KoszulCtx::step_once(cudaStream_t st) {
+    if (form == BW_FORM_INT8) {
+        i8_step_once(st);
+        return;
+    }
     int32_t* src = cur_is_a ? d_ya : d_yb;
     int32_t* dst = cur_is_a ? d_yb : d_ya;
     forward(src, d_z, st);
@@ -471,11 +475,12 @@ KoszulCtx* KoszulCtx::create(const bw_koszul_desc& d, int dev) {
         BW_CUDA(cudaStreamSynchronize(st));
         c->release(tmp);
     }
-    // A zero on the diagonal is allowed by the algebra but not by the recipe.
-    c->d_ya = c->alloc<int32_t>(c->n_src * c->nb);
-    c->d_yb = c->alloc<int32_t>(c->n_src * c->nb);
-    c->d_z = c->alloc<int32_t>(c->n_tgt * c->nb);
-    c->d_xb = c->alloc<int32_t>(c->n_src * c->m);
+    if (c->form == BW_FORM_PLAIN) {   // the INT8 form keeps its state as limb planes
+        c->d_ya = c->alloc<int32_t>(c->n_src * c->nb);
+        c->d_yb = c->alloc<int32_t>(c->n_src * c->nb);
+        c->d_z = c->alloc<int32_t>(c->n_tgt * c->nb);
+        c->d_xb = c->alloc<int32_t>(c->n_src * c->m);
+    }
     c->proj_grid = static_cast<unsigned>(std::min<uint64_t>(static_cast<uint64_t>(c->sms) * 4,
                                                             std::max<uint64_t>(1, (c->n_src + 255) / 256)));
     const uint64_t scratch_before = c->device_bytes;
@@ -489,6 +494,11 @@ KoszulCtx* KoszulCtx::create(const bw_koszul_desc& d, int dev) {
     BW_CUDA(cudaStreamSynchronize(st));
     return c.release();
 }
+
+template int8_t* KoszulCtx::alloc<int8_t>(uint64_t);
+template int16_t* KoszulCtx::alloc<int16_t>(uint64_t);
+template int* KoszulCtx::alloc<int>(uint64_t);
+template uint32_t* KoszulCtx::alloc<uint32_t>(uint64_t);
 
 void KoszulCtx::release(void* p) {
     auto it = std::find(allocations.begin(), allocations.end(), p);
@@ -506,12 +516,18 @@ void KoszulCtx::seq_start(const uint32_t* x, const uint32_t* y0, uint32_t* seq, 
     BW_REQUIRE(capacity >= 1, "seq_start: sequence capacity must be at least 1");
     d_seq = seq;
     seq_capacity = capacity;
-    launch_to_balanced(x, d_xb, n_src * m, st);
-    launch_to_balanced(y0, d_ya, n_src * nb, st);
     cur_is_a = true;
     BW_CUDA(cudaMemsetAsync(d_seq_index, 0, sizeof(unsigned long long), st));
     BW_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), st));
-    project(d_ya, st);
+    if (form == BW_FORM_INT8) {
+        i8_load_x(x, st);
+        i8_to_limbs(y0, i8_plane(0), i8_plane(1), n_src * nb, st);
+        i8_project(i8_plane(0), i8_plane(1), st);
+    } else {
+        launch_to_balanced(x, d_xb, n_src * m, st);
+        launch_to_balanced(y0, d_ya, n_src * nb, st);
+        project(d_ya, st);
+    }
     seq_len = 1;
     // Graphs capture device pointers; a new session may bring a new d_seq.
     for (auto& g : graphs)
@@ -566,9 +582,15 @@ uint64_t KoszulCtx::kernels_per_step() const { return form == BW_FORM_INT8 ? i8_
 
 void KoszulCtx::seq_finish(uint32_t* y_out, uint64_t* nlen_out, cudaStream_t st) {
     BW_REQUIRE(in_session, "seq_finish: no sequence session");
-    if (y_out) launch_to_canonical(cur_is_a ? d_ya : d_yb, y_out, n_src * nb, st);
-    if (nlen_out) *nlen_out = seq_len;
     in_session = false;
+    if (form == BW_FORM_INT8) {
+        if (y_out) i8_from_limbs(i8_plane(cur_is_a ? 0 : 2), i8_plane(cur_is_a ? 1 : 3), y_out, n_src * nb, st);
+        BW_CUDA(cudaStreamSynchronize(st));
+        i8_check_error();
+    } else if (y_out) {
+        launch_to_canonical(cur_is_a ? d_ya : d_yb, y_out, n_src * nb, st);
+    }
+    if (nlen_out) *nlen_out = seq_len;
 }
 
 }  // namespace bw
@@ -620,6 +642,14 @@ extern "C" int bw_koszul_forward(bw_koszul* ctx, const uint32_t* d_y, uint32_t* 
         BW_REQUIRE(!c.in_session, "bw_koszul_forward: a sequence session is open");
         BW_CUDA(cudaSetDevice(c.device));
         cudaStream_t st = pick_stream(&c, stream);
+        if (c.form == BW_FORM_INT8) {
+            c.i8_to_limbs(d_y, c.i8_plane(0), c.i8_plane(1), c.n_src * c.nb, st);
+            c.i8_run(true, c.i8_plane(0), c.i8_plane(1), c.i8_plane(4), c.i8_plane(5), false, st);
+            c.i8_from_limbs(c.i8_plane(4), c.i8_plane(5), d_z, c.n_tgt * c.nb, st);
+            BW_CUDA(cudaStreamSynchronize(st));
+            c.i8_check_error();
+            return;
+        }
         c.launch_to_balanced(d_y, c.d_ya, c.n_src * c.nb, st);
         c.forward(c.d_ya, c.d_z, st);
         c.launch_to_canonical(c.d_z, d_z, c.n_tgt * c.nb, st);
@@ -634,6 +664,14 @@ extern "C" int bw_koszul_transpose(bw_koszul* ctx, const uint32_t* d_z, uint32_t
         BW_REQUIRE(!c.in_session, "bw_koszul_transpose: a sequence session is open");
         BW_CUDA(cudaSetDevice(c.device));
         cudaStream_t st = pick_stream(&c, stream);
+        if (c.form == BW_FORM_INT8) {
+            c.i8_to_limbs(d_z, c.i8_plane(4), c.i8_plane(5), c.n_tgt * c.nb, st);
+            c.i8_run(false, c.i8_plane(4), c.i8_plane(5), c.i8_plane(0), c.i8_plane(1), scale_by_diag != 0, st);
+            c.i8_from_limbs(c.i8_plane(0), c.i8_plane(1), d_w, c.n_src * c.nb, st);
+            BW_CUDA(cudaStreamSynchronize(st));
+            c.i8_check_error();
+            return;
+        }
         c.launch_to_balanced(d_z, c.d_z, c.n_tgt * c.nb, st);
         c.transpose(c.d_z, c.d_ya, scale_by_diag != 0, st);
         c.launch_to_canonical(c.d_ya, d_w, c.n_src * c.nb, st);
@@ -647,6 +685,15 @@ extern "C" int bw_koszul_apply(bw_koszul* ctx, const uint32_t* d_y, uint32_t* d_
         BW_REQUIRE(!c.in_session, "bw_koszul_apply: a sequence session is open");
         BW_CUDA(cudaSetDevice(c.device));
         cudaStream_t st = pick_stream(&c, stream);
+        if (c.form == BW_FORM_INT8) {
+            c.i8_to_limbs(d_y, c.i8_plane(0), c.i8_plane(1), c.n_src * c.nb, st);
+            c.i8_run(true, c.i8_plane(0), c.i8_plane(1), c.i8_plane(4), c.i8_plane(5), false, st);
+            c.i8_run(false, c.i8_plane(4), c.i8_plane(5), c.i8_plane(2), c.i8_plane(3), true, st);
+            c.i8_from_limbs(c.i8_plane(2), c.i8_plane(3), d_out, c.n_src * c.nb, st);
+            BW_CUDA(cudaStreamSynchronize(st));
+            c.i8_check_error();
+            return;
+        }
         c.launch_to_balanced(d_y, c.d_ya, c.n_src * c.nb, st);
         c.forward(c.d_ya, c.d_z, st);
         c.transpose(c.d_z, c.d_yb, true, st);
@@ -715,14 +762,23 @@ extern "C" int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* m
         std::vector<cudaEvent_t> ev(4 * steps);
         for (auto& e : ev) BW_CUDA(cudaEventCreate(&e));
         for (uint64_t s = 0; s < steps; ++s) {
-            int32_t* src = c.cur_is_a ? c.d_ya : c.d_yb;
-            int32_t* dst = c.cur_is_a ? c.d_yb : c.d_ya;
             BW_CUDA(cudaEventRecord(ev[4 * s], st));
-            c.forward(src, c.d_z, st);
-            BW_CUDA(cudaEventRecord(ev[4 * s + 1], st));
-            c.transpose(c.d_z, dst, true, st);
-            BW_CUDA(cudaEventRecord(ev[4 * s + 2], st));
-            c.project(dst, st);
+            if (c.form == BW_FORM_INT8) {
+                const int a = c.cur_is_a ? 0 : 2, b = c.cur_is_a ? 2 : 0;
+                c.i8_run(true, c.i8_plane(a), c.i8_plane(a + 1), c.i8_plane(4), c.i8_plane(5), false, st);
+                BW_CUDA(cudaEventRecord(ev[4 * s + 1], st));
+                c.i8_run(false, c.i8_plane(4), c.i8_plane(5), c.i8_plane(b), c.i8_plane(b + 1), true, st);
+                BW_CUDA(cudaEventRecord(ev[4 * s + 2], st));
+                c.i8_project(c.i8_plane(b), c.i8_plane(b + 1), st);
+            } else {
+                int32_t* src = c.cur_is_a ? c.d_ya : c.d_yb;
+                int32_t* dst = c.cur_is_a ? c.d_yb : c.d_ya;
+                c.forward(src, c.d_z, st);
+                BW_CUDA(cudaEventRecord(ev[4 * s + 1], st));
+                c.transpose(c.d_z, dst, true, st);
+                BW_CUDA(cudaEventRecord(ev[4 * s + 2], st));
+                c.project(dst, st);
+            }
             BW_CUDA(cudaEventRecord(ev[4 * s + 3], st));
             c.cur_is_a = !c.cur_is_a;
             ++c.seq_len;

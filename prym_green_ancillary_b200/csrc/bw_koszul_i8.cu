@@ -1,18 +1,645 @@
 // INT8-limb tensor-core form of the synthetic Koszul operator (tcgen05 kind::i8).
-// Not yet built: requesting the form fails loudly at context creation.
+//
+// Every residue x (balanced, |x| <= (p-1)/2 < 2^14) is stored in HBM as two
+// signed 8-bit limbs in base 255:  x = 255*hi + lo,  lo in [-127, 127],
+// hi in [-63, 63].  The symmetric range makes negation exact in int8, which
+// is how the Koszul signs are applied while operands are staged.
+//
+// One gather-GEMM kernel serves both d and d^T.  For a tile of 128/n output
+// blocks (n = block width) the output is
+//   out[blk][o][j] = sum_{i < r} sum_{u < inner} A[(blk, j)][(i, u)] * Bm[o][(i, u)]
+// with A[(blk, j)][(i, u)] = sign * in[nbr(blk, i)][u][j] (zero when the
+// generator i is not incident to blk) and Bm = the r maps side by side.  The
+// tile is an M = 128 GEMM: A = the gathered input blocks (MN-major in shared
+// memory: one input block row of n limbs is one 16-byte core-matrix row),
+// B = the maps' lo and hi limbs stacked along N (K-major, resident in shared
+// memory for the whole kernel), K = r * inner in steps of 32.  Two MMAs per
+// K-step (A = input lo limbs, A = input hi limbs) give four int32 partial
+// products per output, recombined exactly mod p in the epilogue:
+//   x*m = lo*lo + 255*(lo*hi + hi*lo) + 255^2*hi*hi.
+// int32 accumulation is exact: |K * 127 * 127| < 2^24 for K <= 1024.
+//
+// Warp roles (persistent, one CTA per SM):
+//   warps 0-3  producers: load limb rows, negate where the Koszul sign is -1,
+//              store them into the stage's A tile (zero rows for absent i);
+//   warp 4     allocates TMEM and issues tcgen05.mma / tcgen05.commit;
+//   warps 5-8  epilogue: tcgen05.ld the four partials, recombine, reduce mod p,
+//              scale by D (d^T only), split into limbs and store.
+// Stages are tracked with mbarriers; accumulators are double-buffered in TMEM.
+// Every wait is bounded: on a timeout the kernel records an error code, all
+// roles wind down, in-flight MMAs are drained and TMEM is freed.
 #include "bw_koszul.cuh"
+#include "tc_sm100.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
 
 namespace bw {
 
-struct KoszulCtx::I8State {};
+namespace {
+
+constexpr uint32_t kAbsent = 0xFFFFFFFFu;
+constexpr int kProducerWarps = 4;
+constexpr int kMmaWarp = 4;
+constexpr int kI8Threads = 9 * 32;
+constexpr int kMaxSmem = 227 * 1024;
+
+struct I8Dir {
+    const int8_t* in_lo;
+    const int8_t* in_hi;
+    int8_t* out_lo;
+    int8_t* out_hi;
+    const uint32_t* inc;      // [n_blk][r]: neighbour rank | negative << 31, or kAbsent
+    const int8_t* b_tiles;    // B operand, already in its shared-memory layout
+    const int32_t* diag;      // nullptr, or [n_blk * outer] balanced (scales the output)
+    int* err;
+    long long n_blk;
+    int r, inner, outer, half;   // N = 2 * half, half = outer rounded up to 16
+    int gi;                      // generators per stage
+    int stages_per_tile;         // ceil(r / gi)
+    int ks_full;                 // K-steps of a full stage (gi * inner / 32)
+    int ks_last;                 // K-steps of the last stage
+    int slots;                   // pipeline depth
+    uint32_t b_bytes, slot_bytes, limb_bytes;
+    Mod mod;
+    int32_t c1, c2;              // 255 and 255^2 mod p, balanced
+};
+
+__device__ __forceinline__ int32_t combine(int32_t ll, int32_t lhhl, int32_t hh, const I8Dir& P) {
+    const int32_t a = reduce_partial(ll, P.mod);
+    const int32_t b = reduce_partial(lhhl, P.mod);
+    const int32_t c = reduce_partial(hh, P.mod);
+    return reduce_balanced(a + P.c1 * b + P.c2 * c, P.mod);
+}
+
+__device__ __forceinline__ void split_limbs(int32_t v, int8_t& lo, int8_t& hi) {
+    // v in [-16383, 16383]: q = floor((v + 127) / 255), lo = v - 255 q in [-127, 127]
+    const int32_t q = static_cast<int32_t>(static_cast<uint32_t>(v + 127 + 255 * 128) / 255u) - 128;
+    lo = static_cast<int8_t>(v - 255 * q);
+    hi = static_cast<int8_t>(q);
+}
+
+template <int NB>
+__global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    constexpr int BT = 128 / NB;        // output blocks per tile
+    constexpr int HG = NB / 16;         // 16-byte chunks per input block row
+    const int N = 2 * P.half;
+    uint8_t* sB = smem;
+    uint8_t* sA = smem + P.b_bytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sA + static_cast<size_t>(P.slots) * P.slot_bytes);
+    uint64_t* empty = full + P.slots;
+    uint64_t* accfull = empty + P.slots;
+    uint64_t* accempty = accfull + 2;
+    uint64_t* drained = accempty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const long long n_tiles = (P.n_blk + BT - 1) / BT;
+
+    // B operand: global -> shared (generic stores, made visible to the tensor core below)
+    for (uint32_t off = threadIdx.x * 16; off < P.b_bytes; off += blockDim.x * 16)
+        *reinterpret_cast<int4*>(sB + off) = __ldg(reinterpret_cast<const int4*>(P.b_tiles + off));
+    tc::fence_proxy_async_smem();
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < P.slots; ++s) {
+            tc::mbar_init(&full[s], kProducerWarps * 32);
+            tc::mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            tc::mbar_init(&accfull[b], 1);
+            tc::mbar_init(&accempty[b], 128);
+        }
+        tc::mbar_init(drained, 1);
+        tc::fence_mbar_init();
+    }
+    const uint32_t tmem_cols = (4 * N <= 256) ? 256u : 512u;
+    if (warp == kMmaWarp) {
+        tc::tmem_alloc(tmem_slot, tmem_cols);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp < kProducerWarps) {
+        // ------------------------------------------------------------ producers
+        long long it = 0;
+        bool ok = true;
+        for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+            for (int s = 0; s < P.stages_per_tile && ok; ++s, ++it) {
+                const int slot = static_cast<int>(it % P.slots);
+                const uint32_t ph = static_cast<uint32_t>((it / P.slots) & 1);
+                if (!tc::mbar_wait(&empty[slot], ph ^ 1u, P.err, tc::ERR_WAIT_EMPTY)) {
+                    ok = false;
+                    break;
+                }
+                const int g_s = min(P.gi, P.r - s * P.gi);
+                const int KS = P.gi * P.inner;     // K' extent of a slot
+                uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
+                const int nblocks = 2 * BT * g_s;
+                const int chunks = P.inner * HG;
+                for (int bi = warp; bi < nblocks; bi += kProducerWarps) {
+                    const int limb = bi / (BT * g_s);
+                    const int rem = bi - limb * BT * g_s;
+                    const int t = rem / g_s;
+                    const int il = rem - t * g_s;
+                    const long long blk = tile * BT + t;
+                    const uint32_t e = blk < P.n_blk ? __ldg(P.inc + blk * P.r + s * P.gi + il) : kAbsent;
+                    const int8_t* plane = limb ? P.in_hi : P.in_lo;
+                    uint8_t* dst0 = slotA + static_cast<size_t>(limb) * P.limb_bytes;
+                    for (int w = lane; w < chunks; w += 32) {
+                        const int b = w / HG, h = w - b * HG;
+                        uint8_t* dst = dst0 + static_cast<size_t>(t * HG + h) * KS * 16 +
+                                       static_cast<size_t>(il * P.inner + b) * 16;
+                        int4 v = make_int4(0, 0, 0, 0);
+                        if (e != kAbsent) {
+                            const long long src_blk = static_cast<long long>(e & 0x7FFFFFFFu);
+                            v = __ldg(reinterpret_cast<const int4*>(plane + (src_blk * P.inner + b) * NB + h * 16));
+                            if (e >> 31) {
+                                v.x = static_cast<int>(__vsub4(0u, static_cast<unsigned>(v.x)));
+                                v.y = static_cast<int>(__vsub4(0u, static_cast<unsigned>(v.y)));
+                                v.z = static_cast<int>(__vsub4(0u, static_cast<unsigned>(v.z)));
+                                v.w = static_cast<int>(__vsub4(0u, static_cast<unsigned>(v.w)));
+                            }
+                        }
+                        *reinterpret_cast<int4*>(dst) = v;
+                    }
+                }
+                tc::fence_proxy_async_smem();
+                tc::mbar_arrive(&full[slot]);
+            }
+        }
+    } else if (warp == kMmaWarp) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_i8(128, N, true, false);
+            const uint32_t sA0 = tc::smem_u32(sA), sB0 = tc::smem_u32(sB);
+            const int KS = P.gi * P.inner;
+            long long it = 0, tcount = 0;
+            bool ok = true;
+            for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
+                const int buf = static_cast<int>(tcount & 1);
+                const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
+                if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, P.err, tc::ERR_WAIT_ACCUM_FREE)) break;
+                tc::tc_fence_after();
+                const uint32_t dbase = tmem + static_cast<uint32_t>(buf * 2 * N);
+                for (int s = 0; s < P.stages_per_tile; ++s, ++it) {
+                    const int slot = static_cast<int>(it % P.slots);
+                    const uint32_t ph = static_cast<uint32_t>((it / P.slots) & 1);
+                    if (!tc::mbar_wait(&full[slot], ph, P.err, tc::ERR_WAIT_FULL)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::tc_fence_after();
+                    const int ks_n = (s == P.stages_per_tile - 1) ? P.ks_last : P.ks_full;
+                    for (int limb = 0; limb < 2; ++limb) {
+                        const uint32_t a_base = sA0 + static_cast<uint32_t>(slot) * P.slot_bytes +
+                                                static_cast<uint32_t>(limb) * P.limb_bytes;
+                        for (int ks = 0; ks < ks_n; ++ks) {
+                            const uint64_t ad = tc::smem_desc(a_base + ks * 512u, 128u, static_cast<uint32_t>(KS) * 16u);
+                            const uint32_t gks = static_cast<uint32_t>(s * P.ks_full + ks);
+                            const uint64_t bd = tc::smem_desc(sB0 + gks * static_cast<uint32_t>(N) * 32u, 128u, 256u);
+                            tc::mma_i8(dbase + static_cast<uint32_t>(limb * N), ad, bd, idesc,
+                                       (s > 0 || ks > 0) ? 1u : 0u);
+                        }
+                    }
+                    tc::mma_commit(&empty[slot]);
+                }
+                if (!ok) break;
+                tc::mma_commit(&accfull[buf]);
+            }
+            // drain: every MMA issued above completes before TMEM is released
+            tc::mma_commit(drained);
+            tc::mbar_wait(drained, 0, P.err, tc::ERR_WAIT_FINAL);
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int q = warp & 3;                 // TMEM lane quadrant of this warp
+        const int m = q * 32 + lane;            // tile row = (block t, column j)
+        const int t = m / NB, j = m % NB;
+        const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
+        long long tcount = 0;
+        for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++tcount) {
+            const int buf = static_cast<int>(tcount & 1);
+            const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
+            if (!tc::mbar_wait(&accfull[buf], aph, P.err, tc::ERR_WAIT_ACCUM)) break;
+            tc::tc_fence_after();
+            const long long blk = tile * BT + t;
+            const bool valid = blk < P.n_blk;
+            const uint32_t col0 = tmem + lane_off + static_cast<uint32_t>(buf * 2 * N);
+            for (int o0 = 0; o0 < P.half; o0 += 16) {
+                int32_t ll[16], lh[16], hl[16], hh[16];
+                tc::tmem_ld16(col0 + o0, ll);
+                tc::tmem_ld16(col0 + P.half + o0, lh);
+                tc::tmem_ld16(col0 + N + o0, hl);
+                tc::tmem_ld16(col0 + N + P.half + o0, hh);
+                tc::tmem_ld_wait();
+                if (valid) {
+#pragma unroll
+                    for (int oo = 0; oo < 16; ++oo) {
+                        const int o = o0 + oo;
+                        if (o < P.outer) {
+                            int32_t v = combine(ll[oo], lh[oo] + hl[oo], hh[oo], P);
+                            const long long row = blk * P.outer + o;
+                            if (P.diag) v = reduce_balanced(v * __ldg(P.diag + row), P.mod);
+                            int8_t lo, hi;
+                            split_limbs(v, lo, hi);
+                            P.out_lo[row * NB + j] = lo;
+                            P.out_hi[row * NB + j] = hi;
+                        }
+                    }
+                }
+            }
+            tc::tc_fence_before();
+            tc::mbar_arrive(&accempty[buf]);
+        }
+    }
+
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == kMmaWarp) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, tmem_cols);
+    }
+}
+
+// ---- limb conversions and the projection on limb planes
+
+__global__ void to_limbs_kernel(const uint32_t* __restrict__ in, int8_t* __restrict__ lo, int8_t* __restrict__ hi,
+                                long long count, Mod mod) {
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        int8_t a, b;
+        split_limbs(to_balanced(in[i] % static_cast<uint32_t>(mod.p), mod), a, b);
+        lo[i] = a;
+        hi[i] = b;
+    }
+}
+
+__global__ void from_limbs_kernel(const int8_t* __restrict__ lo, const int8_t* __restrict__ hi,
+                                  uint32_t* __restrict__ out, long long count, Mod mod) {
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+        out[i] = to_canonical(255 * static_cast<int32_t>(hi[i]) + lo[i], mod);
+}
+
+__global__ void to_int16_kernel(const uint32_t* __restrict__ in, int16_t* __restrict__ out, long long count,
+                                Mod mod) {
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+        out[i] = static_cast<int16_t>(to_balanced(in[i] % static_cast<uint32_t>(mod.p), mod));
+}
+
+__device__ __forceinline__ int32_t limb_value(uint32_t lo4, uint32_t hi4, int k) {
+    const int32_t lo = static_cast<int8_t>((lo4 >> (8 * k)) & 0xFF);
+    const int32_t hi = static_cast<int8_t>((hi4 >> (8 * k)) & 0xFF);
+    return 255 * hi + lo;
+}
+
+// a = X^T W into seq[*seq_index]; X int16 balanced (rows x m), W as limb planes (rows x n).
+template <int NB>
+__global__ void __launch_bounds__(256) i8_project_kernel(
+    const int16_t* __restrict__ X, const int8_t* __restrict__ Wlo, const int8_t* __restrict__ Whi, long long rows,
+    int m, int32_t* __restrict__ partials, unsigned int* __restrict__ counter, uint32_t* __restrict__ seq,
+    unsigned long long* __restrict__ seq_index, Mod mod) {
+    constexpr int JG = NB / 4;
+    const int tps = m * JG;
+    const int slices = blockDim.x / tps;
+    const int slice = threadIdx.x / tps;
+    const int sub = threadIdx.x - slice * tps;
+    const int x = sub / JG;
+    const int jg = sub - x * JG;
+    __shared__ int32_t red[256 * 4];
+    __shared__ bool am_last;
+    int32_t acc[4] = {0, 0, 0, 0};
+    int cnt = 0;
+    for (long long row = static_cast<long long>(blockIdx.x) * slices + slice; row < rows;
+         row += static_cast<long long>(gridDim.x) * slices) {
+        const int32_t xv = __ldg(X + row * m + x);
+        const uint32_t lo4 = __ldg(reinterpret_cast<const uint32_t*>(Wlo + row * NB) + jg);
+        const uint32_t hi4 = __ldg(reinterpret_cast<const uint32_t*>(Whi + row * NB) + jg);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[k] += xv * limb_value(lo4, hi4, k);
+        if (++cnt == 8) {
+            cnt = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[k] = reduce_partial(acc[k], mod);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) red[threadIdx.x * 4 + k] = reduce_balanced(acc[k], mod);
+    __syncthreads();
+    if (threadIdx.x < tps) {
+        int32_t s[4] = {0, 0, 0, 0};
+        for (int sl = 0; sl < slices; ++sl)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                s[k] += red[(sl * tps + threadIdx.x) * 4 + k];
+                if ((sl & 7) == 7) s[k] = reduce_partial(s[k], mod);
+            }
+        const int xx = threadIdx.x / JG, jj = threadIdx.x - xx * JG;
+        int32_t* dst = partials + (static_cast<size_t>(blockIdx.x) * m + xx) * NB + jj * 4;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dst[k] = reduce_balanced(s[k], mod);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    const unsigned long long pos = *reinterpret_cast<volatile unsigned long long*>(seq_index);
+    const int entries = m * NB;
+    for (int e = threadIdx.x; e < entries; e += blockDim.x) {
+        int32_t s = 0;
+        for (unsigned b = 0; b < gridDim.x; ++b) {
+            s += reinterpret_cast<volatile int32_t*>(partials)[static_cast<size_t>(b) * entries + e];
+            if ((b & 7) == 7) s = reduce_partial(s, mod);
+        }
+        seq[pos * entries + e] = to_canonical(reduce_balanced(s, mod), mod);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *seq_index = pos + 1;
+        *counter = 0;
+        __threadfence();
+    }
+}
+
+int gcd_int(int a, int b) {
+    while (b) {
+        int t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+void host_split(int32_t v, int8_t& lo, int8_t& hi) {
+    const int32_t q = static_cast<int32_t>(static_cast<uint32_t>(v + 127 + 255 * 128) / 255u) - 128;
+    lo = static_cast<int8_t>(v - 255 * q);
+    hi = static_cast<int8_t>(q);
+}
+
+}  // namespace
+
+// Host-side state of the INT8 form.
+struct KoszulCtx::I8State {
+    struct Dir {
+        I8Dir p{};
+        int8_t* b_tiles = nullptr;
+        uint32_t* inc = nullptr;
+        size_t smem = 0;
+        unsigned grid = 0;
+    } fwd, bwd;
+    int8_t *ya_lo = nullptr, *ya_hi = nullptr, *yb_lo = nullptr, *yb_hi = nullptr, *z_lo = nullptr, *z_hi = nullptr;
+    int16_t* x16 = nullptr;
+    int* err = nullptr;
+};
+
+namespace {
+
+// Plans one direction: stage size, pipeline depth, B operand (host layout).
+void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int outer, bool transpose_maps) {
+    I8Dir& P = D.p;
+    P.r = c.r;
+    P.inner = inner;
+    P.outer = outer;
+    P.half = (outer + 15) / 16 * 16;
+    const int N = 2 * P.half;
+    BW_REQUIRE(N <= 256, "INT8 form: output dimension above 128 is not supported");
+    const int base_g = 32 / gcd_int(inner, 32);
+    BW_REQUIRE(base_g <= c.r || true, "");
+    // grow the stage towards ~40 KB of A per slot
+    int gi = base_g;
+    auto slot_bytes_for = [&](int g) { return static_cast<size_t>(2) * 8 * (g * inner) * 16; };
+    while (gi * 2 <= std::max(base_g, c.r) && slot_bytes_for(gi * 2) <= 48 * 1024) gi *= 2;
+    P.gi = gi;
+    P.stages_per_tile = (c.r + gi - 1) / gi;
+    P.ks_full = gi * inner / 32;
+    const int last_g = c.r - (P.stages_per_tile - 1) * gi;
+    P.ks_last = (last_g * inner + 31) / 32;
+    const int total_ks = (P.stages_per_tile - 1) * P.ks_full + P.ks_last;
+    P.b_bytes = static_cast<uint32_t>(total_ks) * N * 32;
+    P.limb_bytes = static_cast<uint32_t>(8 * gi * inner * 16);
+    P.slot_bytes = 2 * P.limb_bytes;
+    const size_t bars = (2 * 8 + 2 * 2 + 1) * 8 + 16;
+    int slots = 4;
+    while (slots > 1 && P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + bars > static_cast<size_t>(kMaxSmem))
+        --slots;
+    BW_REQUIRE(P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + bars <= static_cast<size_t>(kMaxSmem),
+               "INT8 form: maps too large for shared memory");
+    P.slots = slots;
+    D.smem = P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + bars;
+    P.mod = c.mod;
+    P.c1 = to_balanced(255u % c.p, c.mod);
+    P.c2 = to_balanced(static_cast<uint32_t>((255ull * 255ull) % c.p), c.mod);
+
+    // B: row n < half -> lo limb, n >= half -> hi limb of map coefficient (o = n mod half),
+    // column K' = i * inner + u; K-major, 8x16-byte core matrices, LBO 128, SBO 256.
+    std::vector<int8_t> B(P.b_bytes, 0);
+    const int kp_total = total_ks * 32;
+    for (int kp = 0; kp < kp_total; ++kp) {
+        // K' of global K-step: stages are exact multiples of 32 except the last
+        const int s = std::min(kp / (P.ks_full * 32), P.stages_per_tile - 1);
+        const int local = kp - s * P.ks_full * 32;
+        const int gen_local = local / inner, u = local % inner;
+        const int i = s * gi + gen_local;
+        if (gen_local >= (s == P.stages_per_tile - 1 ? last_g : gi)) continue;   // padding
+        for (int n = 0; n < N; ++n) {
+            const int o = n % P.half;
+            if (o >= outer) continue;
+            // forward: coefficient M_i[o = c][u = b]; transpose: M_i[u = c][o = b]
+            const uint32_t raw = transpose_maps
+                                     ? c.maps_canonical[(static_cast<size_t>(i) * c.co + u) * c.ci + o]
+                                     : c.maps_canonical[(static_cast<size_t>(i) * c.co + o) * c.ci + u];
+            int8_t lo, hi;
+            host_split(to_balanced(raw % c.p, c.mod), lo, hi);
+            const int ks = kp / 32, kk = kp % 32;
+            const size_t off = static_cast<size_t>(ks) * N * 32 + (n / 8) * 256 + (kk / 16) * 128 + (n % 8) * 16 + (kk % 16);
+            B[off] = n < P.half ? lo : hi;
+        }
+    }
+    D.b_tiles = c.alloc<int8_t>(P.b_bytes);
+    BW_CUDA(cudaMemcpyAsync(D.b_tiles, B.data(), B.size(), cudaMemcpyHostToDevice, c.own_stream));
+    BW_CUDA(cudaStreamSynchronize(c.own_stream));
+    P.b_tiles = D.b_tiles;
+}
+
+template <int NB>
+void launch_i8(KoszulCtx& c, KoszulCtx::I8State::Dir& D, cudaStream_t st) {
+    i8_gather_gemm_kernel<NB><<<D.grid, kI8Threads, D.smem, st>>>(D.p);
+    BW_CHECK_LAUNCH();
+    ++c.launches;
+}
+
+template <class F>
+void dispatch_i8_nb(int nb, F&& f) {
+    switch (nb) {
+        case 16: f(std::integral_constant<int, 16>{}); break;
+        case 32: f(std::integral_constant<int, 32>{}); break;
+        default: throw Error("INT8 form supports block widths 16 and 32", 1);
+    }
+}
+
+}  // namespace
 
 void KoszulCtx::i8_destroy() {
     delete i8;
     i8 = nullptr;
 }
-void KoszulCtx::i8_setup() { throw Error("the INT8-limb tensor-core form is not available in this build", 3); }
-void KoszulCtx::i8_forward(const int32_t*, int32_t*, cudaStream_t) { i8_setup(); }
-void KoszulCtx::i8_transpose(const int32_t*, int32_t*, bool, cudaStream_t) { i8_setup(); }
+
+void KoszulCtx::i8_setup() {
+    BW_REQUIRE(nb == 16 || nb == 32, "INT8 form supports block widths 16 and 32");
+    BW_REQUIRE(ci <= 128 && co <= 128, "INT8 form: dim_in and dim_out must be at most 128");
+    BW_REQUIRE(static_cast<long long>(r) * std::max(ci, co) <= 1024, "INT8 form: r * dim above 1024 (int32 bound)");
+    int major = 0;
+    BW_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    BW_REQUIRE(major == 10, "INT8 form needs an sm_100 GPU (tcgen05)");
+    i8 = new I8State();
+    I8State& S = *i8;
+    // dense incidence tables: fwd[T][i] (S = T u i), bwd[S][i] (T = S \ i)
+    std::vector<uint32_t> fwd(n_t * r, kAbsent), bwd(n_s * r, kAbsent);
+    int T[64], Sx[64];
+    for (uint64_t t = 0; t < n_t; ++t) {
+        lex_unrank(t, r, k - 1, T);
+        int pos = 0;
+        for (int i = 0; i < r; ++i) {
+            if (pos < k - 1 && T[pos] == i) {
+                ++pos;
+                continue;
+            }
+            for (int qq = 0, w = 0; qq < k; ++qq) Sx[qq] = (qq == pos) ? i : T[w++];
+            fwd[t * r + i] = static_cast<uint32_t>(lex_rank(Sx, r, k)) | ((pos & 1) ? 0x80000000u : 0u);
+        }
+    }
+    for (uint64_t s = 0; s < n_s; ++s) {
+        lex_unrank(s, r, k, Sx);
+        for (int pos = 0; pos < k; ++pos) {
+            for (int qq = 0, w = 0; qq < k; ++qq)
+                if (qq != pos) T[w++] = Sx[qq];
+            bwd[s * r + Sx[pos]] = static_cast<uint32_t>(lex_rank(T, r, k - 1)) | ((pos & 1) ? 0x80000000u : 0u);
+        }
+    }
+    S.fwd.inc = alloc<uint32_t>(fwd.size());
+    S.bwd.inc = alloc<uint32_t>(bwd.size());
+    BW_CUDA(cudaMemcpyAsync(S.fwd.inc, fwd.data(), fwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
+    BW_CUDA(cudaMemcpyAsync(S.bwd.inc, bwd.data(), bwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
+    S.ya_lo = alloc<int8_t>(n_src * nb);
+    S.ya_hi = alloc<int8_t>(n_src * nb);
+    S.yb_lo = alloc<int8_t>(n_src * nb);
+    S.yb_hi = alloc<int8_t>(n_src * nb);
+    S.z_lo = alloc<int8_t>(n_tgt * nb);
+    S.z_hi = alloc<int8_t>(n_tgt * nb);
+    S.x16 = alloc<int16_t>(n_src * m);
+    S.err = alloc<int>(1);
+    BW_CUDA(cudaMemsetAsync(S.err, 0, sizeof(int), own_stream));
+    plan_direction(*this, S.fwd, ci, co, false);
+    plan_direction(*this, S.bwd, co, ci, true);
+    S.fwd.p.inc = S.fwd.inc;
+    S.bwd.p.inc = S.bwd.inc;
+    S.fwd.p.n_blk = static_cast<long long>(n_t);
+    S.bwd.p.n_blk = static_cast<long long>(n_s);
+    S.fwd.p.err = S.err;
+    S.bwd.p.err = S.err;
+    S.fwd.p.diag = nullptr;
+    S.bwd.p.diag = d_diag;
+    dispatch_i8_nb(nb, [&](auto NBc) {
+        auto kern = i8_gather_gemm_kernel<decltype(NBc)::value>;
+        const int need = static_cast<int>(std::max(S.fwd.smem, S.bwd.smem));
+        BW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
+    });
+    const int bt = 128 / nb;
+    S.fwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_t + bt - 1) / bt, sms)));
+    S.bwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_s + bt - 1) / bt, sms)));
+}
+
 uint64_t KoszulCtx::i8_kernels_per_step() const { return 3; }
+
+// Limb-plane forward / transpose used by the sequence path.
+void KoszulCtx::i8_run(bool forward_dir, const int8_t* in_lo, const int8_t* in_hi, int8_t* out_lo, int8_t* out_hi,
+                       bool scale, cudaStream_t st) {
+    I8State::Dir& D = forward_dir ? i8->fwd : i8->bwd;
+    D.p.in_lo = in_lo;
+    D.p.in_hi = in_hi;
+    D.p.out_lo = out_lo;
+    D.p.out_hi = out_hi;
+    D.p.diag = (!forward_dir && scale) ? d_diag : nullptr;
+    dispatch_i8_nb(nb, [&](auto NBc) { launch_i8<decltype(NBc)::value>(*this, D, st); });
+}
+
+void KoszulCtx::i8_check_error() {
+    int err = 0;
+    BW_CUDA(cudaMemcpy(&err, i8->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err != 0) {
+        cudaMemset(i8->err, 0, sizeof(int));
+        throw Error("INT8 tensor-core kernel gave up waiting (pipeline stage wait, code " + std::to_string(err) + ")", 2);
+    }
+}
+
+void KoszulCtx::i8_to_limbs(const uint32_t* in, int8_t* lo, int8_t* hi, uint64_t count, cudaStream_t st) {
+    unsigned grid = static_cast<unsigned>(std::min<uint64_t>((count + 255) / 256, static_cast<uint64_t>(sms) * 8));
+    to_limbs_kernel<<<std::max(grid, 1u), 256, 0, st>>>(in, lo, hi, static_cast<long long>(count), mod);
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+void KoszulCtx::i8_from_limbs(const int8_t* lo, const int8_t* hi, uint32_t* out, uint64_t count, cudaStream_t st) {
+    unsigned grid = static_cast<unsigned>(std::min<uint64_t>((count + 255) / 256, static_cast<uint64_t>(sms) * 8));
+    from_limbs_kernel<<<std::max(grid, 1u), 256, 0, st>>>(lo, hi, out, static_cast<long long>(count), mod);
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+void KoszulCtx::i8_load_x(const uint32_t* x, cudaStream_t st) {
+    const uint64_t count = n_src * m;
+    unsigned grid = static_cast<unsigned>(std::min<uint64_t>((count + 255) / 256, static_cast<uint64_t>(sms) * 8));
+    to_int16_kernel<<<std::max(grid, 1u), 256, 0, st>>>(x, i8->x16, static_cast<long long>(count), mod);
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+void KoszulCtx::i8_project(const int8_t* lo, const int8_t* hi, cudaStream_t st) {
+    dispatch_i8_nb(nb, [&](auto NBc) {
+        i8_project_kernel<decltype(NBc)::value><<<proj_grid, 256, 0, st>>>(
+            i8->x16, lo, hi, static_cast<long long>(n_src), m, d_partials, d_counter, d_seq, d_seq_index, mod);
+    });
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+// One INT8 step on the limb state: cur -> other, append a_i.
+void KoszulCtx::i8_step_once(cudaStream_t st) {
+    I8State& S = *i8;
+    int8_t* slo = cur_is_a ? S.ya_lo : S.yb_lo;
+    int8_t* shi = cur_is_a ? S.ya_hi : S.yb_hi;
+    int8_t* dlo = cur_is_a ? S.yb_lo : S.ya_lo;
+    int8_t* dhi = cur_is_a ? S.yb_hi : S.ya_hi;
+    i8_run(true, slo, shi, S.z_lo, S.z_hi, false, st);
+    i8_run(false, S.z_lo, S.z_hi, dlo, dhi, true, st);
+    i8_project(dlo, dhi, st);
+    cur_is_a = !cur_is_a;
+}
+int8_t* KoszulCtx::i8_plane(int which) {
+    switch (which) {
+        case 0: return i8->ya_lo;
+        case 1: return i8->ya_hi;
+        case 2: return i8->yb_lo;
+        case 3: return i8->yb_hi;
+        case 4: return i8->z_lo;
+        default: return i8->z_hi;
+    }
+}
+
+void KoszulCtx::i8_forward(const int32_t*, int32_t*, cudaStream_t) {
+    throw Error("internal: the INT8 form runs on limb planes", 3);
+}
+void KoszulCtx::i8_transpose(const int32_t*, int32_t*, bool, cudaStream_t) {
+    throw Error("internal: the INT8 form runs on limb planes", 3);
+}
 
 }  // namespace bw

@@ -22,7 +22,13 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = np.load(Path(__file__).parent / "golden" / "koszul_golden.npz")
 CASES = sorted({k.split("/")[0] for k in GOLDEN.files})
-FORMS = ["plain"]
+FORMS = ["plain", "int8"]
+
+
+def _supported(form, nb):
+    """The INT8-limb form runs block widths 16 and 32."""
+    if form == "int8" and nb not in (16, 32):
+        pytest.skip("INT8-limb form needs block width 16 or 32")
 
 
 def _golden_case(name):
@@ -39,6 +45,7 @@ def _engine(shape, maps, diag, form):
 @pytest.mark.parametrize("name", CASES)
 def test_sequence_matches_golden(name, form):
     shape, nlen, seed = _golden_case(name)
+    _supported(form, shape.nb)
     maps, diag, X, Y = oracle.seeded_problem(shape, seed)
     with _engine(shape, maps, diag, form) as eng:
         seq, yf = eng.sequence_host(X, Y, nlen)
@@ -62,6 +69,7 @@ SHAPES = [
 @pytest.mark.parametrize("dims", SHAPES)
 def test_operators_match_oracle(dims, form):
     shape = oracle.KoszulShape(*dims)
+    _supported(form, shape.nb)
     maps, diag, X, Y = oracle.seeded_problem(shape, 99)
     rng = np.random.default_rng(5)
     Z = rng.integers(0, shape.p, (shape.n_tgt, shape.nb), dtype=np.uint32)
@@ -126,12 +134,12 @@ def _check_sampled_rows(shape, maps, diag, y, out, count, seed):
 
 
 def _projection(x, w, p):
-    # exact int64 X^T W on the host (products < 2^30, 2^20 rows per chunk < 2^50)
-    xn = x.cpu().numpy().astype(np.int64)
-    wn = w.cpu().numpy().astype(np.int64)
-    acc = np.zeros((xn.shape[1], wn.shape[1]), dtype=np.int64)
-    for s in range(0, xn.shape[0], 1 << 20):
-        acc = (acc + xn[s:s + (1 << 20)].T @ wn[s:s + (1 << 20)]) % p
+    # exact int64 X^T W on the host, chunk by chunk (products < 2^30, 2^20 rows per chunk < 2^50)
+    acc = np.zeros((x.shape[1], w.shape[1]), dtype=np.int64)
+    for s in range(0, x.shape[0], 1 << 20):
+        xn = x[s:s + (1 << 20)].cpu().numpy().astype(np.int64)
+        wn = w[s:s + (1 << 20)].cpu().numpy().astype(np.int64)
+        acc = (acc + xn.T @ wn) % p
     return acc.astype(np.uint32)
 
 
@@ -139,6 +147,8 @@ def _projection(x, w, p):
 @pytest.mark.parametrize("cfg", [
     # r = 19, k = 9, dim 20 -> 28, p = 32003, block 16 x 16 (N = 1,847,560)
     ("config2", 19, 9, 20, 28, 32003, 16, 16, 3),
+    # r = 23, k = 11, dim 32 -> 40, block 32 x 32 (N = 43,266,496)
+    ("config5", 23, 11, 32, 40, 32003, 32, 32, 1),
 ])
 def test_full_size_apply_and_session(cfg, form):
     name, r, k, ci, co, p, nb, m, steps = cfg
@@ -172,7 +182,7 @@ def test_full_size_apply_and_session(cfg, form):
 @pytest.mark.parametrize("form", FORMS)
 def test_session_graph_path_matches_direct(form):
     """Long sessions use captured graphs of 16 steps; compare with a direct run."""
-    shape = oracle.KoszulShape(8, 3, 6, 5, 32003, 8, 8)
+    shape = oracle.KoszulShape(8, 3, 6, 5, 32003, 16, 16)
     maps, diag, X, Y = oracle.seeded_problem(shape, 3)
     nlen = 41   # 40 steps: two graph replays of 16 plus 8 direct steps
     want, yf_want = oracle.sequence(shape, maps, diag, X, Y, nlen)
