@@ -204,6 +204,22 @@ BW_API int bw_cyclic_validate(bw_cyclic* ctx, uint32_t columns);
 
 BW_API uint64_t bw_cyclic_launch_count(const bw_cyclic* ctx);
 
+/* Kernel-vector recovery (replaces cuda/cuprym_cyclic_kernel_vectors.cu,
+ * recover_eliminated_kernel_vectors and recover_kernel_vectors_core,
+ * :2550-2986): reads the WDM initial state and its row-mixing sidecar
+ * (hashes and plan checked as in resolve_rowmix_options, :1554-1643), the
+ * generator file (one v x v matrix per line), forms D = sum_k S^k V G_k^t on
+ * the device, certifies F Dc D = 0 and writes the preconditioned and
+ * original-coordinate candidates and the JSON report.  Empty or NULL paths
+ * take the reference's defaults (WDM stem + _generators.txt, WDM +
+ * _nullvectors_{1,2}.txt, WDM + _nullvectors_report.json).  cli_rounds and
+ * cli_seed apply only without a sidecar (rounds_supplied/seed_supplied say
+ * whether the caller passed them). */
+BW_API int bw_cyclic_recover(const char* instance_path, const char* op, uint32_t sector, const char* wdm_path,
+                             const char* generators_path, const char* preconditioned_out, const char* original_out,
+                             const char* report_out, int64_t cli_rounds, uint64_t cli_seed, int rounds_supplied,
+                             int seed_supplied, int validate, int device);
+
 /* Block projection d_out = X^T W (m x n canonical residues; X is rows x m and
  * W rows x n, canonical, device, W 16-byte aligned) that allocates nothing:
  * the cross-CTA scratch is a fixed 1 MiB + 256 B array inside the library.

@@ -435,7 +435,8 @@ std::vector<int32_t> balanced(const std::vector<uint32_t>& v, const Mod& m) {
 }  // namespace
 
 CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& op, size_t sector, size_t num_v,
-                           uint64_t seed, size_t rowmix_rounds, uint64_t rowmix_seed, int dev) {
+                           uint64_t seed, size_t rowmix_rounds, uint64_t rowmix_seed, int dev,
+                           const CyclicSource* src) {
     BW_REQUIRE(op == "eliminated", "--operator must be eliminated");
     BW_REQUIRE(num_v == 4, "the paper pipeline requires exactly 4 block vectors");
     std::unique_ptr<CyclicCtx> c(new CyclicCtx());
@@ -452,11 +453,23 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
     const auto& es = c->es;
     const auto& inst = c->inst;
 
-    // Seeded data in the reference's draw order (cuda/cuprym_cyclic.cu:2196-2199).
-    std::mt19937_64 gen(cyclic::seeded_sector_value(seed, sector));
-    c->row_precond = cyclic::random_vector(es.target_rows, c->p, gen, true);
-    c->col_precond = cyclic::random_vector(es.total_cols(), c->p, gen, true);
-    c->initial_block = cyclic::random_vector(es.total_cols() * num_v, c->p, gen, false);
+    if (src) {
+        // Recovery: preconditioners, initial block and mixing recipe come from the WDM file and sidecar.
+        BW_REQUIRE(src->row_precond.size() == es.target_rows, "WDM row count does not match eliminated sector");
+        BW_REQUIRE(src->col_precond.size() == es.total_cols(), "WDM column count does not match eliminated sector");
+        BW_REQUIRE(src->initial_block.size() == es.total_cols() * num_v, "WDM initial block has the wrong size");
+        c->row_precond = src->row_precond;
+        c->col_precond = src->col_precond;
+        c->initial_block = src->initial_block;
+        rowmix_rounds = src->rowmix_rounds;
+        rowmix_seed = src->rowmix_seed;
+    } else {
+        // Seeded data in the reference's draw order (cuda/cuprym_cyclic.cu:2196-2199).
+        std::mt19937_64 gen(cyclic::seeded_sector_value(seed, sector));
+        c->row_precond = cyclic::random_vector(es.target_rows, c->p, gen, true);
+        c->col_precond = cyclic::random_vector(es.total_cols(), c->p, gen, true);
+        c->initial_block = cyclic::random_vector(es.total_cols() * num_v, c->p, gen, false);
+    }
     c->plan = cyclic::generate_rowmix_plan(es.target_rows, op, sector, c->p, rowmix_rounds, rowmix_seed);
     if (rowmix_rounds > 0) {
         c->precond = cyclic::composite_target_preconditioner(c->plan, c->row_precond, c->p);

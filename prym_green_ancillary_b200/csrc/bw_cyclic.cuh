@@ -34,6 +34,14 @@ struct ElimDev {
     const int32_t *R, *Bk;   // g x n, g x kdim (balanced)
 };
 
+// Preconditioners, initial block and row-mixing recipe of an existing WDM file
+// (kernel-vector recovery reopens the operator of the sequence it recovers from).
+struct CyclicSource {
+    std::vector<uint32_t> row_precond, col_precond, initial_block;
+    size_t rowmix_rounds = 0;
+    uint64_t rowmix_seed = 0;
+};
+
 struct CyclicCtx {
     int device = 0, sms = 0;
     bool host_only = false;
@@ -73,7 +81,8 @@ struct CyclicCtx {
     std::vector<size_t> pair_offsets;
 
     static CyclicCtx* open(const std::string& instance_path, const std::string& op, size_t sector, size_t num_v,
-                           uint64_t seed, size_t rowmix_rounds, uint64_t rowmix_seed, int dev);
+                           uint64_t seed, size_t rowmix_rounds, uint64_t rowmix_seed, int dev,
+                           const CyclicSource* src = nullptr);
     ~CyclicCtx();
 
     template <class T>
@@ -94,9 +103,18 @@ struct CyclicCtx {
     void generate(size_t nlen_target);
     void download_state(std::vector<uint32_t>& current, std::vector<uint32_t>& packed);
     void apply_host(int what, const uint32_t* in, uint32_t* out);
+    // kernel-vector recovery (bw_cyclic_recover.cu)
+    struct Recovery;
+    void recover(const std::vector<uint32_t>& generators, size_t generator_count, std::vector<uint32_t>& candidates,
+                 std::vector<uint32_t>& product, long long& runtime_ms);
     void require_device() const {
         if (host_only) throw Error("this context was opened host-only (device < 0)", 3);
     }
 };
 
+}  // namespace bw
+
+namespace bw {
+// --validate-rowmix self-check of an open context (cuda/cuprym_cyclic.cu:1970-2132).
+void validate_ctx(CyclicCtx& c, uint32_t columns);
 }  // namespace bw

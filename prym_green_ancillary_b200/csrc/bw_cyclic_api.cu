@@ -139,7 +139,12 @@ extern "C" int bw_cyclic_write_wdm(bw_cyclic* ctx, const char* wdm_path) {
 extern "C" int bw_cyclic_validate(bw_cyclic* ctx, uint32_t columns) {
     return guarded([&] {
         BW_REQUIRE(ctx, "bw_cyclic_validate: null context");
-        CyclicCtx& c = *ctx->impl;
+        validate_ctx(*ctx->impl, columns);
+    });
+}
+
+void bw::validate_ctx(CyclicCtx& c, uint32_t columns) {
+    {
         c.require_device();
         BW_CUDA(cudaSetDevice(c.device));
         const size_t cols = std::max<size_t>(1, std::min<size_t>(columns, 16));
@@ -176,7 +181,7 @@ extern "C" int bw_cyclic_validate(bw_cyclic* ctx, uint32_t columns) {
                                 ", <x,Sy>=" + std::to_string(right), 3);
         }
         std::cout << "Validation matched: eliminated square operator symmetry" << std::endl;
-    });
+    }
 }
 
 extern "C" uint64_t bw_cyclic_launch_count(const bw_cyclic* ctx) { return ctx ? ctx->impl->launches : 0; }

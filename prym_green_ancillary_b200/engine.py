@@ -83,6 +83,9 @@ SIGNATURES = {
     "bw_cyclic_launch_count": (_U64, [_VP]),
     "bw_file_read_text": (_INT, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "bw_project_noalloc": (_INT, [_VP, _VP, _U64, _U32, _U32, _U32, _VP, _INT, _VP]),
+    "bw_cyclic_recover": (_INT, [ctypes.c_char_p, ctypes.c_char_p, _U32, ctypes.c_char_p, ctypes.c_char_p,
+                                 ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64, _U64, _INT,
+                                 _INT, _INT, _INT]),
 }
 
 
