@@ -17,7 +17,9 @@ struct Value {
     enum Kind { Null, Bool, Number, String, Array, Object } kind = Null;
     bool b = false;
     bool is_int = false;
+    bool is_u64 = false;        // nonnegative integer above INT64_MAX (held in u)
     int64_t i = 0;
+    uint64_t u = 0;
     double d = 0;
     std::string s;
     std::vector<Value> arr;
@@ -39,6 +41,7 @@ struct Value {
         return i;
     }
     uint64_t as_u64(const std::string& label) const {
+        if (kind == Number && is_u64) return u;
         int64_t v = as_int(label);
         if (v < 0) throw std::runtime_error("expected a nonnegative integer for " + label);
         return static_cast<uint64_t>(v);
@@ -213,10 +216,17 @@ private:
             try {
                 v.i = std::stoll(text);
                 v.is_int = true;
+                v.d = static_cast<double>(v.i);
             } catch (const std::exception&) {
-                fail("integer out of range");
+                if (text[0] == '-') fail("integer out of range");
+                try {
+                    v.u = std::stoull(text);
+                    v.is_u64 = true;
+                    v.d = static_cast<double>(v.u);
+                } catch (const std::exception&) {
+                    fail("integer out of range");
+                }
             }
-            v.d = static_cast<double>(v.i);
         } else {
             v.d = std::stod(text);
         }
