@@ -521,8 +521,8 @@ void KoszulCtx::seq_start(const uint32_t* x, const uint32_t* y0, uint32_t* seq, 
     BW_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), st));
     if (form == BW_FORM_INT8) {
         i8_load_x(x, st);
-        i8_to_limbs(y0, i8_plane(0), i8_plane(1), n_src * nb, st);
-        i8_project(i8_plane(0), i8_plane(1), st);
+        i8_to_limbs(y0, I8_YA, st);
+        i8_project(I8_YA, st);
     } else {
         launch_to_balanced(x, d_xb, n_src * m, st);
         launch_to_balanced(y0, d_ya, n_src * nb, st);
@@ -584,7 +584,7 @@ void KoszulCtx::seq_finish(uint32_t* y_out, uint64_t* nlen_out, cudaStream_t st)
     BW_REQUIRE(in_session, "seq_finish: no sequence session");
     in_session = false;
     if (form == BW_FORM_INT8) {
-        if (y_out) i8_from_limbs(i8_plane(cur_is_a ? 0 : 2), i8_plane(cur_is_a ? 1 : 3), y_out, n_src * nb, st);
+        if (y_out) i8_from_limbs(cur_is_a ? I8_YA : I8_YB, y_out, st);
         BW_CUDA(cudaStreamSynchronize(st));
         i8_check_error();
     } else if (y_out) {
@@ -643,9 +643,9 @@ extern "C" int bw_koszul_forward(bw_koszul* ctx, const uint32_t* d_y, uint32_t* 
         BW_CUDA(cudaSetDevice(c.device));
         cudaStream_t st = pick_stream(&c, stream);
         if (c.form == BW_FORM_INT8) {
-            c.i8_to_limbs(d_y, c.i8_plane(0), c.i8_plane(1), c.n_src * c.nb, st);
-            c.i8_run(true, c.i8_plane(0), c.i8_plane(1), c.i8_plane(4), c.i8_plane(5), false, st);
-            c.i8_from_limbs(c.i8_plane(4), c.i8_plane(5), d_z, c.n_tgt * c.nb, st);
+            c.i8_to_limbs(d_y, KoszulCtx::I8_YA, st);
+            c.i8_run(true, KoszulCtx::I8_YA, KoszulCtx::I8_Z, false, st);
+            c.i8_from_limbs(KoszulCtx::I8_Z, d_z, st);
             BW_CUDA(cudaStreamSynchronize(st));
             c.i8_check_error();
             return;
@@ -665,9 +665,9 @@ extern "C" int bw_koszul_transpose(bw_koszul* ctx, const uint32_t* d_z, uint32_t
         BW_CUDA(cudaSetDevice(c.device));
         cudaStream_t st = pick_stream(&c, stream);
         if (c.form == BW_FORM_INT8) {
-            c.i8_to_limbs(d_z, c.i8_plane(4), c.i8_plane(5), c.n_tgt * c.nb, st);
-            c.i8_run(false, c.i8_plane(4), c.i8_plane(5), c.i8_plane(0), c.i8_plane(1), scale_by_diag != 0, st);
-            c.i8_from_limbs(c.i8_plane(0), c.i8_plane(1), d_w, c.n_src * c.nb, st);
+            c.i8_to_limbs(d_z, KoszulCtx::I8_Z, st);
+            c.i8_run(false, KoszulCtx::I8_Z, KoszulCtx::I8_YA, scale_by_diag != 0, st);
+            c.i8_from_limbs(KoszulCtx::I8_YA, d_w, st);
             BW_CUDA(cudaStreamSynchronize(st));
             c.i8_check_error();
             return;
@@ -686,10 +686,10 @@ extern "C" int bw_koszul_apply(bw_koszul* ctx, const uint32_t* d_y, uint32_t* d_
         BW_CUDA(cudaSetDevice(c.device));
         cudaStream_t st = pick_stream(&c, stream);
         if (c.form == BW_FORM_INT8) {
-            c.i8_to_limbs(d_y, c.i8_plane(0), c.i8_plane(1), c.n_src * c.nb, st);
-            c.i8_run(true, c.i8_plane(0), c.i8_plane(1), c.i8_plane(4), c.i8_plane(5), false, st);
-            c.i8_run(false, c.i8_plane(4), c.i8_plane(5), c.i8_plane(2), c.i8_plane(3), true, st);
-            c.i8_from_limbs(c.i8_plane(2), c.i8_plane(3), d_out, c.n_src * c.nb, st);
+            c.i8_to_limbs(d_y, KoszulCtx::I8_YA, st);
+            c.i8_run(true, KoszulCtx::I8_YA, KoszulCtx::I8_Z, false, st);
+            c.i8_run(false, KoszulCtx::I8_Z, KoszulCtx::I8_YB, true, st);
+            c.i8_from_limbs(KoszulCtx::I8_YB, d_out, st);
             BW_CUDA(cudaStreamSynchronize(st));
             c.i8_check_error();
             return;
@@ -764,12 +764,13 @@ extern "C" int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* m
         for (uint64_t s = 0; s < steps; ++s) {
             BW_CUDA(cudaEventRecord(ev[4 * s], st));
             if (c.form == BW_FORM_INT8) {
-                const int a = c.cur_is_a ? 0 : 2, b = c.cur_is_a ? 2 : 0;
-                c.i8_run(true, c.i8_plane(a), c.i8_plane(a + 1), c.i8_plane(4), c.i8_plane(5), false, st);
+                const int a = c.cur_is_a ? KoszulCtx::I8_YA : KoszulCtx::I8_YB;
+                const int b = c.cur_is_a ? KoszulCtx::I8_YB : KoszulCtx::I8_YA;
+                c.i8_run(true, a, KoszulCtx::I8_Z, false, st);
                 BW_CUDA(cudaEventRecord(ev[4 * s + 1], st));
-                c.i8_run(false, c.i8_plane(4), c.i8_plane(5), c.i8_plane(b), c.i8_plane(b + 1), true, st);
+                c.i8_run(false, KoszulCtx::I8_Z, b, true, st);
                 BW_CUDA(cudaEventRecord(ev[4 * s + 2], st));
-                c.i8_project(c.i8_plane(b), c.i8_plane(b + 1), st);
+                c.i8_project(b, st);
             } else {
                 int32_t* src = c.cur_is_a ? c.d_ya : c.d_yb;
                 int32_t* dst = c.cur_is_a ? c.d_yb : c.d_ya;

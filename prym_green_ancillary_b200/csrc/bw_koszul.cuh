@@ -80,15 +80,16 @@ struct KoszulCtx {
     void i8_forward(const int32_t* y, int32_t* z, cudaStream_t st);
     void i8_transpose(const int32_t* z, int32_t* w, bool scale, cudaStream_t st);
     uint64_t i8_kernels_per_step() const;
-    void i8_run(bool forward_dir, const int8_t* in_lo, const int8_t* in_hi, int8_t* out_lo, int8_t* out_hi,
-                bool scale, cudaStream_t st);
+    enum { I8_YA = 0, I8_YB = 1, I8_Z = 2 };   // limb-plane block arrays
+    void i8_run(bool forward_dir, int in_buf, int out_buf, bool scale, cudaStream_t st);
     void i8_check_error();
-    void i8_to_limbs(const uint32_t* in, int8_t* lo, int8_t* hi, uint64_t count, cudaStream_t st);
-    void i8_from_limbs(const int8_t* lo, const int8_t* hi, uint32_t* out, uint64_t count, cudaStream_t st);
+    void i8_to_limbs(const uint32_t* in, int buf, cudaStream_t st);
+    void i8_from_limbs(int buf, uint32_t* out, cudaStream_t st);
     void i8_load_x(const uint32_t* x, cudaStream_t st);
-    void i8_project(const int8_t* lo, const int8_t* hi, cudaStream_t st);
+    void i8_project(int buf, cudaStream_t st);
     void i8_step_once(cudaStream_t st);
-    int8_t* i8_plane(int which);   // 0/1: Y_a lo/hi, 2/3: Y_b lo/hi, 4/5: Z lo/hi
+    int i8_dim(int buf) const;
+    uint64_t i8_rows(int buf) const;
 };
 
 }  // namespace bw

@@ -11,7 +11,7 @@
 // with A[(blk, j)][(i, u)] = sign * in[nbr(blk, i)][u][j] (zero when the
 // generator i is not incident to blk) and Bm = the r maps side by side.  The
 // tile is an M = 128 GEMM: A = the gathered input blocks (MN-major in shared
-// memory: one input block row of n limbs is one 16-byte core-matrix row),
+// memory: 16 limbs of one input row form one 16-byte core-matrix row),
 // B = the maps' lo and hi limbs stacked along N (K-major, resident in shared
 // memory for the whole kernel), K = r * inner in steps of 32.  Two MMAs per
 // K-step (A = input lo limbs, A = input hi limbs) give four int32 partial
@@ -19,15 +19,24 @@
 //   x*m = lo*lo + 255*(lo*hi + hi*lo) + 255^2*hi*hi.
 // int32 accumulation is exact: |K * 127 * 127| < 2^24 for K <= 1024.
 //
+// Limb planes in HBM: four planes per block array (lo, hi, -lo, -hi), each
+// laid out [blk][h][u][16 bytes] (h = j / 16), so that every (block, h) is one
+// contiguous run of inner * 16 bytes.  The producer therefore fills a stage
+// with one bulk copy (cp.async.bulk) per (limb, block, generator, h): from the
+// +plane or the -plane by the Koszul sign, or from a zero buffer when the
+// generator is absent.  The epilogue writes all four planes of its output.
+//
 // Warp roles (persistent, one CTA per SM):
-//   warps 0-3  producers: load limb rows, negate where the Koszul sign is -1,
-//              store them into the stage's A tile (zero rows for absent i);
-//   warp 4     allocates TMEM and issues tcgen05.mma / tcgen05.commit;
-//   warps 5-8  epilogue: tcgen05.ld the four partials, recombine, reduce mod p,
+//   warp 0     producer: per tile, stages the tile's incidence rows in shared
+//              memory; per stage, one elected lane posts the stage's byte count
+//              and the 32 lanes issue the bulk copies;
+//   warp 1     allocates TMEM and issues tcgen05.mma / tcgen05.commit;
+//   warps 2-5  epilogue: tcgen05.ld the four partials, recombine, reduce mod p,
 //              scale by D (d^T only), split into limbs and store.
-// Stages are tracked with mbarriers; accumulators are double-buffered in TMEM.
-// Every wait is bounded: on a timeout the kernel records an error code, all
-// roles wind down, in-flight MMAs are drained and TMEM is freed.
+// Stages are tracked with mbarriers (byte-count completion for the copies);
+// accumulators are double-buffered in TMEM.  Every wait is bounded: on a
+// timeout the kernel records an error code, all roles wind down, in-flight
+// MMAs are drained and TMEM is freed.
 #include "bw_koszul.cuh"
 #include "tc_sm100.cuh"
 
@@ -40,16 +49,19 @@ namespace bw {
 namespace {
 
 constexpr uint32_t kAbsent = 0xFFFFFFFFu;
-constexpr int kProducerWarps = 4;
-constexpr int kMmaWarp = 4;
-constexpr int kI8Threads = 9 * 32;
+constexpr int kProducerWarp = 0;
+constexpr int kMmaWarp = 1;
+constexpr int kI8Threads = 6 * 32;
 constexpr int kMaxSmem = 227 * 1024;
+constexpr int kMaxIncPerTile = 512;   // BT * r words of shared memory for the tile's incidence rows
+
+// Plane index inside a four-plane block array.
+enum : int { PL_LO = 0, PL_HI = 1, PL_NLO = 2, PL_NHI = 3 };
 
 struct I8Dir {
-    const int8_t* in_lo;
-    const int8_t* in_hi;
-    int8_t* out_lo;
-    int8_t* out_hi;
+    const int8_t* in[4];      // input planes lo, hi, -lo, -hi: [blk][h][inner][16]
+    int8_t* out[4];           // output planes, same layout with `outer`
+    const int8_t* zeros;      // at least inner * 16 zero bytes
     const uint32_t* inc;      // [n_blk][r]: neighbour rank | negative << 31, or kAbsent
     const int8_t* b_tiles;    // B operand, already in its shared-memory layout
     const int32_t* diag;      // nullptr, or [n_blk * outer] balanced (scales the output)
@@ -73,18 +85,23 @@ __device__ __forceinline__ int32_t combine(int32_t ll, int32_t lhhl, int32_t hh,
     return reduce_balanced(a + P.c1 * b + P.c2 * c, P.mod);
 }
 
-__device__ __forceinline__ void split_limbs(int32_t v, int8_t& lo, int8_t& hi) {
+__host__ __device__ __forceinline__ void split_limbs(int32_t v, int8_t& lo, int8_t& hi) {
     // v in [-16383, 16383]: q = floor((v + 127) / 255), lo = v - 255 q in [-127, 127]
     const int32_t q = static_cast<int32_t>(static_cast<uint32_t>(v + 127 + 255 * 128) / 255u) - 128;
     lo = static_cast<int8_t>(v - 255 * q);
     hi = static_cast<int8_t>(q);
 }
 
+// Byte offset of element (row = blk * dim + u, column j) in a plane of width NB.
+__host__ __device__ __forceinline__ long long plane_offset(long long blk, int u, int j, int dim, int NB) {
+    return blk * (static_cast<long long>(NB) * dim) + static_cast<long long>(j >> 4) * dim * 16 + u * 16 + (j & 15);
+}
+
 template <int NB>
 __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int BT = 128 / NB;        // output blocks per tile
-    constexpr int HG = NB / 16;         // 16-byte chunks per input block row
+    constexpr int HG = NB / 16;         // 16-byte column groups per block row
     const int N = 2 * P.half;
     uint8_t* sB = smem;
     uint8_t* sA = smem + P.b_bytes;
@@ -94,6 +111,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
     uint64_t* accempty = accfull + 2;
     uint64_t* drained = accempty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
+    uint32_t* sInc = tmem_slot + 4;     // BT * r incidence words of the producer's current tile
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const long long n_tiles = (P.n_blk + BT - 1) / BT;
@@ -104,7 +122,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
     tc::fence_proxy_async_smem();
     if (threadIdx.x == 0) {
         for (int s = 0; s < P.slots; ++s) {
-            tc::mbar_init(&full[s], kProducerWarps * 32);
+            tc::mbar_init(&full[s], 1);
             tc::mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -123,53 +141,55 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    const int KS = P.gi * P.inner;                       // K' rows of a slot
+    const uint32_t block_bytes = static_cast<uint32_t>(P.inner) * 16;
 
-    if (warp < kProducerWarps) {
-        // ------------------------------------------------------------ producers
+    if (warp == kProducerWarp) {
+        // ------------------------------------------------------------ producer
         long long it = 0;
         bool ok = true;
         for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
-            for (int s = 0; s < P.stages_per_tile && ok; ++s, ++it) {
+            __syncwarp();
+            for (int e = lane; e < BT * P.r; e += 32) {
+                const int t = e / P.r;
+                const long long blk = tile * BT + t;
+                sInc[e] = blk < P.n_blk ? __ldg(P.inc + blk * P.r + (e - t * P.r)) : kAbsent;
+            }
+            __syncwarp();
+            for (int s = 0; s < P.stages_per_tile; ++s, ++it) {
                 const int slot = static_cast<int>(it % P.slots);
                 const uint32_t ph = static_cast<uint32_t>((it / P.slots) & 1);
-                if (!tc::mbar_wait(&empty[slot], ph ^ 1u, P.err, tc::ERR_WAIT_EMPTY)) {
+                int got = 1;
+                if (lane == 0) got = tc::mbar_wait(&empty[slot], ph ^ 1u, P.err, tc::ERR_WAIT_EMPTY) ? 1 : 0;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) {
                     ok = false;
                     break;
                 }
                 const int g_s = min(P.gi, P.r - s * P.gi);
-                const int KS = P.gi * P.inner;     // K' extent of a slot
+                const int nblocks = 2 * BT * g_s * HG;     // (limb, t, il, h)
+                if (lane == 0) tc::mbar_arrive_expect_tx(&full[slot], static_cast<uint32_t>(nblocks) * block_bytes);
+                __syncwarp();
                 uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
-                const int nblocks = 2 * BT * g_s;
-                const int chunks = P.inner * HG;
-                for (int bi = warp; bi < nblocks; bi += kProducerWarps) {
-                    const int limb = bi / (BT * g_s);
-                    const int rem = bi - limb * BT * g_s;
-                    const int t = rem / g_s;
-                    const int il = rem - t * g_s;
-                    const long long blk = tile * BT + t;
-                    const uint32_t e = blk < P.n_blk ? __ldg(P.inc + blk * P.r + s * P.gi + il) : kAbsent;
-                    const int8_t* plane = limb ? P.in_hi : P.in_lo;
-                    uint8_t* dst0 = slotA + static_cast<size_t>(limb) * P.limb_bytes;
-                    for (int w = lane; w < chunks; w += 32) {
-                        const int b = w / HG, h = w - b * HG;
-                        uint8_t* dst = dst0 + static_cast<size_t>(t * HG + h) * KS * 16 +
-                                       static_cast<size_t>(il * P.inner + b) * 16;
-                        int4 v = make_int4(0, 0, 0, 0);
-                        if (e != kAbsent) {
-                            const long long src_blk = static_cast<long long>(e & 0x7FFFFFFFu);
-                            v = __ldg(reinterpret_cast<const int4*>(plane + (src_blk * P.inner + b) * NB + h * 16));
-                            if (e >> 31) {
-                                v.x = static_cast<int>(__vsub4(0u, static_cast<unsigned>(v.x)));
-                                v.y = static_cast<int>(__vsub4(0u, static_cast<unsigned>(v.y)));
-                                v.z = static_cast<int>(__vsub4(0u, static_cast<unsigned>(v.z)));
-                                v.w = static_cast<int>(__vsub4(0u, static_cast<unsigned>(v.w)));
-                            }
-                        }
-                        *reinterpret_cast<int4*>(dst) = v;
+                for (int bi = lane; bi < nblocks; bi += 32) {
+                    const int h = bi % HG;
+                    const int rest = bi / HG;
+                    const int il = rest % g_s;
+                    const int rest2 = rest / g_s;
+                    const int t = rest2 % BT;
+                    const int limb = rest2 / BT;
+                    const uint32_t e = sInc[t * P.r + s * P.gi + il];
+                    const int8_t* src;
+                    if (e == kAbsent) {
+                        src = P.zeros;
+                    } else {
+                        const long long nbr = static_cast<long long>(e & 0x7FFFFFFFu);
+                        src = P.in[limb + ((e >> 31) ? 2 : 0)] + (nbr * HG + h) * block_bytes;
                     }
+                    uint8_t* dst = slotA + static_cast<size_t>(limb) * P.limb_bytes +
+                                   static_cast<size_t>(t * HG + h) * KS * 16 + static_cast<size_t>(il) * block_bytes;
+                    tc::bulk_g2s(dst, src, block_bytes, &full[slot]);
                 }
-                tc::fence_proxy_async_smem();
-                tc::mbar_arrive(&full[slot]);
             }
         }
     } else if (warp == kMmaWarp) {
@@ -177,7 +197,6 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_i8(128, N, true, false);
             const uint32_t sA0 = tc::smem_u32(sA), sB0 = tc::smem_u32(sB);
-            const int KS = P.gi * P.inner;
             long long it = 0, tcount = 0;
             bool ok = true;
             for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
@@ -244,12 +263,14 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                         const int o = o0 + oo;
                         if (o < P.outer) {
                             int32_t v = combine(ll[oo], lh[oo] + hl[oo], hh[oo], P);
-                            const long long row = blk * P.outer + o;
-                            if (P.diag) v = reduce_balanced(v * __ldg(P.diag + row), P.mod);
+                            if (P.diag) v = reduce_balanced(v * __ldg(P.diag + blk * P.outer + o), P.mod);
                             int8_t lo, hi;
                             split_limbs(v, lo, hi);
-                            P.out_lo[row * NB + j] = lo;
-                            P.out_hi[row * NB + j] = hi;
+                            const long long off = plane_offset(blk, o, j, P.outer, NB);
+                            P.out[PL_LO][off] = lo;
+                            P.out[PL_HI][off] = hi;
+                            P.out[PL_NLO][off] = static_cast<int8_t>(-lo);
+                            P.out[PL_NHI][off] = static_cast<int8_t>(-hi);
                         }
                     }
                 }
@@ -269,22 +290,37 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
 
 // ---- limb conversions and the projection on limb planes
 
+// canonical row-major (rows = n_blk * dim, NB columns) -> four planes
+template <int NB>
 __global__ void to_limbs_kernel(const uint32_t* __restrict__ in, int8_t* __restrict__ lo, int8_t* __restrict__ hi,
-                                long long count, Mod mod) {
+                                int8_t* __restrict__ nlo, int8_t* __restrict__ nhi, long long count, int dim,
+                                Mod mod) {
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
         int8_t a, b;
         split_limbs(to_balanced(in[i] % static_cast<uint32_t>(mod.p), mod), a, b);
-        lo[i] = a;
-        hi[i] = b;
+        const long long row = i / NB;
+        const int j = static_cast<int>(i - row * NB);
+        const long long blk = row / dim;
+        const long long off = plane_offset(blk, static_cast<int>(row - blk * dim), j, dim, NB);
+        lo[off] = a;
+        hi[off] = b;
+        nlo[off] = static_cast<int8_t>(-a);
+        nhi[off] = static_cast<int8_t>(-b);
     }
 }
 
+template <int NB>
 __global__ void from_limbs_kernel(const int8_t* __restrict__ lo, const int8_t* __restrict__ hi,
-                                  uint32_t* __restrict__ out, long long count, Mod mod) {
+                                  uint32_t* __restrict__ out, long long count, int dim, Mod mod) {
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
-         i += static_cast<long long>(gridDim.x) * blockDim.x)
-        out[i] = to_canonical(255 * static_cast<int32_t>(hi[i]) + lo[i], mod);
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long row = i / NB;
+        const int j = static_cast<int>(i - row * NB);
+        const long long blk = row / dim;
+        const long long off = plane_offset(blk, static_cast<int>(row - blk * dim), j, dim, NB);
+        out[i] = to_canonical(255 * static_cast<int32_t>(hi[off]) + lo[off], mod);
+    }
 }
 
 __global__ void to_int16_kernel(const uint32_t* __restrict__ in, int16_t* __restrict__ out, long long count,
@@ -300,11 +336,11 @@ __device__ __forceinline__ int32_t limb_value(uint32_t lo4, uint32_t hi4, int k)
     return 255 * hi + lo;
 }
 
-// a = X^T W into seq[*seq_index]; X int16 balanced (rows x m), W as limb planes (rows x n).
+// a = X^T W into seq[*seq_index]; X int16 balanced (rows x m), W as limb planes.
 template <int NB>
 __global__ void __launch_bounds__(256) i8_project_kernel(
     const int16_t* __restrict__ X, const int8_t* __restrict__ Wlo, const int8_t* __restrict__ Whi, long long rows,
-    int m, int32_t* __restrict__ partials, unsigned int* __restrict__ counter, uint32_t* __restrict__ seq,
+    int dim, int m, int32_t* __restrict__ partials, unsigned int* __restrict__ counter, uint32_t* __restrict__ seq,
     unsigned long long* __restrict__ seq_index, Mod mod) {
     constexpr int JG = NB / 4;
     const int tps = m * JG;
@@ -319,9 +355,11 @@ __global__ void __launch_bounds__(256) i8_project_kernel(
     int cnt = 0;
     for (long long row = static_cast<long long>(blockIdx.x) * slices + slice; row < rows;
          row += static_cast<long long>(gridDim.x) * slices) {
+        const long long blk = row / dim;
+        const long long off = plane_offset(blk, static_cast<int>(row - blk * dim), jg * 4, dim, NB);
         const int32_t xv = __ldg(X + row * m + x);
-        const uint32_t lo4 = __ldg(reinterpret_cast<const uint32_t*>(Wlo + row * NB) + jg);
-        const uint32_t hi4 = __ldg(reinterpret_cast<const uint32_t*>(Whi + row * NB) + jg);
+        const uint32_t lo4 = __ldg(reinterpret_cast<const uint32_t*>(Wlo + off));
+        const uint32_t hi4 = __ldg(reinterpret_cast<const uint32_t*>(Whi + off));
 #pragma unroll
         for (int k = 0; k < 4; ++k) acc[k] += xv * limb_value(lo4, hi4, k);
         if (++cnt == 8) {
@@ -379,10 +417,13 @@ int gcd_int(int a, int b) {
     return a;
 }
 
-void host_split(int32_t v, int8_t& lo, int8_t& hi) {
-    const int32_t q = static_cast<int32_t>(static_cast<uint32_t>(v + 127 + 255 * 128) / 255u) - 128;
-    lo = static_cast<int8_t>(v - 255 * q);
-    hi = static_cast<int8_t>(q);
+template <class F>
+void dispatch_i8_nb(int nb, F&& f) {
+    switch (nb) {
+        case 16: f(std::integral_constant<int, 16>{}); break;
+        case 32: f(std::integral_constant<int, 32>{}); break;
+        default: throw Error("INT8 form supports block widths 16 and 32", 1);
+    }
 }
 
 }  // namespace
@@ -396,7 +437,8 @@ struct KoszulCtx::I8State {
         size_t smem = 0;
         unsigned grid = 0;
     } fwd, bwd;
-    int8_t *ya_lo = nullptr, *ya_hi = nullptr, *yb_lo = nullptr, *yb_hi = nullptr, *z_lo = nullptr, *z_hi = nullptr;
+    int8_t* planes[3][4] = {};     // Y_a, Y_b, Z: lo, hi, -lo, -hi
+    int8_t* zeros = nullptr;
     int16_t* x16 = nullptr;
     int* err = nullptr;
 };
@@ -413,7 +455,6 @@ void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     const int N = 2 * P.half;
     BW_REQUIRE(N <= 256, "INT8 form: output dimension above 128 is not supported");
     const int base_g = 32 / gcd_int(inner, 32);
-    BW_REQUIRE(base_g <= c.r || true, "");
     // grow the stage towards ~40 KB of A per slot
     int gi = base_g;
     auto slot_bytes_for = [&](int g) { return static_cast<size_t>(2) * 8 * (g * inner) * 16; };
@@ -427,14 +468,15 @@ void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     P.b_bytes = static_cast<uint32_t>(total_ks) * N * 32;
     P.limb_bytes = static_cast<uint32_t>(8 * gi * inner * 16);
     P.slot_bytes = 2 * P.limb_bytes;
-    const size_t bars = (2 * 8 + 2 * 2 + 1) * 8 + 16;
+    BW_REQUIRE(P.slot_bytes / 16 < 4096 || true, "");
+    const size_t extra = (2 * 8 + 2 * 2 + 1) * 8 + 16 + kMaxIncPerTile * 4;
     int slots = 4;
-    while (slots > 1 && P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + bars > static_cast<size_t>(kMaxSmem))
+    while (slots > 1 && P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra > static_cast<size_t>(kMaxSmem))
         --slots;
-    BW_REQUIRE(P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + bars <= static_cast<size_t>(kMaxSmem),
+    BW_REQUIRE(P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra <= static_cast<size_t>(kMaxSmem),
                "INT8 form: maps too large for shared memory");
     P.slots = slots;
-    D.smem = P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + bars;
+    D.smem = P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra;
     P.mod = c.mod;
     P.c1 = to_balanced(255u % c.p, c.mod);
     P.c2 = to_balanced(static_cast<uint32_t>((255ull * 255ull) % c.p), c.mod);
@@ -444,7 +486,6 @@ void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     std::vector<int8_t> B(P.b_bytes, 0);
     const int kp_total = total_ks * 32;
     for (int kp = 0; kp < kp_total; ++kp) {
-        // K' of global K-step: stages are exact multiples of 32 except the last
         const int s = std::min(kp / (P.ks_full * 32), P.stages_per_tile - 1);
         const int local = kp - s * P.ks_full * 32;
         const int gen_local = local / inner, u = local % inner;
@@ -458,7 +499,7 @@ void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
                                      ? c.maps_canonical[(static_cast<size_t>(i) * c.co + u) * c.ci + o]
                                      : c.maps_canonical[(static_cast<size_t>(i) * c.co + o) * c.ci + u];
             int8_t lo, hi;
-            host_split(to_balanced(raw % c.p, c.mod), lo, hi);
+            split_limbs(to_balanced(raw % c.p, c.mod), lo, hi);
             const int ks = kp / 32, kk = kp % 32;
             const size_t off = static_cast<size_t>(ks) * N * 32 + (n / 8) * 256 + (kk / 16) * 128 + (n % 8) * 16 + (kk % 16);
             B[off] = n < P.half ? lo : hi;
@@ -477,15 +518,6 @@ void launch_i8(KoszulCtx& c, KoszulCtx::I8State::Dir& D, cudaStream_t st) {
     ++c.launches;
 }
 
-template <class F>
-void dispatch_i8_nb(int nb, F&& f) {
-    switch (nb) {
-        case 16: f(std::integral_constant<int, 16>{}); break;
-        case 32: f(std::integral_constant<int, 32>{}); break;
-        default: throw Error("INT8 form supports block widths 16 and 32", 1);
-    }
-}
-
 }  // namespace
 
 void KoszulCtx::i8_destroy() {
@@ -497,6 +529,7 @@ void KoszulCtx::i8_setup() {
     BW_REQUIRE(nb == 16 || nb == 32, "INT8 form supports block widths 16 and 32");
     BW_REQUIRE(ci <= 128 && co <= 128, "INT8 form: dim_in and dim_out must be at most 128");
     BW_REQUIRE(static_cast<long long>(r) * std::max(ci, co) <= 1024, "INT8 form: r * dim above 1024 (int32 bound)");
+    BW_REQUIRE((128 / nb) * r <= kMaxIncPerTile, "INT8 form: too many generators for one tile");
     int major = 0;
     BW_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
     BW_REQUIRE(major == 10, "INT8 form needs an sm_100 GPU (tcgen05)");
@@ -529,25 +562,24 @@ void KoszulCtx::i8_setup() {
     S.bwd.inc = alloc<uint32_t>(bwd.size());
     BW_CUDA(cudaMemcpyAsync(S.fwd.inc, fwd.data(), fwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
     BW_CUDA(cudaMemcpyAsync(S.bwd.inc, bwd.data(), bwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
-    S.ya_lo = alloc<int8_t>(n_src * nb);
-    S.ya_hi = alloc<int8_t>(n_src * nb);
-    S.yb_lo = alloc<int8_t>(n_src * nb);
-    S.yb_hi = alloc<int8_t>(n_src * nb);
-    S.z_lo = alloc<int8_t>(n_tgt * nb);
-    S.z_hi = alloc<int8_t>(n_tgt * nb);
+    for (int b = 0; b < 3; ++b)
+        for (int pl = 0; pl < 4; ++pl) S.planes[b][pl] = alloc<int8_t>((b < 2 ? n_src : n_tgt) * nb);
+    const size_t zbytes = static_cast<size_t>(std::max(ci, co)) * 16;
+    S.zeros = alloc<int8_t>(zbytes);
+    BW_CUDA(cudaMemsetAsync(S.zeros, 0, zbytes, own_stream));
     S.x16 = alloc<int16_t>(n_src * m);
     S.err = alloc<int>(1);
     BW_CUDA(cudaMemsetAsync(S.err, 0, sizeof(int), own_stream));
     plan_direction(*this, S.fwd, ci, co, false);
     plan_direction(*this, S.bwd, co, ci, true);
+    for (I8State::Dir* D : {&S.fwd, &S.bwd}) {
+        D->p.zeros = S.zeros;
+        D->p.err = S.err;
+    }
     S.fwd.p.inc = S.fwd.inc;
     S.bwd.p.inc = S.bwd.inc;
     S.fwd.p.n_blk = static_cast<long long>(n_t);
     S.bwd.p.n_blk = static_cast<long long>(n_s);
-    S.fwd.p.err = S.err;
-    S.bwd.p.err = S.err;
-    S.fwd.p.diag = nullptr;
-    S.bwd.p.diag = d_diag;
     dispatch_i8_nb(nb, [&](auto NBc) {
         auto kern = i8_gather_gemm_kernel<decltype(NBc)::value>;
         const int need = static_cast<int>(std::max(S.fwd.smem, S.bwd.smem));
@@ -556,18 +588,17 @@ void KoszulCtx::i8_setup() {
     const int bt = 128 / nb;
     S.fwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_t + bt - 1) / bt, sms)));
     S.bwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_s + bt - 1) / bt, sms)));
+    BW_CUDA(cudaStreamSynchronize(own_stream));
 }
 
 uint64_t KoszulCtx::i8_kernels_per_step() const { return 3; }
 
-// Limb-plane forward / transpose used by the sequence path.
-void KoszulCtx::i8_run(bool forward_dir, const int8_t* in_lo, const int8_t* in_hi, int8_t* out_lo, int8_t* out_hi,
-                       bool scale, cudaStream_t st) {
+void KoszulCtx::i8_run(bool forward_dir, int in_buf, int out_buf, bool scale, cudaStream_t st) {
     I8State::Dir& D = forward_dir ? i8->fwd : i8->bwd;
-    D.p.in_lo = in_lo;
-    D.p.in_hi = in_hi;
-    D.p.out_lo = out_lo;
-    D.p.out_hi = out_hi;
+    for (int pl = 0; pl < 4; ++pl) {
+        D.p.in[pl] = i8->planes[in_buf][pl];
+        D.p.out[pl] = i8->planes[out_buf][pl];
+    }
     D.p.diag = (!forward_dir && scale) ? d_diag : nullptr;
     dispatch_i8_nb(nb, [&](auto NBc) { launch_i8<decltype(NBc)::value>(*this, D, st); });
 }
@@ -581,16 +612,29 @@ void KoszulCtx::i8_check_error() {
     }
 }
 
-void KoszulCtx::i8_to_limbs(const uint32_t* in, int8_t* lo, int8_t* hi, uint64_t count, cudaStream_t st) {
+int KoszulCtx::i8_dim(int buf) const { return buf == I8_Z ? co : ci; }
+uint64_t KoszulCtx::i8_rows(int buf) const { return buf == I8_Z ? n_tgt : n_src; }
+
+void KoszulCtx::i8_to_limbs(const uint32_t* in, int buf, cudaStream_t st) {
+    const uint64_t count = i8_rows(buf) * nb;
     unsigned grid = static_cast<unsigned>(std::min<uint64_t>((count + 255) / 256, static_cast<uint64_t>(sms) * 8));
-    to_limbs_kernel<<<std::max(grid, 1u), 256, 0, st>>>(in, lo, hi, static_cast<long long>(count), mod);
+    int8_t** pl = i8->planes[buf];
+    dispatch_i8_nb(nb, [&](auto NBc) {
+        to_limbs_kernel<decltype(NBc)::value><<<std::max(grid, 1u), 256, 0, st>>>(
+            in, pl[0], pl[1], pl[2], pl[3], static_cast<long long>(count), i8_dim(buf), mod);
+    });
     BW_CHECK_LAUNCH();
     ++launches;
 }
 
-void KoszulCtx::i8_from_limbs(const int8_t* lo, const int8_t* hi, uint32_t* out, uint64_t count, cudaStream_t st) {
+void KoszulCtx::i8_from_limbs(int buf, uint32_t* out, cudaStream_t st) {
+    const uint64_t count = i8_rows(buf) * nb;
     unsigned grid = static_cast<unsigned>(std::min<uint64_t>((count + 255) / 256, static_cast<uint64_t>(sms) * 8));
-    from_limbs_kernel<<<std::max(grid, 1u), 256, 0, st>>>(lo, hi, out, static_cast<long long>(count), mod);
+    int8_t** pl = i8->planes[buf];
+    dispatch_i8_nb(nb, [&](auto NBc) {
+        from_limbs_kernel<decltype(NBc)::value><<<std::max(grid, 1u), 256, 0, st>>>(
+            pl[0], pl[1], out, static_cast<long long>(count), i8_dim(buf), mod);
+    });
     BW_CHECK_LAUNCH();
     ++launches;
 }
@@ -603,10 +647,11 @@ void KoszulCtx::i8_load_x(const uint32_t* x, cudaStream_t st) {
     ++launches;
 }
 
-void KoszulCtx::i8_project(const int8_t* lo, const int8_t* hi, cudaStream_t st) {
+void KoszulCtx::i8_project(int buf, cudaStream_t st) {
     dispatch_i8_nb(nb, [&](auto NBc) {
         i8_project_kernel<decltype(NBc)::value><<<proj_grid, 256, 0, st>>>(
-            i8->x16, lo, hi, static_cast<long long>(n_src), m, d_partials, d_counter, d_seq, d_seq_index, mod);
+            i8->x16, i8->planes[buf][0], i8->planes[buf][1], static_cast<long long>(n_src), ci, m, d_partials,
+            d_counter, d_seq, d_seq_index, mod);
     });
     BW_CHECK_LAUNCH();
     ++launches;
@@ -614,25 +659,11 @@ void KoszulCtx::i8_project(const int8_t* lo, const int8_t* hi, cudaStream_t st) 
 
 // One INT8 step on the limb state: cur -> other, append a_i.
 void KoszulCtx::i8_step_once(cudaStream_t st) {
-    I8State& S = *i8;
-    int8_t* slo = cur_is_a ? S.ya_lo : S.yb_lo;
-    int8_t* shi = cur_is_a ? S.ya_hi : S.yb_hi;
-    int8_t* dlo = cur_is_a ? S.yb_lo : S.ya_lo;
-    int8_t* dhi = cur_is_a ? S.yb_hi : S.ya_hi;
-    i8_run(true, slo, shi, S.z_lo, S.z_hi, false, st);
-    i8_run(false, S.z_lo, S.z_hi, dlo, dhi, true, st);
-    i8_project(dlo, dhi, st);
+    const int src = cur_is_a ? I8_YA : I8_YB, dst = cur_is_a ? I8_YB : I8_YA;
+    i8_run(true, src, I8_Z, false, st);
+    i8_run(false, I8_Z, dst, true, st);
+    i8_project(dst, st);
     cur_is_a = !cur_is_a;
-}
-int8_t* KoszulCtx::i8_plane(int which) {
-    switch (which) {
-        case 0: return i8->ya_lo;
-        case 1: return i8->ya_hi;
-        case 2: return i8->yb_lo;
-        case 3: return i8->yb_hi;
-        case 4: return i8->z_lo;
-        default: return i8->z_hi;
-    }
 }
 
 void KoszulCtx::i8_forward(const int32_t*, int32_t*, cudaStream_t) {

@@ -134,13 +134,13 @@ def _check_sampled_rows(shape, maps, diag, y, out, count, seed):
 
 
 def _projection(x, w, p):
-    # exact int64 X^T W on the host, chunk by chunk (products < 2^30, 2^20 rows per chunk < 2^50)
-    acc = np.zeros((x.shape[1], w.shape[1]), dtype=np.int64)
-    for s in range(0, x.shape[0], 1 << 20):
-        xn = x[s:s + (1 << 20)].cpu().numpy().astype(np.int64)
-        wn = w[s:s + (1 << 20)].cpu().numpy().astype(np.int64)
-        acc = (acc + xn.T @ wn) % p
-    return acc.astype(np.uint32)
+    """Exact X^T W mod p on the GPU in float64: residues are below 2^15, so a
+    product is below 2^30 and a chunk of 2^21 rows sums below 2^51 < 2^53."""
+    acc = torch.zeros((x.shape[1], w.shape[1]), dtype=torch.float64, device=x.device)
+    for s in range(0, x.shape[0], 1 << 21):
+        part = x[s:s + (1 << 21)].to(torch.float64).T @ w[s:s + (1 << 21)].to(torch.float64)
+        acc = torch.remainder(acc + torch.remainder(part, p), p)
+    return acc.to(torch.int64).cpu().numpy().astype(np.uint32)
 
 
 @pytest.mark.parametrize("form", FORMS)
