@@ -6,8 +6,10 @@
  * 2 = CUDA error, 3 = failed precondition); bw_last_error() then returns the
  * message (thread-local, valid until the next failing call on that thread).
  * No exception crosses this boundary.  Pointers documented as "device" are
- * CUDA device pointers of the context's device; "stream" is a cudaStream_t
- * (NULL = the context's own stream).
+ * CUDA device pointers of the context's device; "stream" is a cudaStream_t.
+ * A NULL stream orders the call like the legacy default stream (the work runs
+ * on the context's own stream after everything already issued on the legacy
+ * stream, and later legacy-stream work waits for it).
  *
  * Residues are canonical uint32 values in [0, p); blocks are row-major
  * (row * width + column), the layout of the reference's dense blocks

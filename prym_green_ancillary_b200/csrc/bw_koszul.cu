@@ -345,6 +345,7 @@ KoszulCtx::~KoszulCtx() {
     for (auto& g : graphs)
         if (g) cudaGraphExecDestroy(g);
     for (void* p : allocations) cudaFree(p);
+    if (ev_join) cudaEventDestroy(ev_join);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -434,6 +435,7 @@ KoszulCtx* KoszulCtx::create(const bw_koszul_desc& d, int dev) {
     c->n_src = c->n_s * c->ci;
     c->n_tgt = c->n_t * c->co;
     BW_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    BW_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
 
     const size_t smem_fwd = static_cast<size_t>(c->r) * c->ci * c->co4 * sizeof(int32_t);
     const size_t smem_bwd = static_cast<size_t>(c->r) * c->co * c->ci4 * sizeof(int32_t);
@@ -603,9 +605,24 @@ struct bw_koszul {
     KoszulCtx* impl;
 };
 
-static cudaStream_t pick_stream(KoszulCtx* c, void* stream) {
-    return stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
-}
+// A NULL stream means "ordered like the legacy default stream": the call's
+// work runs on the context's own stream after everything issued before it on
+// the legacy stream, and later legacy-stream work waits for it.
+struct StreamScope {
+    KoszulCtx& c;
+    cudaStream_t st;
+    bool joined;
+    StreamScope(KoszulCtx& ctx, void* stream)
+        : c(ctx), st(stream ? static_cast<cudaStream_t>(stream) : ctx.own_stream), joined(stream == nullptr) {
+        if (joined) {
+            BW_CUDA(cudaEventRecord(c.ev_join, cudaStreamLegacy));
+            BW_CUDA(cudaStreamWaitEvent(st, c.ev_join, 0));
+        }
+    }
+    ~StreamScope() {
+        if (joined && cudaEventRecord(c.ev_join, st) == cudaSuccess) cudaStreamWaitEvent(cudaStreamLegacy, c.ev_join, 0);
+    }
+};
 
 extern "C" int bw_koszul_create(const bw_koszul_desc* desc, int device, bw_koszul** out) {
     return guarded([&] {
@@ -641,7 +658,8 @@ extern "C" int bw_koszul_forward(bw_koszul* ctx, const uint32_t* d_y, uint32_t* 
         KoszulCtx& c = *ctx->impl;
         BW_REQUIRE(!c.in_session, "bw_koszul_forward: a sequence session is open");
         BW_CUDA(cudaSetDevice(c.device));
-        cudaStream_t st = pick_stream(&c, stream);
+        StreamScope scope(c, stream);
+        cudaStream_t st = scope.st;
         if (c.form == BW_FORM_INT8) {
             c.i8_to_limbs(d_y, KoszulCtx::I8_YA, st);
             c.i8_run(true, KoszulCtx::I8_YA, KoszulCtx::I8_Z, false, st);
@@ -663,7 +681,8 @@ extern "C" int bw_koszul_transpose(bw_koszul* ctx, const uint32_t* d_z, uint32_t
         KoszulCtx& c = *ctx->impl;
         BW_REQUIRE(!c.in_session, "bw_koszul_transpose: a sequence session is open");
         BW_CUDA(cudaSetDevice(c.device));
-        cudaStream_t st = pick_stream(&c, stream);
+        StreamScope scope(c, stream);
+        cudaStream_t st = scope.st;
         if (c.form == BW_FORM_INT8) {
             c.i8_to_limbs(d_z, KoszulCtx::I8_Z, st);
             c.i8_run(false, KoszulCtx::I8_Z, KoszulCtx::I8_YA, scale_by_diag != 0, st);
@@ -684,7 +703,8 @@ extern "C" int bw_koszul_apply(bw_koszul* ctx, const uint32_t* d_y, uint32_t* d_
         KoszulCtx& c = *ctx->impl;
         BW_REQUIRE(!c.in_session, "bw_koszul_apply: a sequence session is open");
         BW_CUDA(cudaSetDevice(c.device));
-        cudaStream_t st = pick_stream(&c, stream);
+        StreamScope scope(c, stream);
+        cudaStream_t st = scope.st;
         if (c.form == BW_FORM_INT8) {
             c.i8_to_limbs(d_y, KoszulCtx::I8_YA, st);
             c.i8_run(true, KoszulCtx::I8_YA, KoszulCtx::I8_Z, false, st);
@@ -707,7 +727,8 @@ extern "C" int bw_koszul_seq_start(bw_koszul* ctx, const uint32_t* d_x, const ui
         BW_REQUIRE(ctx != nullptr, "bw_koszul_seq_start: null context");
         KoszulCtx& c = *ctx->impl;
         BW_CUDA(cudaSetDevice(c.device));
-        c.seq_start(d_x, d_y0, d_seq, seq_capacity, pick_stream(&c, stream));
+        StreamScope scope(c, stream);
+        c.seq_start(d_x, d_y0, d_seq, seq_capacity, scope.st);
     });
 }
 
@@ -716,7 +737,8 @@ extern "C" int bw_koszul_seq_step(bw_koszul* ctx, uint64_t steps, void* stream) 
         BW_REQUIRE(ctx != nullptr, "bw_koszul_seq_step: null context");
         KoszulCtx& c = *ctx->impl;
         BW_CUDA(cudaSetDevice(c.device));
-        c.seq_step(steps, pick_stream(&c, stream));
+        StreamScope scope(c, stream);
+        c.seq_step(steps, scope.st);
     });
 }
 
@@ -725,7 +747,8 @@ extern "C" int bw_koszul_seq_finish(bw_koszul* ctx, uint32_t* d_y_out, uint64_t*
         BW_REQUIRE(ctx != nullptr, "bw_koszul_seq_finish: null context");
         KoszulCtx& c = *ctx->impl;
         BW_CUDA(cudaSetDevice(c.device));
-        c.seq_finish(d_y_out, nlen_out, pick_stream(&c, stream));
+        StreamScope scope(c, stream);
+        c.seq_finish(d_y_out, nlen_out, scope.st);
     });
 }
 
@@ -758,7 +781,8 @@ extern "C" int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* m
         BW_REQUIRE(c.in_session, "bw_koszul_seq_step_timed: no sequence session");
         BW_REQUIRE(c.seq_len + steps <= c.seq_capacity, "bw_koszul_seq_step_timed: capacity exceeded");
         BW_CUDA(cudaSetDevice(c.device));
-        cudaStream_t st = pick_stream(&c, stream);
+        StreamScope scope(c, stream);
+        cudaStream_t st = scope.st;
         std::vector<cudaEvent_t> ev(4 * steps);
         for (auto& e : ev) BW_CUDA(cudaEventCreate(&e));
         for (uint64_t s = 0; s < steps; ++s) {

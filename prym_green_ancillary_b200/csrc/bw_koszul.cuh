@@ -19,6 +19,7 @@ struct KoszulCtx {
 
     // device state
     cudaStream_t own_stream = nullptr;
+    cudaEvent_t ev_join = nullptr;     // orders NULL-stream calls with the legacy stream
     std::vector<void*> allocations;
     uint64_t device_bytes = 0, scratch_bytes = 0;
     int32_t *d_coef_fwd = nullptr, *d_coef_bwd = nullptr;

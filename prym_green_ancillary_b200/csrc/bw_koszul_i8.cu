@@ -51,7 +51,8 @@ namespace {
 constexpr uint32_t kAbsent = 0xFFFFFFFFu;
 constexpr int kProducerWarp = 0;
 constexpr int kMmaWarp = 1;
-constexpr int kI8Threads = 6 * 32;
+constexpr int kEpilogueWarps = 8;                 // two per TMEM lane quadrant
+constexpr int kI8Threads = (2 + kEpilogueWarps) * 32;
 constexpr int kMaxSmem = 227 * 1024;
 constexpr int kMaxIncPerTile = 512;   // BT * r words of shared memory for the tile's incidence rows
 
@@ -127,7 +128,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         }
         for (int b = 0; b < 2; ++b) {
             tc::mbar_init(&accfull[b], 1);
-            tc::mbar_init(&accempty[b], 128);
+            tc::mbar_init(&accempty[b], kEpilogueWarps * 32);
         }
         tc::mbar_init(drained, 1);
         tc::fence_mbar_init();
@@ -237,20 +238,42 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         __syncwarp();
     } else {
         // ------------------------------------------------------------ epilogue
-        const int q = warp & 3;                 // TMEM lane quadrant of this warp
-        const int m = q * 32 + lane;            // tile row = (block t, column j)
+        // Warps 2..9: warp & 3 is the TMEM lane quadrant it may read; the two
+        // warps of a quadrant split the 16-column output chunks between them.
+        const int q = warp & 3;
+        const int half_id = (warp - 2) >> 2;      // 0 or 1
+        const int m = q * 32 + lane;               // tile row = (block t, column j)
         const int t = m / NB, j = m % NB;
         const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
+        const int chunks = P.half / 16;
+        const uint32_t j_off = static_cast<uint32_t>((j >> 4) * P.outer * 16 + (j & 15));
         long long tcount = 0;
         for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++tcount) {
             const int buf = static_cast<int>(tcount & 1);
             const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
-            if (!tc::mbar_wait(&accfull[buf], aph, P.err, tc::ERR_WAIT_ACCUM)) break;
-            tc::tc_fence_after();
             const long long blk = tile * BT + t;
             const bool valid = blk < P.n_blk;
+            // prefetch the diagonal entries of this warp's first chunk before waiting for the accumulator
+            int32_t dg[16];
+            auto load_diag = [&](int c) {
+#pragma unroll
+                for (int oo = 0; oo < 16; ++oo) {
+                    const int o = c * 16 + oo;
+                    dg[oo] = (P.diag && valid && o < P.outer) ? __ldg(P.diag + blk * P.outer + o) : 0;
+                }
+            };
+            load_diag(half_id);
+            if (!tc::mbar_wait(&accfull[buf], aph, P.err, tc::ERR_WAIT_ACCUM)) break;
+            tc::tc_fence_after();
             const uint32_t col0 = tmem + lane_off + static_cast<uint32_t>(buf * 2 * N);
-            for (int o0 = 0; o0 < P.half; o0 += 16) {
+            const long long base = blk * static_cast<long long>(NB) * P.outer;
+            int8_t* o_lo = P.out[PL_LO] + base;
+            int8_t* o_hi = P.out[PL_HI] + base;
+            int8_t* o_nlo = P.out[PL_NLO] + base;
+            int8_t* o_nhi = P.out[PL_NHI] + base;
+            for (int c = half_id; c < chunks; c += 2) {
+                const int o0 = c * 16;
+                if (c != half_id) load_diag(c);
                 int32_t ll[16], lh[16], hl[16], hh[16];
                 tc::tmem_ld16(col0 + o0, ll);
                 tc::tmem_ld16(col0 + P.half + o0, lh);
@@ -263,14 +286,14 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                         const int o = o0 + oo;
                         if (o < P.outer) {
                             int32_t v = combine(ll[oo], lh[oo] + hl[oo], hh[oo], P);
-                            if (P.diag) v = reduce_balanced(v * __ldg(P.diag + blk * P.outer + o), P.mod);
+                            if (P.diag) v = reduce_balanced(v * dg[oo], P.mod);
                             int8_t lo, hi;
                             split_limbs(v, lo, hi);
-                            const long long off = plane_offset(blk, o, j, P.outer, NB);
-                            P.out[PL_LO][off] = lo;
-                            P.out[PL_HI][off] = hi;
-                            P.out[PL_NLO][off] = static_cast<int8_t>(-lo);
-                            P.out[PL_NHI][off] = static_cast<int8_t>(-hi);
+                            const uint32_t off = j_off + static_cast<uint32_t>(o) * 16u;
+                            o_lo[off] = lo;
+                            o_hi[off] = hi;
+                            o_nlo[off] = static_cast<int8_t>(-lo);
+                            o_nhi[off] = static_cast<int8_t>(-hi);
                         }
                     }
                 }
@@ -353,10 +376,21 @@ __global__ void __launch_bounds__(256) i8_project_kernel(
     __shared__ bool am_last;
     int32_t acc[4] = {0, 0, 0, 0};
     int cnt = 0;
-    for (long long row = static_cast<long long>(blockIdx.x) * slices + slice; row < rows;
-         row += static_cast<long long>(gridDim.x) * slices) {
-        const long long blk = row / dim;
-        const long long off = plane_offset(blk, static_cast<int>(row - blk * dim), jg * 4, dim, NB);
+    // row = blk * dim + u advances by a fixed stride: keep (blk, u) incrementally (no 64-bit division per row)
+    const long long stride = static_cast<long long>(gridDim.x) * slices;
+    const long long stride_blk = stride / dim;
+    const int stride_u = static_cast<int>(stride - stride_blk * dim);
+    long long row = static_cast<long long>(blockIdx.x) * slices + slice;
+    long long blk = row / dim;
+    int u = static_cast<int>(row - blk * dim);
+    for (; row < rows; row += stride) {
+        const long long off = plane_offset(blk, u, jg * 4, dim, NB);
+        blk += stride_blk;
+        u += stride_u;
+        if (u >= dim) {
+            u -= dim;
+            ++blk;
+        }
         const int32_t xv = __ldg(X + row * m + x);
         const uint32_t lo4 = __ldg(reinterpret_cast<const uint32_t*>(Wlo + off));
         const uint32_t hi4 = __ldg(reinterpret_cast<const uint32_t*>(Whi + off));
