@@ -21,22 +21,27 @@
 //
 // Limb planes in HBM: four planes per block array (lo, hi, -lo, -hi), each
 // laid out [blk][h][u][16 bytes] (h = j / 16), so that every (block, h) is one
-// contiguous run of inner * 16 bytes.  The producer therefore fills a stage
-// with one bulk copy (cp.async.bulk) per (limb, block, generator, h): from the
-// +plane or the -plane by the Koszul sign, or from a zero buffer when the
-// generator is absent.  The epilogue writes all four planes of its output.
+// contiguous run of inner * 16 bytes.  The producers fill a stage with 16-byte
+// cp.async copies (one per K' row, limb and column group) from the +plane or
+// the -plane by the Koszul sign; the rows of an absent generator are zeroed
+// with shared-memory stores (about half of all rows: a common zero source in
+// global memory would funnel that half of the traffic through one L2 slice).
+// The epilogue writes all four planes of its output.
 //
 // Warp roles (persistent, one CTA per SM):
-//   warp 0     producer: per tile, stages the tile's incidence rows in shared
-//              memory; per stage, one elected lane posts the stage's byte count
-//              and the 32 lanes issue the bulk copies;
-//   warp 1     allocates TMEM and issues tcgen05.mma / tcgen05.commit;
-//   warps 2-5  epilogue: tcgen05.ld the four partials, recombine, reduce mod p,
-//              scale by D (d^T only), split into limbs and store.
-// Stages are tracked with mbarriers (byte-count completion for the copies);
-// accumulators are double-buffered in TMEM.  Every wait is bounded: on a
+//   warps 0-3   producers: each owns a quarter of the tile's output blocks and
+//               keeps their incidence rows in registers (one generator per
+//               lane); every thread arrives on the stage barrier through
+//               cp.async.mbarrier.arrive.noinc when its copies have landed;
+//   warp 4      allocates TMEM and issues tcgen05.mma / tcgen05.commit (after a
+//               proxy fence: the stage was written through the generic proxy);
+//   warps 5-12  epilogue, two warps per TMEM lane quadrant: tcgen05.ld the four
+//               partials, recombine, reduce mod p, scale by D (d^T only), split
+//               into limbs and store.
+// Stages are tracked with mbarriers; accumulators are double-buffered in TMEM.
+// Every wait is bounded and polls only a shared-memory give-up flag: on a
 // timeout the kernel records an error code, all roles wind down, in-flight
-// MMAs are drained and TMEM is freed.
+// copies and MMAs are drained and TMEM is freed.
 #include "bw_koszul.cuh"
 #include "tc_sm100.cuh"
 
@@ -49,12 +54,13 @@ namespace bw {
 namespace {
 
 constexpr uint32_t kAbsent = 0xFFFFFFFFu;
-constexpr int kProducerWarp = 0;
-constexpr int kMmaWarp = 1;
+constexpr int kProducerWarps = 4;
+constexpr int kMmaWarp = 4;
+constexpr int kEpilogueWarp0 = 5;
 constexpr int kEpilogueWarps = 8;                 // two per TMEM lane quadrant
-constexpr int kI8Threads = (2 + kEpilogueWarps) * 32;
+constexpr int kI8Threads = (kProducerWarps + 1 + kEpilogueWarps) * 32;
 constexpr int kMaxSmem = 227 * 1024;
-constexpr int kMaxIncPerTile = 512;   // BT * r words of shared memory for the tile's incidence rows
+constexpr int kMaxRowTable = 2048;    // bytes of the K'-row -> generator table
 
 // Plane index inside a four-plane block array.
 enum : int { PL_LO = 0, PL_HI = 1, PL_NLO = 2, PL_NHI = 3 };
@@ -62,7 +68,6 @@ enum : int { PL_LO = 0, PL_HI = 1, PL_NLO = 2, PL_NHI = 3 };
 struct I8Dir {
     const int8_t* in[4];      // input planes lo, hi, -lo, -hi: [blk][h][inner][16]
     int8_t* out[4];           // output planes, same layout with `outer`
-    const int8_t* zeros;      // at least inner * 16 zero bytes
     const uint32_t* inc;      // [n_blk][r]: neighbour rank | negative << 31, or kAbsent
     const int8_t* b_tiles;    // B operand, already in its shared-memory layout
     const int32_t* diag;      // nullptr, or [n_blk * outer] balanced (scales the output)
@@ -112,7 +117,8 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
     uint64_t* accempty = accfull + 2;
     uint64_t* drained = accempty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
-    uint32_t* sInc = tmem_slot + 4;     // BT * r incidence words of the producer's current tile
+    volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);   // CTA give-up flag
+    uint8_t* il_of_row = reinterpret_cast<uint8_t*>(tmem_slot + 4);   // K' row of a slot -> generator slot
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const long long n_tiles = (P.n_blk + BT - 1) / BT;
@@ -123,7 +129,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
     tc::fence_proxy_async_smem();
     if (threadIdx.x == 0) {
         for (int s = 0; s < P.slots; ++s) {
-            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&full[s], 2 * kProducerWarps * 32);   // per thread: copies landed + own stores
             tc::mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -132,67 +138,100 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         }
         tc::mbar_init(drained, 1);
         tc::fence_mbar_init();
+        *abort = 0;
     }
     const uint32_t tmem_cols = (4 * N <= 256) ? 256u : 512u;
     if (warp == kMmaWarp) {
         tc::tmem_alloc(tmem_slot, tmem_cols);
         tc::tmem_relinquish();
     }
+    const int KS = P.gi * P.inner;                       // K' rows of a slot
+    for (int w = threadIdx.x; w < KS; w += blockDim.x) il_of_row[w] = static_cast<uint8_t>(w / P.inner);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const int KS = P.gi * P.inner;                       // K' rows of a slot
     const uint32_t block_bytes = static_cast<uint32_t>(P.inner) * 16;
 
-    if (warp == kProducerWarp) {
-        // ------------------------------------------------------------ producer
+    if (warp < kProducerWarps) {
+        // ------------------------------------------------------------ producers
+        // Warp w stages the output blocks t = w, w + 4, ... of each tile.  Lane
+        // i holds the incidence entry of generator i for those blocks (read by
+        // shuffle; the next tile's entries are loaded one tile ahead), and the
+        // warp's lanes walk the K' rows of every (limb, block, column group):
+        // a 16-byte cp.async from the +plane or -plane of the neighbour block,
+        // or a zero store for an absent generator.  Each thread arrives on the
+        // stage barrier twice: once through cp.async.mbarrier.arrive.noinc when
+        // its copies have landed, once with release semantics for its stores.
+        constexpr int TPW = (BT + kProducerWarps - 1) / kProducerWarps;   // blocks per producer warp
+        auto load_inc = [&](long long tile, uint32_t (&dst)[TPW]) {
+#pragma unroll
+            for (int k = 0; k < TPW; ++k) {
+                const int t = warp + k * kProducerWarps;
+                const long long blk = tile * BT + t;
+                dst[k] = (tile < n_tiles && t < BT && blk < P.n_blk && lane < P.r) ? __ldg(P.inc + blk * P.r + lane)
+                                                                                  : kAbsent;
+            }
+        };
         long long it = 0;
         bool ok = true;
+        uint32_t incr[TPW], incn[TPW];
+        load_inc(blockIdx.x, incn);
         for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
-            __syncwarp();
-            for (int e = lane; e < BT * P.r; e += 32) {
-                const int t = e / P.r;
-                const long long blk = tile * BT + t;
-                sInc[e] = blk < P.n_blk ? __ldg(P.inc + blk * P.r + (e - t * P.r)) : kAbsent;
-            }
-            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < TPW; ++k) incr[k] = incn[k];
+            load_inc(tile + gridDim.x, incn);
             for (int s = 0; s < P.stages_per_tile; ++s, ++it) {
                 const int slot = static_cast<int>(it % P.slots);
                 const uint32_t ph = static_cast<uint32_t>((it / P.slots) & 1);
                 int got = 1;
-                if (lane == 0) got = tc::mbar_wait(&empty[slot], ph ^ 1u, P.err, tc::ERR_WAIT_EMPTY) ? 1 : 0;
+                if (lane == 0) got = tc::mbar_wait(&empty[slot], ph ^ 1u, abort, P.err, tc::ERR_WAIT_EMPTY) ? 1 : 0;
                 got = __shfl_sync(0xffffffffu, got, 0);
                 if (!got) {
                     ok = false;
                     break;
                 }
                 const int g_s = min(P.gi, P.r - s * P.gi);
-                const int nblocks = 2 * BT * g_s * HG;     // (limb, t, il, h)
-                if (lane == 0) tc::mbar_arrive_expect_tx(&full[slot], static_cast<uint32_t>(nblocks) * block_bytes);
-                __syncwarp();
+                const int rows = g_s * P.inner;             // K' rows filled in this stage
                 uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
-                for (int bi = lane; bi < nblocks; bi += 32) {
-                    const int h = bi % HG;
-                    const int rest = bi / HG;
-                    const int il = rest % g_s;
-                    const int rest2 = rest / g_s;
-                    const int t = rest2 % BT;
-                    const int limb = rest2 / BT;
-                    const uint32_t e = sInc[t * P.r + s * P.gi + il];
-                    const int8_t* src;
-                    if (e == kAbsent) {
-                        src = P.zeros;
-                    } else {
-                        const long long nbr = static_cast<long long>(e & 0x7FFFFFFFu);
-                        src = P.in[limb + ((e >> 31) ? 2 : 0)] + (nbr * HG + h) * block_bytes;
+#pragma unroll
+                for (int k = 0; k < TPW; ++k) {
+                    const int t = warp + k * kProducerWarps;
+                    if (t >= BT) break;
+                    for (int w0 = 0; w0 < rows; w0 += 32) {
+                        const int w = w0 + lane;
+                        const int il = il_of_row[min(w, rows - 1)];
+                        const uint32_t e = __shfl_sync(0xffffffffu, incr[k], s * P.gi + il);
+                        if (w >= rows) continue;
+                        const int b = w - il * P.inner;
+                        uint8_t* dst0 = slotA + static_cast<size_t>(t * HG) * KS * 16 + static_cast<size_t>(w) * 16;
+                        if (e == kAbsent) {
+                            // absent generator: zero rows written here (a shared zero source in
+                            // global memory would send every SM's reads to one L2 slice)
+#pragma unroll
+                            for (int limb = 0; limb < 2; ++limb)
+#pragma unroll
+                                for (int h = 0; h < HG; ++h)
+                                    *reinterpret_cast<int4*>(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
+                                                             static_cast<size_t>(h) * KS * 16) = make_int4(0, 0, 0, 0);
+                        } else {
+                            const long long nbr = static_cast<long long>(e & 0x7FFFFFFFu);
+                            const int neg = (e >> 31) ? 2 : 0;
+#pragma unroll
+                            for (int limb = 0; limb < 2; ++limb)
+#pragma unroll
+                                for (int h = 0; h < HG; ++h)
+                                    tc::cp_async16(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
+                                                       static_cast<size_t>(h) * KS * 16,
+                                                   P.in[limb + neg] + (nbr * HG + h) * block_bytes + b * 16);
+                        }
                     }
-                    uint8_t* dst = slotA + static_cast<size_t>(limb) * P.limb_bytes +
-                                   static_cast<size_t>(t * HG + h) * KS * 16 + static_cast<size_t>(il) * block_bytes;
-                    tc::bulk_g2s(dst, src, block_bytes, &full[slot]);
                 }
+                tc::cp_async_arrive_noinc(&full[slot]);   // when this thread's copies have landed
+                tc::mbar_arrive(&full[slot]);              // release: this thread's zero stores
             }
         }
+        tc::cp_async_wait_all();   // no copy may still be landing when the CTA exits
     } else if (warp == kMmaWarp) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
@@ -203,16 +242,17 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
             for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
                 const int buf = static_cast<int>(tcount & 1);
                 const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
-                if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, P.err, tc::ERR_WAIT_ACCUM_FREE)) break;
+                if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, abort, P.err, tc::ERR_WAIT_ACCUM_FREE)) break;
                 tc::tc_fence_after();
                 const uint32_t dbase = tmem + static_cast<uint32_t>(buf * 2 * N);
                 for (int s = 0; s < P.stages_per_tile; ++s, ++it) {
                     const int slot = static_cast<int>(it % P.slots);
                     const uint32_t ph = static_cast<uint32_t>((it / P.slots) & 1);
-                    if (!tc::mbar_wait(&full[slot], ph, P.err, tc::ERR_WAIT_FULL)) {
+                    if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL)) {
                         ok = false;
                         break;
                     }
+                    tc::fence_proxy_async_smem();
                     tc::tc_fence_after();
                     const int ks_n = (s == P.stages_per_tile - 1) ? P.ks_last : P.ks_full;
                     for (int limb = 0; limb < 2; ++limb) {
@@ -232,16 +272,17 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                 tc::mma_commit(&accfull[buf]);
             }
             // drain: every MMA issued above completes before TMEM is released
+            // (this wait ignores the give-up flag; issued MMAs always finish)
             tc::mma_commit(drained);
-            tc::mbar_wait(drained, 0, P.err, tc::ERR_WAIT_FINAL);
+            tc::mbar_wait(drained, 0, nullptr, P.err, tc::ERR_WAIT_FINAL);
         }
         __syncwarp();
     } else {
         // ------------------------------------------------------------ epilogue
-        // Warps 2..9: warp & 3 is the TMEM lane quadrant it may read; the two
+        // Warps 5..12: warp & 3 is the TMEM lane quadrant it may read; the two
         // warps of a quadrant split the 16-column output chunks between them.
         const int q = warp & 3;
-        const int half_id = (warp - 2) >> 2;      // 0 or 1
+        const int half_id = (warp - kEpilogueWarp0) >> 2;      // 0 or 1
         const int m = q * 32 + lane;               // tile row = (block t, column j)
         const int t = m / NB, j = m % NB;
         const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
@@ -263,7 +304,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                 }
             };
             load_diag(half_id);
-            if (!tc::mbar_wait(&accfull[buf], aph, P.err, tc::ERR_WAIT_ACCUM)) break;
+            if (!tc::mbar_wait(&accfull[buf], aph, abort, P.err, tc::ERR_WAIT_ACCUM)) break;
             tc::tc_fence_after();
             const uint32_t col0 = tmem + lane_off + static_cast<uint32_t>(buf * 2 * N);
             const long long base = blk * static_cast<long long>(NB) * P.outer;
@@ -472,7 +513,6 @@ struct KoszulCtx::I8State {
         unsigned grid = 0;
     } fwd, bwd;
     int8_t* planes[3][4] = {};     // Y_a, Y_b, Z: lo, hi, -lo, -hi
-    int8_t* zeros = nullptr;
     int16_t* x16 = nullptr;
     int* err = nullptr;
 };
@@ -502,8 +542,8 @@ void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     P.b_bytes = static_cast<uint32_t>(total_ks) * N * 32;
     P.limb_bytes = static_cast<uint32_t>(8 * gi * inner * 16);
     P.slot_bytes = 2 * P.limb_bytes;
-    BW_REQUIRE(P.slot_bytes / 16 < 4096 || true, "");
-    const size_t extra = (2 * 8 + 2 * 2 + 1) * 8 + 16 + kMaxIncPerTile * 4;
+    BW_REQUIRE(gi * inner <= kMaxRowTable, "INT8 form: stage too deep for the row table");
+    const size_t extra = (2 * 8 + 2 * 2 + 1) * 8 + 16 + kMaxRowTable;
     int slots = 4;
     while (slots > 1 && P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra > static_cast<size_t>(kMaxSmem))
         --slots;
@@ -563,7 +603,7 @@ void KoszulCtx::i8_setup() {
     BW_REQUIRE(nb == 16 || nb == 32, "INT8 form supports block widths 16 and 32");
     BW_REQUIRE(ci <= 128 && co <= 128, "INT8 form: dim_in and dim_out must be at most 128");
     BW_REQUIRE(static_cast<long long>(r) * std::max(ci, co) <= 1024, "INT8 form: r * dim above 1024 (int32 bound)");
-    BW_REQUIRE((128 / nb) * r <= kMaxIncPerTile, "INT8 form: too many generators for one tile");
+    BW_REQUIRE(r <= 32, "INT8 form: at most 32 generators (one per lane)");
     int major = 0;
     BW_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
     BW_REQUIRE(major == 10, "INT8 form needs an sm_100 GPU (tcgen05)");
@@ -598,16 +638,12 @@ void KoszulCtx::i8_setup() {
     BW_CUDA(cudaMemcpyAsync(S.bwd.inc, bwd.data(), bwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
     for (int b = 0; b < 3; ++b)
         for (int pl = 0; pl < 4; ++pl) S.planes[b][pl] = alloc<int8_t>((b < 2 ? n_src : n_tgt) * nb);
-    const size_t zbytes = static_cast<size_t>(std::max(ci, co)) * 16;
-    S.zeros = alloc<int8_t>(zbytes);
-    BW_CUDA(cudaMemsetAsync(S.zeros, 0, zbytes, own_stream));
     S.x16 = alloc<int16_t>(n_src * m);
     S.err = alloc<int>(1);
     BW_CUDA(cudaMemsetAsync(S.err, 0, sizeof(int), own_stream));
     plan_direction(*this, S.fwd, ci, co, false);
     plan_direction(*this, S.bwd, co, ci, true);
     for (I8State::Dir* D : {&S.fwd, &S.bwd}) {
-        D->p.zeros = S.zeros;
         D->p.err = S.err;
     }
     S.fwd.p.inc = S.fwd.inc;

@@ -60,12 +60,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Wait for the phase with the given parity to complete, at most kWaitLimit tries.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+// Wait for the phase with the given parity to complete, at most kWaitLimit
+// tries.  `abort` (shared memory, or null) is the CTA's give-up flag: the wait
+// returns false once another role of the CTA has given up, and a wait that
+// runs out sets it and records `code` in the global error word.  Polling only
+// the shared flag keeps every spin on-chip.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort, int* err, int code) {
     for (uint32_t i = 0; i < kWaitLimit; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (*reinterpret_cast<volatile int*>(err) != ERR_NONE) return false;   // another role gave up
+        if (abort != nullptr && *abort != 0) return false;
     }
+    if (abort != nullptr) *abort = 1;
     atomicCAS(err, ERR_NONE, code);
     return false;
 }
@@ -78,6 +83,20 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+
+// 16-byte asynchronous copy global -> shared through L2 (cp.async.cg).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// Arrive on `bar` once every cp.async issued so far by this thread has landed
+// (the arrival is one of the barrier's expected arrivals).
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Wait until every cp.async issued by this thread has completed.
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // ---- TMEM
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
