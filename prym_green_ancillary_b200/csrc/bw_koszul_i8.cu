@@ -84,11 +84,13 @@ struct I8Dir {
     int32_t c1, c2;              // 255 and 255^2 mod p, balanced
 };
 
-__device__ __forceinline__ int32_t combine(int32_t ll, int32_t lhhl, int32_t hh, const I8Dir& P) {
-    const int32_t a = reduce_partial(ll, P.mod);
-    const int32_t b = reduce_partial(lhhl, P.mod);
-    const int32_t c = reduce_partial(hh, P.mod);
-    return reduce_balanced(a + P.c1 * b + P.c2 * c, P.mod);
+// ll + 255 (lh + hl) + 255^2 hh mod p (balanced); c1 = 255, c2 = 255^2 mod p, balanced.
+__device__ __forceinline__ int32_t combine(int32_t ll, int32_t lhhl, int32_t hh, const Mod& mod, int32_t c1,
+                                           int32_t c2) {
+    const int32_t a = reduce_partial(ll, mod);
+    const int32_t b = reduce_partial(lhhl, mod);
+    const int32_t c = reduce_partial(hh, mod);
+    return reduce_balanced(a + c1 * b + c2 * c, mod);
 }
 
 __host__ __device__ __forceinline__ void split_limbs(int32_t v, int8_t& lo, int8_t& hi) {
@@ -326,7 +328,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                     for (int oo = 0; oo < 16; ++oo) {
                         const int o = o0 + oo;
                         if (o < P.outer) {
-                            int32_t v = combine(ll[oo], lh[oo] + hl[oo], hh[oo], P);
+                            int32_t v = combine(ll[oo], lh[oo] + hl[oo], hh[oo], P.mod, P.c1, P.c2);
                             if (P.diag) v = reduce_balanced(v * dg[oo], P.mod);
                             int8_t lo, hi;
                             split_limbs(v, lo, hi);
@@ -387,99 +389,251 @@ __global__ void from_limbs_kernel(const int8_t* __restrict__ lo, const int8_t* _
     }
 }
 
-__global__ void to_int16_kernel(const uint32_t* __restrict__ in, int16_t* __restrict__ out, long long count,
-                                Mod mod) {
-    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
-         i += static_cast<long long>(gridDim.x) * blockDim.x)
-        out[i] = static_cast<int16_t>(to_balanced(in[i] % static_cast<uint32_t>(mod.p), mod));
-}
+// ---- projection a = X^T W on the tensor cores
+//
+// K = the source rows.  A = X in limbs: M rows = the lo limbs of the m
+// projection columns in groups of 16, then their hi limbs (MN-major; laid out
+// once per session as one contiguous tile per stage).  B = the lo and hi
+// planes of W side by side (N = 2 NB, MN-major: one 16-byte plane row is one
+// core-matrix row, so a block's rows copy straight from HBM).  A stage is SB
+// whole source blocks, SB * dim rows padded to KP (a multiple of 32); the
+// padding rows of the X tile are zero, so whatever the stage buffer holds
+// there adds nothing.  The M = 128 descriptor also reads past the X tile: the
+// TMEM rows at and above 32 * MG are never read back.
+//   D[lo x][j]      = sum lo(X) lo(W),   D[lo x][NB + j] = sum lo(X) hi(W),
+//   D[hi x][j]      = sum hi(X) lo(W),   D[hi x][NB + j] = sum hi(X) hi(W)
+// int32 accumulation is exact for at most 2^31 / 127^2 > 131072 rows, so the
+// accumulator is drained (double-buffered) every `drain` stages.
+//
+// Warps: 0 producer (bulk copies: the stage's X tile and W block runs), 1 MMA
+// issuer (allocates TMEM), 2-5 epilogue (tcgen05.ld + reduction mod p).  The
+// CTA's combined partial goes to partials[blockIdx]; the last CTA to finish
+// reduces them into seq[*seq_index] and advances the index.
+constexpr int kProjThreads = 6 * 32;
+constexpr int kProjStageTarget = 32 * 1024;   // bytes of X tile + W runs per stage
 
-__device__ __forceinline__ int32_t limb_value(uint32_t lo4, uint32_t hi4, int k) {
-    const int32_t lo = static_cast<int8_t>((lo4 >> (8 * k)) & 0xFF);
-    const int32_t hi = static_cast<int8_t>((hi4 >> (8 * k)) & 0xFF);
-    return 255 * hi + lo;
-}
+struct I8Proj {
+    const int8_t* xt;           // [stage][2 MG][KP][16]
+    const int8_t* w[2];         // W lo, hi planes: [blk][h][u][16]
+    int32_t* partials;          // [grid][m][NB]
+    unsigned int* counter;
+    uint32_t* seq;
+    unsigned long long* seq_index;
+    int* err;
+    long long n_blk;
+    int dim, m, mg, sb, kp, n_stages, slots, drain;
+    uint32_t a_bytes, slot_bytes, pad_bytes;
+    Mod mod;
+    int32_t c1, c2;
+};
 
-// a = X^T W into seq[*seq_index]; X int16 balanced (rows x m), W as limb planes.
 template <int NB>
-__global__ void __launch_bounds__(256) i8_project_kernel(
-    const int16_t* __restrict__ X, const int8_t* __restrict__ Wlo, const int8_t* __restrict__ Whi, long long rows,
-    int dim, int m, int32_t* __restrict__ partials, unsigned int* __restrict__ counter, uint32_t* __restrict__ seq,
-    unsigned long long* __restrict__ seq_index, Mod mod) {
-    constexpr int JG = NB / 4;
-    const int tps = m * JG;
-    const int slices = blockDim.x / tps;
-    const int slice = threadIdx.x / tps;
-    const int sub = threadIdx.x - slice * tps;
-    const int x = sub / JG;
-    const int jg = sub - x * JG;
-    __shared__ int32_t red[256 * 4];
+__global__ void __launch_bounds__(kProjThreads, 1) i8_project_tc_kernel(I8Proj P) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    constexpr int HG = NB / 16;
+    constexpr int N = 2 * NB;
+    int32_t* red = reinterpret_cast<int32_t*>(smem + static_cast<size_t>(P.slots) * P.slot_bytes + P.pad_bytes);
+    uint64_t* full = reinterpret_cast<uint64_t*>(red + 32 * P.mg * N);
+    uint64_t* empty = full + P.slots;
+    uint64_t* accfull = empty + P.slots;
+    uint64_t* accempty = accfull + 2;
+    uint64_t* drained = accempty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
+    volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
     __shared__ bool am_last;
-    int32_t acc[4] = {0, 0, 0, 0};
-    int cnt = 0;
-    // row = blk * dim + u advances by a fixed stride: keep (blk, u) incrementally (no 64-bit division per row)
-    const long long stride = static_cast<long long>(gridDim.x) * slices;
-    const long long stride_blk = stride / dim;
-    const int stride_u = static_cast<int>(stride - stride_blk * dim);
-    long long row = static_cast<long long>(blockIdx.x) * slices + slice;
-    long long blk = row / dim;
-    int u = static_cast<int>(row - blk * dim);
-    for (; row < rows; row += stride) {
-        const long long off = plane_offset(blk, u, jg * 4, dim, NB);
-        blk += stride_blk;
-        u += stride_u;
-        if (u >= dim) {
-            u -= dim;
-            ++blk;
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const long long n_my = blockIdx.x < P.n_stages ? (P.n_stages - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const long long n_chunks = (n_my + P.drain - 1) / P.drain;
+    const uint32_t tmem_cols = 2 * N;   // two accumulators (64 or 128 columns)
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < P.slots; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
         }
-        const int32_t xv = __ldg(X + row * m + x);
-        const uint32_t lo4 = __ldg(reinterpret_cast<const uint32_t*>(Wlo + off));
-        const uint32_t hi4 = __ldg(reinterpret_cast<const uint32_t*>(Whi + off));
-#pragma unroll
-        for (int k = 0; k < 4; ++k) acc[k] += xv * limb_value(lo4, hi4, k);
-        if (++cnt == 8) {
-            cnt = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) acc[k] = reduce_partial(acc[k], mod);
+        for (int b = 0; b < 2; ++b) {
+            tc::mbar_init(&accfull[b], 1);
+            tc::mbar_init(&accempty[b], 4 * 32);
         }
+        tc::mbar_init(drained, 1);
+        tc::fence_mbar_init();
+        *abort = 0;
     }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) red[threadIdx.x * 4 + k] = reduce_balanced(acc[k], mod);
+    if (warp == 1) {
+        tc::tmem_alloc(tmem_slot, tmem_cols);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
     __syncthreads();
-    if (threadIdx.x < tps) {
-        int32_t s[4] = {0, 0, 0, 0};
-        for (int sl = 0; sl < slices; ++sl)
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                s[k] += red[(sl * tps + threadIdx.x) * 4 + k];
-                if ((sl & 7) == 7) s[k] = reduce_partial(s[k], mod);
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t run_bytes = static_cast<uint32_t>(P.dim) * 16;   // one (block, h) run of a plane
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        for (long long i = 0; i < n_my; ++i) {
+            const int slot = static_cast<int>(i % P.slots);
+            const uint32_t ph = static_cast<uint32_t>((i / P.slots) & 1);
+            const long long st = blockIdx.x + i * gridDim.x;
+            const long long blk0 = st * P.sb;
+            const int nbh = static_cast<int>(min(static_cast<long long>(P.sb), P.n_blk - blk0));
+            int got = 1;
+            if (lane == 0) {
+                got = tc::mbar_wait(&empty[slot], ph ^ 1u, abort, P.err, tc::ERR_WAIT_EMPTY) ? 1 : 0;
+                if (got)
+                    tc::mbar_arrive_expect_tx(&full[slot], P.a_bytes + 2u * HG * nbh * run_bytes);
             }
-        const int xx = threadIdx.x / JG, jj = threadIdx.x - xx * JG;
-        int32_t* dst = partials + (static_cast<size_t>(blockIdx.x) * m + xx) * NB + jj * 4;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) break;
+            uint8_t* sA = smem + static_cast<size_t>(slot) * P.slot_bytes;
+            uint8_t* sB = sA + P.a_bytes;
+            const uint32_t group_bytes = static_cast<uint32_t>(P.kp) * 16;
+            if (lane == 0) tc::bulk_g2s(sA, P.xt + st * P.a_bytes, P.a_bytes, &full[slot]);
+            if (HG == 1) {
+                // consecutive blocks are consecutive rows of a 16-column plane
+                if (lane < 2)
+                    tc::bulk_g2s(sB + lane * group_bytes, P.w[lane] + blk0 * run_bytes, nbh * run_bytes, &full[slot]);
+            } else {
+                for (int q = lane; q < nbh * 2 * HG; q += 32) {
+                    const int b = q / (2 * HG), limb = (q / HG) % 2, h = q % HG;
+                    tc::bulk_g2s(sB + (limb * HG + h) * group_bytes + b * run_bytes,
+                                 P.w[limb] + ((blk0 + b) * HG + h) * static_cast<long long>(run_bytes), run_bytes,
+                                 &full[slot]);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_i8(128, N, true, true);
+            const uint32_t s0 = tc::smem_u32(smem);
+            const uint32_t gb = static_cast<uint32_t>(P.kp) * 16;
+            const int ksteps = P.kp / 32;
+            long long i = 0;
+            bool ok = true;
+            for (long long c = 0; c < n_chunks && ok; ++c) {
+                const int buf = static_cast<int>(c & 1);
+                const uint32_t aph = static_cast<uint32_t>((c >> 1) & 1);
+                if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, abort, P.err, tc::ERR_WAIT_ACCUM_FREE)) break;
+                tc::tc_fence_after();
+                const uint32_t dcol = tmem + static_cast<uint32_t>(buf * N);
+                const long long i_end = min(n_my, (c + 1) * P.drain);
+                for (bool first = true; i < i_end; ++i, first = false) {
+                    const int slot = static_cast<int>(i % P.slots);
+                    const uint32_t ph = static_cast<uint32_t>((i / P.slots) & 1);
+                    if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::tc_fence_after();
+                    const uint32_t a0 = s0 + static_cast<uint32_t>(slot) * P.slot_bytes;
+                    const uint32_t b0 = a0 + P.a_bytes;
+                    for (int ks = 0; ks < ksteps; ++ks)
+                        tc::mma_i8(dcol, tc::smem_desc(a0 + ks * 512u, 128u, gb), tc::smem_desc(b0 + ks * 512u, 128u, gb),
+                                   idesc, (!first || ks > 0) ? 1u : 0u);
+                    tc::mma_commit(&empty[slot]);
+                }
+                if (!ok) break;
+                tc::mma_commit(&accfull[buf]);
+            }
+            tc::mma_commit(drained);
+            tc::mbar_wait(drained, 0, nullptr, P.err, tc::ERR_WAIT_FINAL);
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int q = warp & 3;                  // TMEM lane quadrant of this warp
+        const int row = q * 32 + lane;           // D row
+        const bool active = q < P.mg;            // rows below 32 * MG carry the X limbs
+        int32_t acc[N];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) dst[k] = reduce_balanced(s[k], mod);
+        for (int c = 0; c < N; ++c) acc[c] = 0;
+        for (long long c = 0; c < n_chunks; ++c) {
+            const int buf = static_cast<int>(c & 1);
+            const uint32_t aph = static_cast<uint32_t>((c >> 1) & 1);
+            if (!tc::mbar_wait(&accfull[buf], aph, abort, P.err, tc::ERR_WAIT_ACCUM)) break;
+            tc::tc_fence_after();
+            if (active) {
+                const uint32_t col0 = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(buf * N);
+#pragma unroll
+                for (int c0 = 0; c0 < N; c0 += 16) {
+                    int32_t v[16];
+                    tc::tmem_ld16(col0 + c0, v);
+                    tc::tmem_ld_wait();
+#pragma unroll
+                    for (int cc = 0; cc < 16; ++cc) acc[c0 + cc] = reduce_balanced(acc[c0 + cc] + reduce_partial(v[cc], P.mod), P.mod);
+                }
+            }
+            tc::tc_fence_before();
+            tc::mbar_arrive(&accempty[buf]);
+        }
+        if (active)
+#pragma unroll
+            for (int c = 0; c < N; ++c) red[row * N + c] = acc[c];
+    }
+
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, tmem_cols);
+    }
+    // x * w = lo*lo + 255 (lo*hi + hi*lo) + 255^2 hi*hi, per (x, j)
+    const int entries = P.m * NB;
+    const int hi_row = 16 * P.mg;
+    for (int e = threadIdx.x; e < entries; e += blockDim.x) {
+        const int x = e / NB, j = e - (e / NB) * NB;
+        const int32_t ll = red[x * N + j], lh = red[x * N + NB + j];
+        const int32_t hl = red[(hi_row + x) * N + j], hh = red[(hi_row + x) * N + NB + j];
+        P.partials[static_cast<size_t>(blockIdx.x) * entries + e] = combine(ll, lh + hl, hh, P.mod, P.c1, P.c2);
     }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    if (threadIdx.x == 0) am_last = (atomicAdd(P.counter, 1u) == gridDim.x - 1);
     __syncthreads();
     if (!am_last) return;
     __threadfence();
-    const unsigned long long pos = *reinterpret_cast<volatile unsigned long long*>(seq_index);
-    const int entries = m * NB;
+    const unsigned long long pos = *reinterpret_cast<volatile unsigned long long*>(P.seq_index);
     for (int e = threadIdx.x; e < entries; e += blockDim.x) {
-        int32_t s = 0;
+        int32_t sum = 0;
         for (unsigned b = 0; b < gridDim.x; ++b) {
-            s += reinterpret_cast<volatile int32_t*>(partials)[static_cast<size_t>(b) * entries + e];
-            if ((b & 7) == 7) s = reduce_partial(s, mod);
+            sum += reinterpret_cast<volatile int32_t*>(P.partials)[static_cast<size_t>(b) * entries + e];
+            if ((b & 7) == 7) sum = reduce_partial(sum, P.mod);
         }
-        seq[pos * entries + e] = to_canonical(reduce_balanced(s, mod), mod);
+        P.seq[pos * entries + e] = to_canonical(reduce_balanced(sum, P.mod), P.mod);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        *seq_index = pos + 1;
-        *counter = 0;
+        *P.seq_index = pos + 1;
+        *P.counter = 0;
         __threadfence();
+    }
+}
+
+// X (canonical, rows x m) -> the projection's A tiles [stage][2 MG][KP][16]:
+// group g < MG holds the lo limbs of columns 16 g .. 16 g + 15, group MG + g
+// their hi limbs; rows past the stage's SB * dim, past the last row or columns
+// past m are zero.
+__global__ void x_tiles_kernel(const uint32_t* __restrict__ X, int8_t* __restrict__ xt, long long rows, int m,
+                               int mg, int dim, int sb, int kp, long long n_units, Mod mod) {
+    for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < n_units;
+         q += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long per_stage = 2LL * mg * kp;
+        const long long st = q / per_stage;
+        const int rem = static_cast<int>(q - st * per_stage);
+        const int g = rem / kp, kr = rem - (rem / kp) * kp;
+        const long long row = st * sb * dim + kr;
+        const bool valid = kr < sb * dim && row < rows;
+        const int limb = g / mg, x0 = (g % mg) * 16;
+        uint32_t packed[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int xi = 0; xi < 16; ++xi) {
+            const int x = x0 + xi;
+            int8_t lo = 0, hi = 0;
+            if (valid && x < m) split_limbs(to_balanced(X[row * m + x] % static_cast<uint32_t>(mod.p), mod), lo, hi);
+            packed[xi / 4] |= static_cast<uint32_t>(static_cast<uint8_t>(limb ? hi : lo)) << (8 * (xi % 4));
+        }
+        *reinterpret_cast<uint4*>(xt + q * 16) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
     }
 }
 
@@ -513,7 +667,10 @@ struct KoszulCtx::I8State {
         unsigned grid = 0;
     } fwd, bwd;
     int8_t* planes[3][4] = {};     // Y_a, Y_b, Z: lo, hi, -lo, -hi
-    int16_t* x16 = nullptr;
+    I8Proj proj{};             // projection plan (X tiles, stage shape, grid)
+    int8_t* xt = nullptr;
+    size_t proj_smem = 0;
+    unsigned proj_grid = 0;
     int* err = nullptr;
 };
 
@@ -585,6 +742,56 @@ void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     P.b_tiles = D.b_tiles;
 }
 
+// Projection stage shape: SB whole source blocks per stage, KP = SB * dim
+// rounded up to 32, about kProjStageTarget bytes of X tile and W runs, the
+// least padding first.  Allocates the X tiles.
+void plan_projection(KoszulCtx& c, KoszulCtx::I8State& S) {
+    I8Proj& P = S.proj;
+    BW_REQUIRE(c.m >= 1 && c.m <= 64, "INT8 form: projection width must be 1..64");
+    P.m = c.m;
+    P.mg = (c.m + 15) / 16;
+    P.dim = c.ci;
+    P.n_blk = static_cast<long long>(c.n_s);
+    const int row_bytes = (2 * P.mg + 2 * (c.nb / 16)) * 16;
+    int best_sb = 1;
+    double best_fill = 0;
+    for (int sb = 1; sb <= 4096; ++sb) {
+        const int kp = (sb * P.dim + 31) / 32 * 32;
+        if (sb > 1 && kp * row_bytes > kProjStageTarget) break;
+        const double fill = static_cast<double>(sb * P.dim) / kp;
+        if (fill >= best_fill) {
+            best_fill = fill;
+            best_sb = sb;
+        }
+    }
+    P.sb = best_sb;
+    P.kp = (best_sb * P.dim + 31) / 32 * 32;
+    P.n_stages = static_cast<int>((P.n_blk + P.sb - 1) / P.sb);
+    P.drain = std::max(1, 131072 / P.kp);
+    const uint32_t group_bytes = static_cast<uint32_t>(P.kp) * 16;
+    P.a_bytes = 2 * P.mg * group_bytes;
+    P.slot_bytes = P.a_bytes + 2 * (c.nb / 16) * group_bytes;
+    // the M = 128 A descriptor spans 8 groups from the tile start
+    const uint32_t reach = 8 * group_bytes;
+    P.pad_bytes = reach > P.slot_bytes ? reach - P.slot_bytes : 0;
+    const size_t extra = static_cast<size_t>(32) * P.mg * 2 * c.nb * 4 + (2 * 8 + 2 * 2 + 1) * 8 + 16;
+    const size_t limit = static_cast<size_t>(kMaxSmem) - 1024;   // headroom for the kernel's static flag
+    int slots = 4;
+    while (slots > 2 && static_cast<size_t>(slots) * P.slot_bytes + P.pad_bytes + extra > limit) --slots;
+    BW_REQUIRE(static_cast<size_t>(slots) * P.slot_bytes + P.pad_bytes + extra <= limit,
+               "INT8 form: projection stage does not fit in shared memory");
+    P.slots = slots;
+    S.proj_smem = static_cast<size_t>(slots) * P.slot_bytes + P.pad_bytes + extra;
+    P.mod = c.mod;
+    P.c1 = to_balanced(255u % c.p, c.mod);
+    P.c2 = to_balanced(static_cast<uint32_t>((255ull * 255ull) % c.p), c.mod);
+    P.err = S.err;
+    S.proj_grid = static_cast<unsigned>(std::max(1, std::min(P.n_stages, c.sms)));
+    BW_REQUIRE(S.proj_grid <= c.proj_grid, "INT8 form: projection grid above the partials buffer");
+    S.xt = c.alloc<int8_t>(static_cast<uint64_t>(P.n_stages) * P.a_bytes);
+    P.xt = S.xt;
+}
+
 template <int NB>
 void launch_i8(KoszulCtx& c, KoszulCtx::I8State::Dir& D, cudaStream_t st) {
     i8_gather_gemm_kernel<NB><<<D.grid, kI8Threads, D.smem, st>>>(D.p);
@@ -638,9 +845,9 @@ void KoszulCtx::i8_setup() {
     BW_CUDA(cudaMemcpyAsync(S.bwd.inc, bwd.data(), bwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
     for (int b = 0; b < 3; ++b)
         for (int pl = 0; pl < 4; ++pl) S.planes[b][pl] = alloc<int8_t>((b < 2 ? n_src : n_tgt) * nb);
-    S.x16 = alloc<int16_t>(n_src * m);
     S.err = alloc<int>(1);
     BW_CUDA(cudaMemsetAsync(S.err, 0, sizeof(int), own_stream));
+    plan_projection(*this, S);
     plan_direction(*this, S.fwd, ci, co, false);
     plan_direction(*this, S.bwd, co, ci, true);
     for (I8State::Dir* D : {&S.fwd, &S.bwd}) {
@@ -654,6 +861,8 @@ void KoszulCtx::i8_setup() {
         auto kern = i8_gather_gemm_kernel<decltype(NBc)::value>;
         const int need = static_cast<int>(std::max(S.fwd.smem, S.bwd.smem));
         BW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
+        BW_CUDA(cudaFuncSetAttribute(i8_project_tc_kernel<decltype(NBc)::value>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S.proj_smem)));
     });
     const int bt = 128 / nb;
     S.fwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_t + bt - 1) / bt, sms)));
@@ -710,18 +919,25 @@ void KoszulCtx::i8_from_limbs(int buf, uint32_t* out, cudaStream_t st) {
 }
 
 void KoszulCtx::i8_load_x(const uint32_t* x, cudaStream_t st) {
-    const uint64_t count = n_src * m;
-    unsigned grid = static_cast<unsigned>(std::min<uint64_t>((count + 255) / 256, static_cast<uint64_t>(sms) * 8));
-    to_int16_kernel<<<std::max(grid, 1u), 256, 0, st>>>(x, i8->x16, static_cast<long long>(count), mod);
+    const I8Proj& P = i8->proj;
+    const long long units = static_cast<long long>(P.n_stages) * 2 * P.mg * P.kp;
+    unsigned grid = static_cast<unsigned>(std::min<long long>((units + 255) / 256, static_cast<long long>(sms) * 8));
+    x_tiles_kernel<<<std::max(grid, 1u), 256, 0, st>>>(x, i8->xt, static_cast<long long>(n_src), m, P.mg, ci, P.sb,
+                                                        P.kp, units, mod);
     BW_CHECK_LAUNCH();
     ++launches;
 }
 
 void KoszulCtx::i8_project(int buf, cudaStream_t st) {
+    I8Proj P = i8->proj;
+    P.w[0] = i8->planes[buf][0];
+    P.w[1] = i8->planes[buf][1];
+    P.partials = d_partials;
+    P.counter = d_counter;
+    P.seq = d_seq;
+    P.seq_index = d_seq_index;
     dispatch_i8_nb(nb, [&](auto NBc) {
-        i8_project_kernel<decltype(NBc)::value><<<proj_grid, 256, 0, st>>>(
-            i8->x16, i8->planes[buf][0], i8->planes[buf][1], static_cast<long long>(n_src), ci, m, d_partials,
-            d_counter, d_seq, d_seq_index, mod);
+        i8_project_tc_kernel<decltype(NBc)::value><<<i8->proj_grid, kProjThreads, i8->proj_smem, st>>>(P);
     });
     BW_CHECK_LAUNCH();
     ++launches;
