@@ -47,7 +47,7 @@ METRIC = "block-Wiedemann steps/s, INT8-limb TC vs plain CUDA-core, bit-exact; %
 def parse():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--form", choices=["int8", "plain", "auto"], default="auto")
