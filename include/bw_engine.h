@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define BW_ABI_VERSION 1
+#define BW_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define BW_API __attribute__((visibility("default")))
@@ -152,7 +152,7 @@ typedef struct bw_cyclic bw_cyclic;
 
 typedef struct bw_cyclic_info {
     uint64_t rows;          /* target rows of F in this sector (N_r) */
-    uint64_t cols;          /* source columns x + z (N_c) */
+    uint64_t cols;          /* source columns of the operator (N_c: x + z, +2 for augmented) */
     uint64_t x_cols, z_cols, t_rows, y_rows;
     uint64_t dm_nnz, d2_nnz;
     uint64_t default_nlen;  /* 2 N_c / 4 + 50 (cuda/cuprym_cyclic.cu:2316) */
@@ -165,13 +165,19 @@ typedef struct bw_cyclic_info {
 /* Loads the instance JSON, assembles the sector, draws the seeded
  * preconditioners and initial block, builds the row-mixing plan and uploads
  * everything.  Replaces load_cyclic_instance, build_*_generic and the set-up
- * half of run_eliminated_sector (cuda/cuprym_cyclic.cu:483-819, 2136-2324).
- * op must be "eliminated"; num_v must be 4 (the paper recipe).  device < 0
- * opens a host-only context (assembly, seeded data, plan, sidecar; every
- * device call then fails with status 3). */
+ * half of run_eliminated_sector (cuda/cuprym_cyclic.cu:483-819, 2136-2324),
+ * and for op "augmented" / "replacement" the set-up of
+ * run_deformation_eliminated_variant (cuda/cuprym_deformation.cu:2554-2797):
+ *   augmented   F = [F0 | -b],  source = base columns + 2 dense columns;
+ *   replacement F = F0 without the two columns of drop_path, + the 2 dense
+ *               columns of dense_path (cuda/cuprym_deformation.cu:426-473).
+ * dense_path is required for the deformation operators and drop_path for
+ * replacement only (NULL or "" = none; ignored for "eliminated").  num_v must
+ * be 4 (the paper recipe).  device < 0 opens a host-only context (assembly,
+ * seeded data, plan, sidecar; every device call then fails with status 3). */
 BW_API int bw_cyclic_open(const char* instance_path, const char* op, uint32_t sector, uint32_t num_v,
-                          uint64_t seed, uint32_t rowmix_rounds, uint64_t rowmix_seed, int device,
-                          bw_cyclic** out);
+                          uint64_t seed, uint32_t rowmix_rounds, uint64_t rowmix_seed, const char* dense_path,
+                          const char* drop_path, int device, bw_cyclic** out);
 BW_API int bw_cyclic_info_get(const bw_cyclic* ctx, bw_cyclic_info* out);
 BW_API void bw_cyclic_close(bw_cyclic* ctx);
 
@@ -208,7 +214,10 @@ BW_API uint64_t bw_cyclic_launch_count(const bw_cyclic* ctx);
 
 /* Kernel-vector recovery (replaces cuda/cuprym_cyclic_kernel_vectors.cu,
  * recover_eliminated_kernel_vectors and recover_kernel_vectors_core,
- * :2550-2986): reads the WDM initial state and its row-mixing sidecar
+ * :2550-2986, and recover_deformation_eliminated_variant,
+ * cuda/cuprym_deformation_kernel_vectors.cu:3067-3487, for op "augmented" /
+ * "replacement" with dense_path / drop_path as in bw_cyclic_open): reads the
+ * WDM initial state and its row-mixing sidecar
  * (hashes and plan checked as in resolve_rowmix_options, :1554-1643), the
  * generator file (one v x v matrix per line), forms D = sum_k S^k V G_k^t on
  * the device, certifies F Dc D = 0 and writes the preconditioned and
@@ -219,8 +228,9 @@ BW_API uint64_t bw_cyclic_launch_count(const bw_cyclic* ctx);
  * whether the caller passed them). */
 BW_API int bw_cyclic_recover(const char* instance_path, const char* op, uint32_t sector, const char* wdm_path,
                              const char* generators_path, const char* preconditioned_out, const char* original_out,
-                             const char* report_out, int64_t cli_rounds, uint64_t cli_seed, int rounds_supplied,
-                             int seed_supplied, int validate, int device);
+                             const char* report_out, const char* dense_path, const char* drop_path,
+                             int64_t cli_rounds, uint64_t cli_seed, int rounds_supplied, int seed_supplied,
+                             int validate, int device);
 
 /* Block projection d_out = X^T W (m x n canonical residues; X is rows x m and
  * W rows x n, canonical, device, W 16-byte aligned) that allocates nothing:

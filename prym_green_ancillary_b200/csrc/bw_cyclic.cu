@@ -93,6 +93,32 @@ __device__ __forceinline__ void decode_coef(int32_t e, int& local, int32_t& coef
     for (long long var = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; var < (count); \
          var += static_cast<long long>(gridDim.x) * blockDim.x)
 
+// Operator column of base column q: q itself, or (replacement) q less the
+// dropped columns before it, -1 for a dropped column.
+__device__ __forceinline__ long long op_col(const ElimDev& E, long long q) {
+    if (E.drop0 < 0) return q;
+    if (q == E.drop0 || q == E.drop1) return -1;
+    return q - (q > E.drop0 ? 1 : 0) - (q > E.drop1 ? 1 : 0);
+}
+
+// xs = the scaled source in base order: rows [0, base_cols) take operator
+// column op_col(q) times dc (zero for a dropped column), rows base_cols + j
+// take the extra column kept_cols + j (dc == nullptr: no scaling).
+__global__ void cyc_source_kernel(ElimDev E, const int32_t* __restrict__ in, const int32_t* __restrict__ dc,
+                                  int32_t* __restrict__ xs) {
+    BW_ROWS(q, static_cast<long long>(E.base_cols) + E.n_extra) {
+        const long long src = q < static_cast<long long>(E.base_cols)
+                                  ? op_col(E, q)
+                                  : static_cast<long long>(E.kept_cols) + (q - static_cast<long long>(E.base_cols));
+        if (src < 0) {
+            st4(xs, q, make_int4(0, 0, 0, 0));
+            continue;
+        }
+        const int4 v = ld4(in, src);
+        st4(xs, q, dc ? scale4(v, __ldg(dc + src), E.mod) : v);
+    }
+}
+
 // out[row] = dc[row] * in[row]  (dc == nullptr: copy)
 __global__ void cyc_scale_kernel(const int32_t* __restrict__ in, const int32_t* __restrict__ dc,
                                  int32_t* __restrict__ out, long long rows, Mod mod) {
@@ -184,13 +210,29 @@ __global__ void cyc_elim_y_kernel(ElimDev E, const int32_t* __restrict__ xs, con
     }
 }
 
-// u = D_(m-1) y  (rows (S2, beta) over (m-2)-subsets)
+// u = D_(m-1) y  (rows (S2, beta) over (m-2)-subsets), plus dense_sign *
+// dense xs_extra for the deformation variants (|terms| stay below 2^31: a
+// balanced residue plus two products of balanced residues).
 template <bool SMALL>
-__global__ void cyc_d2_forward_kernel(ElimDev E, const int32_t* __restrict__ y, int32_t* __restrict__ u) {
+__global__ void cyc_d2_forward_kernel(ElimDev E, const int32_t* __restrict__ y, const int32_t* __restrict__ xs,
+                                      int32_t* __restrict__ u) {
     BW_ROWS(ur, E.n_r) {
         const uint32_t S2 = __ldg(E.u_sub + ur);
-        st4(u, ur, koszul_row<SMALL>(E, E.d2_row_inc + static_cast<size_t>(S2) * E.d2_row_width, E.d2_row_width,
-                                     E.y_off, y, __ldg(E.u_beta + ur)));
+        int4 v = koszul_row<SMALL>(E, E.d2_row_inc + static_cast<size_t>(S2) * E.d2_row_width, E.d2_row_width,
+                                   E.y_off, y, __ldg(E.u_beta + ur));
+        if (E.n_extra) {
+            for (int j = 0; j < E.n_extra; ++j) {
+                const int32_t c = E.dense_sign * __ldg(E.dense + ur * E.n_extra + j);
+                const int4 e = ld4(xs, static_cast<long long>(E.base_cols) + j);
+                v.x += c * e.x;
+                v.y += c * e.y;
+                v.z += c * e.z;
+                v.w += c * e.w;
+            }
+            v = make_int4(reduce_balanced(v.x, E.mod), reduce_balanced(v.y, E.mod), reduce_balanced(v.z, E.mod),
+                          reduce_balanced(v.w, E.mod));
+        }
+        st4(u, ur, v);
     }
 }
 
@@ -242,7 +284,8 @@ __global__ void cyc_adjoint_t_z_kernel(ElimDev E, const int32_t* __restrict__ h,
                 const int32_t c = __ldg(E.Bk + __ldg(E.y_a + yr) * E.kdim + kap);
                 if (c) acc.mac(c, ld4(h, yr));
             }
-            const long long orow = static_cast<long long>(E.x_cols) + zr;
+            const long long orow = op_col(E, static_cast<long long>(E.x_cols) + zr);
+            if (orow < 0) continue;   // dropped base column (replacement)
             const int4 v = acc.reduce(E.mod);
             st4(out, orow, dc ? scale4(v, __ldg(dc + orow), E.mod) : v);
         }
@@ -254,10 +297,12 @@ template <bool SMALL>
 __global__ void cyc_dm_transpose_kernel(ElimDev E, const int32_t* __restrict__ t_adj, const int32_t* __restrict__ dc,
                                         int32_t* __restrict__ out) {
     BW_ROWS(xr, E.x_cols) {
+        const long long orow = op_col(E, xr);
+        if (orow < 0) continue;   // dropped base column (replacement)
         const uint32_t S = __ldg(E.x_sub + xr);
         const int4 v = neg4(koszul_col<SMALL>(E, E.dm_col_inc + static_cast<size_t>(S) * E.dm_col_width,
                                               E.dm_col_width, E.t_off, t_adj, __ldg(E.x_a + xr)));
-        st4(out, xr, dc ? scale4(v, __ldg(dc + xr), E.mod) : v);
+        st4(out, orow, dc ? scale4(v, __ldg(dc + orow), E.mod) : v);
     }
 }
 
@@ -365,6 +410,75 @@ __global__ void __launch_bounds__(kThreads) cyc_gram_kernel(
     }
 }
 
+// Extra source rows of the deformation transpose:
+//   out[kept_cols + j][c] = dense_sign * dc[kept_cols + j] * sum_row dense[row][j] u2[row][c]
+// (dc == nullptr: unscaled).  Each CTA sums a stripe of rows; the last CTA to
+// finish combines the per-CTA sums and writes the n_extra rows (deterministic,
+// no atomics on data; the counter resets itself for the next launch).
+__global__ void __launch_bounds__(kThreads) cyc_dense_t_kernel(ElimDev E, const int32_t* __restrict__ u2,
+                                                               const int32_t* __restrict__ dc,
+                                                               int32_t* __restrict__ out, int32_t* __restrict__ partials,
+                                                               unsigned int* __restrict__ counter) {
+    int32_t acc[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) acc[e] = 0;
+    int cnt = 0;
+    for (long long row = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; row < static_cast<long long>(E.n_r);
+         row += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int4 v = ld4(u2, row);
+        for (int j = 0; j < E.n_extra; ++j) {
+            const int32_t d = __ldg(E.dense + row * E.n_extra + j);
+            acc[4 * j] += d * v.x;
+            acc[4 * j + 1] += d * v.y;
+            acc[4 * j + 2] += d * v.z;
+            acc[4 * j + 3] += d * v.w;
+        }
+        if (++cnt == 8) {   // 8 products of balanced residues stay below 2^31
+            cnt = 0;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) acc[e] = reduce_partial(acc[e], E.mod);
+        }
+    }
+    __shared__ int32_t red[kThreads / 32][8];
+    __shared__ bool am_last;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        int32_t v = reduce_balanced(acc[e], E.mod);
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) red[warp][e] = reduce_balanced(v, E.mod);
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        int32_t sum = 0;
+        for (int w = 0; w < kThreads / 32; ++w) sum += red[w][threadIdx.x];
+        partials[static_cast<size_t>(blockIdx.x) * 8 + threadIdx.x] = reduce_balanced(sum, E.mod);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    if (threadIdx.x < 4 * E.n_extra) {
+        int32_t sum = 0;
+        for (unsigned b = 0; b < gridDim.x; ++b) {
+            sum += reinterpret_cast<volatile int32_t*>(partials)[static_cast<size_t>(b) * 8 + threadIdx.x];
+            if ((b & 7) == 7) sum = reduce_partial(sum, E.mod);
+        }
+        const int j = threadIdx.x / 4, c = threadIdx.x % 4;
+        const long long orow = static_cast<long long>(E.kept_cols) + j;
+        int32_t v = E.dense_sign * reduce_balanced(sum, E.mod);
+        if (dc) v = reduce_balanced(v * __ldg(dc + orow), E.mod);
+        out[orow * 4 + c] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *counter = 0;
+        __threadfence();
+    }
+}
+
 __global__ void cyc_to_balanced_kernel(const uint32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
                                        Mod mod) {
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
@@ -436,8 +550,9 @@ std::vector<int32_t> balanced(const std::vector<uint32_t>& v, const Mod& m) {
 
 CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& op, size_t sector, size_t num_v,
                            uint64_t seed, size_t rowmix_rounds, uint64_t rowmix_seed, int dev,
-                           const CyclicSource* src) {
-    BW_REQUIRE(op == "eliminated", "--operator must be eliminated");
+                           const CyclicSource* src, const DeformInputs* deform) {
+    BW_REQUIRE(op == "eliminated" || op == "augmented" || op == "replacement",
+               "--operator must be one of: eliminated, augmented, replacement.");
     BW_REQUIRE(num_v == 4, "the paper pipeline requires exactly 4 block vectors");
     std::unique_ptr<CyclicCtx> c(new CyclicCtx());
     c->op = op;
@@ -452,12 +567,38 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
     c->es = cyclic::assemble_eliminated_sector(c->inst, sector);
     const auto& es = c->es;
     const auto& inst = c->inst;
+    c->base_cols = c->op_cols = c->kept_cols = es.total_cols();
+    const bool deformation = op != "eliminated";
+    if (deformation) {
+        // run_deformation_eliminated_variant / recover_deformation_eliminated_variant
+        // (cuda/cuprym_deformation.cu:2600-2623, cuda/cuprym_deformation_kernel_vectors.cu:3094-3138)
+        const bool rec = deform && deform->recovery;
+        BW_REQUIRE(deform && !deform->dense_path.empty(),
+                   rec ? "deformation recovery requires --dense-file" : "deformation operators require --dense-file");
+        c->dense = cyclic::load_dense_block_file(deform->dense_path, c->p);
+        BW_REQUIRE(c->dense.rows == es.target_rows && c->dense.columns == 2,
+                   rec ? "dense block dimensions do not match the deformation target sector"
+                       : "dense block dimensions do not match the eliminated target sector");
+        if (op == "replacement") {
+            BW_REQUIRE(!deform->drop_path.empty(), rec ? "replacement recovery requires --drop-columns"
+                                                       : "replacement operator requires --drop-columns");
+            c->drop = cyclic::load_drop_columns_file(deform->drop_path, c->dense.columns, c->base_cols);
+            c->kept_cols = c->base_cols - c->drop.size();
+        } else {
+            BW_REQUIRE(deform->drop_path.empty(), "--drop-columns is only meaningful for replacement");
+        }
+        c->op_cols = (op == "augmented" ? c->base_cols : c->kept_cols) + c->dense.columns;
+    }
+    const size_t ncols = c->op_cols;
 
     if (src) {
         // Recovery: preconditioners, initial block and mixing recipe come from the WDM file and sidecar.
-        BW_REQUIRE(src->row_precond.size() == es.target_rows, "WDM row count does not match eliminated sector");
-        BW_REQUIRE(src->col_precond.size() == es.total_cols(), "WDM column count does not match eliminated sector");
-        BW_REQUIRE(src->initial_block.size() == es.total_cols() * num_v, "WDM initial block has the wrong size");
+        BW_REQUIRE(src->row_precond.size() == es.target_rows,
+                   deformation ? "WDM row count does not match deformation sector"
+                               : "WDM row count does not match eliminated sector");
+        BW_REQUIRE(src->col_precond.size() == ncols, deformation ? "WDM column count does not match deformation operator"
+                                                                 : "WDM column count does not match eliminated sector");
+        BW_REQUIRE(src->initial_block.size() == ncols * num_v, "WDM initial block has the wrong size");
         c->row_precond = src->row_precond;
         c->col_precond = src->col_precond;
         c->initial_block = src->initial_block;
@@ -467,8 +608,8 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
         // Seeded data in the reference's draw order (cuda/cuprym_cyclic.cu:2196-2199).
         std::mt19937_64 gen(cyclic::seeded_sector_value(seed, sector));
         c->row_precond = cyclic::random_vector(es.target_rows, c->p, gen, true);
-        c->col_precond = cyclic::random_vector(es.total_cols(), c->p, gen, true);
-        c->initial_block = cyclic::random_vector(es.total_cols() * num_v, c->p, gen, false);
+        c->col_precond = cyclic::random_vector(ncols, c->p, gen, true);
+        c->initial_block = cyclic::random_vector(ncols * num_v, c->p, gen, false);
     }
     c->plan = cyclic::generate_rowmix_plan(es.target_rows, op, sector, c->p, rowmix_rounds, rowmix_seed);
     if (rowmix_rounds > 0) {
@@ -575,15 +716,22 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
     E.tl = c->upload(tl);
     E.R = c->upload(balanced(inst.right_inverse, c->mod));
     E.Bk = c->upload(balanced(inst.kernel_basis, c->mod));
+    E.base_cols = c->base_cols;
+    E.kept_cols = c->kept_cols;
+    E.drop0 = c->drop.size() > 0 ? static_cast<long long>(c->drop[0]) : -1;
+    E.drop1 = c->drop.size() > 1 ? static_cast<long long>(c->drop[1]) : -1;
+    E.n_extra = static_cast<int>(c->dense.columns);
+    E.dense_sign = op == "augmented" ? -1 : 1;
+    E.dense = deformation ? c->upload(balanced(c->dense.values, c->mod)) : nullptr;
     c->d_dc = c->upload(balanced(c->col_precond, c->mod));
     c->d_p_ptr = c->upload(c->precond.row_ptr);
     c->d_p_col = c->upload(c->precond.col);
     c->d_p_val = c->upload(balanced(c->precond.val, c->mod));
 
-    const size_t nc = es.total_cols(), v = num_v;
+    const size_t nc = ncols, v = num_v;
     c->d_b = c->alloc<int32_t>(nc * v);
     c->d_d = c->alloc<int32_t>(nc * v);
-    c->d_xs = c->alloc<int32_t>(nc * v);
+    c->d_xs = c->alloc<int32_t>((c->base_cols + c->dense.columns) * v);
     c->d_y = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
     c->d_t = c->alloc<int32_t>(std::max<size_t>(es.t_rows, 1) * v);
     c->d_h = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
@@ -593,6 +741,13 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
                                                                                 static_cast<size_t>(c->sms) * 2)));
     c->d_partials = c->alloc<int32_t>(static_cast<size_t>(c->gram_grid) * 20);
     c->d_counter = c->alloc<unsigned int>(1);
+    if (deformation) {
+        c->dense_grid = static_cast<unsigned>(std::max<size_t>(
+            1, std::min<size_t>((es.target_rows + kThreads - 1) / kThreads, static_cast<size_t>(c->sms) * 2)));
+        c->d_dpart = c->alloc<int32_t>(static_cast<size_t>(c->dense_grid) * 8);
+        c->d_dcounter = c->alloc<unsigned int>(1);
+        BW_CUDA(cudaMemsetAsync(c->d_dcounter, 0, sizeof(unsigned int), c->stream));
+    }
     c->d_seq_index = c->alloc<unsigned long long>(1);
     BW_CUDA(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int), c->stream));
     BW_CUDA(cudaMemsetAsync(c->d_seq_index, 0, sizeof(unsigned long long), c->stream));
@@ -616,18 +771,17 @@ void CyclicCtx::to_canonical(const int32_t* in, uint32_t* out, size_t count) {
 }
 
 void CyclicCtx::forward(const int32_t* in, int32_t* u, bool precondition) {
-    const size_t nc = es.total_cols();
-    cyc_scale_kernel<<<grid_for(nc), kThreads, 0, stream>>>(in, precondition ? d_dc : nullptr, d_xs,
-                                                            static_cast<long long>(nc), mod);
+    cyc_source_kernel<<<grid_for(base_cols + dense.columns), kThreads, 0, stream>>>(E, in, precondition ? d_dc : nullptr,
+                                                                                    d_xs);
     BW_CHECK_LAUNCH();
     if (small) {
         cyc_dm_forward_kernel<true><<<grid_for(es.t_rows), kThreads, 0, stream>>>(E, d_xs, d_t);
         cyc_elim_y_kernel<true><<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, d_xs, d_t, d_y);
-        cyc_d2_forward_kernel<true><<<grid_for(es.target_rows), kThreads, 0, stream>>>(E, d_y, u);
+        cyc_d2_forward_kernel<true><<<grid_for(es.target_rows), kThreads, 0, stream>>>(E, d_y, d_xs, u);
     } else {
         cyc_dm_forward_kernel<false><<<grid_for(es.t_rows), kThreads, 0, stream>>>(E, d_xs, d_t);
         cyc_elim_y_kernel<false><<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, d_xs, d_t, d_y);
-        cyc_d2_forward_kernel<false><<<grid_for(es.target_rows), kThreads, 0, stream>>>(E, d_y, u);
+        cyc_d2_forward_kernel<false><<<grid_for(es.target_rows), kThreads, 0, stream>>>(E, d_y, d_xs, u);
     }
     BW_CHECK_LAUNCH();
     launches += 4;
@@ -647,6 +801,11 @@ void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
     }
     BW_CHECK_LAUNCH();
     launches += 3;
+    if (E.n_extra) {
+        cyc_dense_t_kernel<<<dense_grid, kThreads, 0, stream>>>(E, u2, dc, out, d_dpart, d_dcounter);
+        BW_CHECK_LAUNCH();
+        ++launches;
+    }
 }
 
 void CyclicCtx::target_precondition(const int32_t* u, int32_t* u2) {
@@ -668,7 +827,7 @@ void CyclicCtx::apply_square(const int32_t* in, int32_t* out) {
 
 void CyclicCtx::gram(const int32_t* a1, const int32_t* c1, const int32_t* a2, const int32_t* c2, int count) {
     cyc_gram_kernel<<<gram_grid, kThreads, 0, stream>>>(a1, c1, a2 ? a2 : a1, c2 ? c2 : c1, count,
-                                                        static_cast<long long>(es.total_cols()), d_partials,
+                                                        static_cast<long long>(op_cols), d_partials,
                                                         d_counter, d_seq, d_seq_index, mod);
     BW_CHECK_LAUNCH();
     ++launches;
@@ -684,7 +843,7 @@ void CyclicCtx::round() {
 }
 
 void CyclicCtx::generate(size_t nlen_target) {
-    const size_t nc = es.total_cols();
+    const size_t nc = op_cols;
     const size_t default_nlen = (2 * nc) / num_v + 50;
     const size_t max_nlen = nlen_target == 0 ? default_nlen : nlen_target;
     const size_t rounds = (max_nlen - 1 + 3) / 4;
@@ -732,12 +891,12 @@ void CyclicCtx::generate(size_t nlen_target) {
 }
 
 uint32_t* CyclicCtx::scratch_canonical() {
-    if (!d_canon) d_canon = alloc<uint32_t>(std::max<size_t>(es.total_cols(), es.target_rows) * num_v);
+    if (!d_canon) d_canon = alloc<uint32_t>(std::max<size_t>(op_cols, es.target_rows) * num_v);
     return d_canon;
 }
 
 void CyclicCtx::download_state(std::vector<uint32_t>& current, std::vector<uint32_t>& packed) {
-    const size_t nc = es.total_cols();
+    const size_t nc = op_cols;
     uint32_t* tmp = scratch_canonical();
     to_canonical(d_b, tmp, nc * num_v);
     current.resize(nc * num_v);
@@ -749,7 +908,7 @@ void CyclicCtx::download_state(std::vector<uint32_t>& current, std::vector<uint3
 
 // Host-buffer operator applications (validation and tests).
 void CyclicCtx::apply_host(int what, const uint32_t* in, uint32_t* out) {
-    const size_t nc = es.total_cols(), nr = es.target_rows, v = num_v;
+    const size_t nc = op_cols, nr = es.target_rows, v = num_v;
     uint32_t* tmp = scratch_canonical();
     if (what == BW_CYCLIC_APPLY_SQUARE || what == BW_CYCLIC_APPLY_FORWARD) {
         BW_CUDA(cudaMemcpyAsync(tmp, in, nc * v * 4, cudaMemcpyHostToDevice, stream));

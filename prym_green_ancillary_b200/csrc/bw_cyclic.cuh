@@ -32,6 +32,13 @@ struct ElimDev {
     const uint32_t *fl_off, *tl_off;
     const int32_t *fl, *tl;
     const int32_t *R, *Bk;   // g x n, g x kdim (balanced)
+    // Deformation variants (cuda/cuprym_deformation.cu:2554-3066): the source
+    // is the base columns with drop0 / drop1 removed (replacement) followed by
+    // n_extra dense columns; F = [F0 | dense_sign * dense].
+    uint64_t base_cols, kept_cols;
+    long long drop0, drop1;       // dropped base columns, -1 when none (drop0 < drop1)
+    int n_extra, dense_sign;      // 0 / 0 for the eliminated operator
+    const int32_t* dense;         // n_r x n_extra balanced, row-major
 };
 
 // Preconditioners, initial block and row-mixing recipe of an existing WDM file
@@ -40,6 +47,13 @@ struct CyclicSource {
     std::vector<uint32_t> row_precond, col_precond, initial_block;
     size_t rowmix_rounds = 0;
     uint64_t rowmix_seed = 0;
+};
+
+// Inputs of the augmented / replacement operators: the dense block JSON and,
+// for replacement, the two dropped base columns.
+struct DeformInputs {
+    std::string dense_path, drop_path;
+    bool recovery = false;   // word refusals as the recovery stage does
 };
 
 struct CyclicCtx {
@@ -55,6 +69,10 @@ struct CyclicCtx {
     std::vector<uint32_t> row_precond, col_precond, initial_block;
     cyclic::RowMixPlan plan;
     cyclic::Csr precond;
+    // source columns: base_cols = x + z; op_cols = the operator's (the vectors' rows)
+    size_t base_cols = 0, op_cols = 0, kept_cols = 0;
+    std::vector<uint32_t> drop;
+    cyclic::DenseBlockFile dense;
 
     cudaStream_t stream = nullptr;
     std::vector<void*> allocations;
@@ -68,7 +86,9 @@ struct CyclicCtx {
     bool small = false;          // int32 accumulation is exact for this sector
     uint64_t max_terms = 0;      // most products summed into one output by any kernel
     uint32_t* d_canon = nullptr;
-    unsigned gram_grid = 1;
+    unsigned gram_grid = 1, dense_grid = 1;
+    int32_t* d_dpart = nullptr;           // dense-transpose partials and counter
+    unsigned int* d_dcounter = nullptr;
     int32_t* d_partials = nullptr;
     unsigned int* d_counter = nullptr;
     unsigned long long* d_seq_index = nullptr;
@@ -82,7 +102,7 @@ struct CyclicCtx {
 
     static CyclicCtx* open(const std::string& instance_path, const std::string& op, size_t sector, size_t num_v,
                            uint64_t seed, size_t rowmix_rounds, uint64_t rowmix_seed, int dev,
-                           const CyclicSource* src = nullptr);
+                           const CyclicSource* src = nullptr, const DeformInputs* deform = nullptr);
     ~CyclicCtx();
 
     template <class T>

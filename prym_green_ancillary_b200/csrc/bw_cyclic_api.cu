@@ -13,12 +13,14 @@ struct bw_cyclic {
 };
 
 extern "C" int bw_cyclic_open(const char* instance_path, const char* op, uint32_t sector, uint32_t num_v,
-                              uint64_t seed, uint32_t rowmix_rounds, uint64_t rowmix_seed, int device,
-                              bw_cyclic** out) {
+                              uint64_t seed, uint32_t rowmix_rounds, uint64_t rowmix_seed, const char* dense_path,
+                              const char* drop_path, int device, bw_cyclic** out) {
     return guarded([&] {
         BW_REQUIRE(instance_path && op && out, "bw_cyclic_open: null argument");
         *out = nullptr;
-        CyclicCtx* c = CyclicCtx::open(instance_path, op, sector, num_v, seed, rowmix_rounds, rowmix_seed, device);
+        DeformInputs deform{dense_path ? dense_path : "", drop_path ? drop_path : ""};
+        CyclicCtx* c = CyclicCtx::open(instance_path, op, sector, num_v, seed, rowmix_rounds, rowmix_seed, device,
+                                       nullptr, &deform);
         *out = new bw_cyclic{c};
     });
 }
@@ -29,14 +31,14 @@ extern "C" int bw_cyclic_info_get(const bw_cyclic* ctx, bw_cyclic_info* out) {
         const CyclicCtx& c = *ctx->impl;
         std::memset(out, 0, sizeof(*out));
         out->rows = c.es.target_rows;
-        out->cols = c.es.total_cols();
+        out->cols = c.op_cols;
         out->x_cols = c.es.x_cols;
         out->z_cols = c.es.z_cols;
         out->t_rows = c.es.t_rows;
         out->y_rows = c.es.y_rows;
         out->dm_nnz = c.es.dm_nnz;
         out->d2_nnz = c.es.d2_nnz;
-        out->default_nlen = (2 * c.es.total_cols()) / c.num_v + 50;
+        out->default_nlen = (2 * c.op_cols) / c.num_v + 50;
         out->seq_len = c.seq_len;
         out->rowmix_realized_seed = c.plan.realized_seed;
         out->rowmix_hash = cyclic::rowmix_plan_hash(c.plan);
@@ -113,7 +115,7 @@ extern "C" int bw_cyclic_write_sidecar(const bw_cyclic* ctx, const char* wdm_pat
     return guarded([&] {
         BW_REQUIRE(ctx && wdm_path, "bw_cyclic_write_sidecar: null argument");
         const CyclicCtx& c = *ctx->impl;
-        cyclic::write_rowmix_sidecar(wdm_path, c.op, c.es.sector, c.es.target_rows, c.es.total_cols(), c.num_v, c.p,
+        cyclic::write_rowmix_sidecar(wdm_path, c.op, c.es.sector, c.es.target_rows, c.op_cols, c.num_v, c.p,
                                      c.seed, c.plan, c.row_precond, c.col_precond, c.initial_block);
     });
 }
@@ -128,7 +130,7 @@ extern "C" int bw_cyclic_write_wdm(bw_cyclic* ctx, const char* wdm_path) {
         BW_CUDA(cudaSetDevice(c.device));
         std::vector<uint32_t> cur, packed;
         c.download_state(cur, packed);
-        const std::string text = wdm::format_sym(c.es.target_rows, c.es.total_cols(), c.p, c.num_v, c.row_precond,
+        const std::string text = wdm::format_sym(c.es.target_rows, c.op_cols, c.p, c.num_v, c.row_precond,
                                                  c.col_precond, c.initial_block, cur, packed, c.seq_len);
         const std::string tmp = std::string(wdm_path) + ".tmp";
         wdm::write_file(tmp, text);
@@ -152,7 +154,7 @@ void bw::validate_ctx(CyclicCtx& c, uint32_t columns) {
                   << std::endl;
         cyclic::validate_rowmix_transpose_identity(c.plan, cols, c.p);
         std::cout << "Validation matched: eliminated target rowmix transpose identity" << std::endl;
-        const size_t nc = c.es.total_cols();
+        const size_t nc = c.op_cols;
         const uint64_t salts[3] = {0x404ULL, 0x505ULL, 0x606ULL};
         std::vector<std::vector<uint32_t>> blocks, images;
         for (int idx = 0; idx < 3; ++idx) {

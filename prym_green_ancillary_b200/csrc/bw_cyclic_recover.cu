@@ -50,7 +50,7 @@ __global__ void cyc_advance_index_kernel(unsigned long long* k_index) { *k_index
 void CyclicCtx::recover(const std::vector<uint32_t>& generators, size_t generator_count,
                         std::vector<uint32_t>& candidates, std::vector<uint32_t>& product, long long& runtime_ms) {
     require_device();
-    const size_t nc = es.total_cols(), nr = es.target_rows, v = num_v;
+    const size_t nc = op_cols, nr = es.target_rows, v = num_v;
     BW_REQUIRE(generators.size() == generator_count * v * v, "generator storage has the wrong size");
     // 4 x 4 balanced generator matrices; products of a 4-term row stay far inside int32
     std::vector<int32_t> g(generators.size());
@@ -269,8 +269,9 @@ using namespace bw;
 // and opens the operator with the WDM's preconditioners and initial block.
 extern "C" int bw_cyclic_recover(const char* instance_path, const char* op, uint32_t sector, const char* wdm_path,
                                  const char* generators_path, const char* preconditioned_out,
-                                 const char* original_out, const char* report_out, int64_t cli_rounds,
-                                 uint64_t cli_seed, int rounds_supplied, int seed_supplied, int validate, int device) {
+                                 const char* original_out, const char* report_out, const char* dense_path,
+                                 const char* drop_path, int64_t cli_rounds, uint64_t cli_seed, int rounds_supplied,
+                                 int seed_supplied, int validate, int device) {
     return guarded([&] {
         BW_REQUIRE(instance_path && op && wdm_path, "bw_cyclic_recover: null argument");
         const std::string wdm(wdm_path);
@@ -284,13 +285,17 @@ extern "C" int bw_cyclic_recover(const char* instance_path, const char* op, uint
                                 {gens, "Generators"}})
             if (!std::filesystem::exists(f)) throw Error(std::string(label) + " file does not exist: " + f, 1);
 
-        // Host-only open: assembly and sector shapes (no device work yet).
-        std::unique_ptr<CyclicCtx> probe(CyclicCtx::open(instance_path, op, sector, 4, 1, 0, 0, -1));
+        // Host-only open: assembly, deformation inputs and sector shapes (no device work yet).
+        const DeformInputs deform{dense_path ? dense_path : "", drop_path ? drop_path : "", true};
+        const bool deformation = std::string(op) != "eliminated";
+        std::unique_ptr<CyclicCtx> probe(CyclicCtx::open(instance_path, op, sector, 4, 1, 0, 0, -1, nullptr, &deform));
         wdm::InitialState st = wdm::read_initial_state(wdm);
         const uint32_t p = probe->p;
         BW_REQUIRE(st.prime == p, "WDM prime does not match instance modulus");
-        BW_REQUIRE(st.rows == probe->es.target_rows, "WDM row count does not match eliminated sector");
-        BW_REQUIRE(st.cols == probe->es.total_cols(), "WDM column count does not match eliminated sector");
+        BW_REQUIRE(st.rows == probe->es.target_rows, deformation ? "WDM row count does not match deformation sector"
+                                                                 : "WDM row count does not match eliminated sector");
+        BW_REQUIRE(st.cols == probe->op_cols, deformation ? "WDM column count does not match deformation operator"
+                                                          : "WDM column count does not match eliminated sector");
         BW_REQUIRE(st.num_v == 4, "WDM vector count must be 4 for this engine");
         for (size_t i = 0; i < st.row_precond.size(); ++i)
             BW_REQUIRE(st.row_precond[i] % p, "row preconditioner has a zero entry modulo the prime at index " +
@@ -350,7 +355,7 @@ extern "C" int bw_cyclic_recover(const char* instance_path, const char* op, uint
         }
         std::vector<uint32_t> flat;
         const size_t count = recovery::load_generators(gens, st.num_v, p, flat);
-        std::unique_ptr<CyclicCtx> c(CyclicCtx::open(instance_path, op, sector, 4, 1, 0, 0, device, &src));
+        std::unique_ptr<CyclicCtx> c(CyclicCtx::open(instance_path, op, sector, 4, 1, 0, 0, device, &src, &deform));
         std::cout << "Recovery dimensions: rows=" << st.rows << ", columns=" << st.cols << ", v=" << st.num_v
                   << ", WDM sequence length=" << st.nlen << ", generator matrices=" << count << std::endl;
         if (count > st.nlen)

@@ -46,7 +46,7 @@ int main(int argc, char** argv) {
         std::cout << "Loading cyclic Prym instance JSON: " << app.str("instance") << std::endl;
         bw_cyclic* ctx = nullptr;
         bwcli::check(bw_cyclic_open(app.str("instance").c_str(), "eliminated", static_cast<uint32_t>(sector), 4, seed,
-                                    static_cast<uint32_t>(rounds), rseed, device, &ctx));
+                                    static_cast<uint32_t>(rounds), rseed, nullptr, nullptr, device, &ctx));
         bw_cyclic_info info;
         bwcli::check(bw_cyclic_info_get(ctx, &info));
         std::cout << "\n=== Eliminated Sector " << sector << " ===" << std::endl;

@@ -40,7 +40,7 @@ int main(int argc, char** argv) {
         bwcli::check(bw_cyclic_recover(app.str("instance").c_str(), "eliminated", static_cast<uint32_t>(sector),
                                        app.str("--wdm-file").c_str(), app.str("--generators-file").c_str(),
                                        app.str("--preconditioned-output").c_str(), app.str("--original-output").c_str(),
-                                       app.str("--metadata-output").c_str(), rounds, rseed,
+                                       app.str("--metadata-output").c_str(), nullptr, nullptr, rounds, rseed,
                                        app.has("--rowmix-rounds") ? 1 : 0, app.has("--rowmix-seed") ? 1 : 0,
                                        app.on("--validate-rowmix") ? 1 : 0,
                                        static_cast<int>(app.integer("--device"))));

@@ -138,5 +138,19 @@ struct EliminatedSector {
 };
 EliminatedSector assemble_eliminated_sector(const Instance& inst, size_t sector);
 
+// ----- deformation inputs (cuda/cuprym_deformation.cu:426-473)
+// Both files are read the way the reference reads them: a key is its first
+// quoted occurrence anywhere in the text, a scalar is the unsigned digit run
+// after the colon, and an array is every unsigned digit run between its
+// brackets (nested arrays flatten, signs are not read).
+struct DenseBlockFile {
+    size_t rows = 0, columns = 0;
+    uint32_t prime = 0;
+    std::vector<uint32_t> values;   // rows x columns, row-major, reduced mod prime
+};
+DenseBlockFile load_dense_block_file(const std::string& path, uint32_t expected_prime);
+// `expected_count` distinct base-column indices below `base_columns`, sorted ascending.
+std::vector<uint32_t> load_drop_columns_file(const std::string& path, size_t expected_count, size_t base_columns);
+
 }  // namespace cyclic
 }  // namespace bw

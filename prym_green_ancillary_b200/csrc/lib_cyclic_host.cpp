@@ -4,6 +4,7 @@
 #include "json_lite.hpp"
 
 #include <algorithm>
+#include <cctype>
 #include <filesystem>
 #include <fstream>
 #include <iomanip>
@@ -687,6 +688,115 @@ EliminatedSector assemble_eliminated_sector(const Instance& inst, size_t sector)
         inst.expected_elim_rows[sector] != es.target_rows)
         throw std::runtime_error("eliminated sector row count does not match fixture metadata");
     return es;
+}
+
+// ----- deformation inputs (cuda/cuprym_deformation.cu:253-473): text scanning
+namespace {
+
+// Position just past the colon that follows the first quoted occurrence of `key`.
+size_t scan_key(const std::string& text, const std::string& key) {
+    const std::string needle = "\"" + key + "\"";
+    const size_t at = text.find(needle);
+    if (at == std::string::npos) throw std::runtime_error("missing JSON key '" + key + "'");
+    const size_t colon = text.find(':', at + needle.size());
+    if (colon == std::string::npos) throw std::runtime_error("missing ':' after JSON key '" + key + "'");
+    return colon + 1;
+}
+
+uint64_t scan_u64(const std::string& text, const std::string& key) {
+    size_t pos = scan_key(text, key);
+    while (pos < text.size() && std::isspace(static_cast<unsigned char>(text[pos]))) ++pos;
+    if (pos >= text.size() || !std::isdigit(static_cast<unsigned char>(text[pos])))
+        throw std::runtime_error("expected unsigned integer for " + key);
+    uint64_t v = 0;
+    for (; pos < text.size() && std::isdigit(static_cast<unsigned char>(text[pos])); ++pos) {
+        const uint64_t d = static_cast<uint64_t>(text[pos] - '0');
+        if (v > (std::numeric_limits<uint64_t>::max() - d) / 10) throw std::runtime_error(key + " overflows u64");
+        v = v * 10 + d;
+    }
+    return v;
+}
+
+// Every unsigned digit run inside the bracketed array that follows `key`.
+std::vector<uint64_t> scan_u64_array(const std::string& text, const std::string& key, const std::string& label) {
+    const size_t colon = scan_key(text, key);
+    const size_t open = text.find('[', colon);
+    if (open == std::string::npos) throw std::runtime_error("JSON key '" + key + "' is not an array");
+    size_t depth = 0, close = std::string::npos;
+    bool in_str = false, esc = false;
+    for (size_t q = open; q < text.size() && close == std::string::npos; ++q) {
+        const char ch = text[q];
+        if (in_str) {
+            if (esc) esc = false;
+            else if (ch == '\\') esc = true;
+            else if (ch == '"') in_str = false;
+        } else if (ch == '"') {
+            in_str = true;
+        } else if (ch == '[') {
+            ++depth;
+        } else if (ch == ']' && --depth == 0) {
+            close = q;
+        }
+    }
+    if (close == std::string::npos) throw std::runtime_error("failed to find matching JSON delimiter");
+    std::vector<uint64_t> out;
+    for (size_t q = open; q <= close;) {
+        if (!std::isdigit(static_cast<unsigned char>(text[q]))) {
+            ++q;
+            continue;
+        }
+        uint64_t v = 0;
+        for (; q <= close && std::isdigit(static_cast<unsigned char>(text[q])); ++q) {
+            const uint64_t d = static_cast<uint64_t>(text[q] - '0');
+            if (v > (std::numeric_limits<uint64_t>::max() - d) / 10)
+                throw std::runtime_error(label + " entry overflows u64");
+            v = v * 10 + d;
+        }
+        out.push_back(v);
+    }
+    return out;
+}
+
+}  // namespace
+
+DenseBlockFile load_dense_block_file(const std::string& path, uint32_t expected_prime) {
+    const std::string text = read_file(path);
+    const uint64_t rows = scan_u64(text, "rows"), cols = scan_u64(text, "columns"), prime = scan_u64(text, "prime");
+    if (prime > std::numeric_limits<uint32_t>::max()) throw std::runtime_error("dense block scalar metadata is too large");
+    DenseBlockFile b;
+    b.rows = static_cast<size_t>(rows);
+    b.columns = static_cast<size_t>(cols);
+    b.prime = static_cast<uint32_t>(prime);
+    if (b.prime != expected_prime) throw std::runtime_error("dense block prime does not match instance modulus");
+    if (cols != 0 && rows > std::numeric_limits<size_t>::max() / cols)
+        throw std::runtime_error("dense block value count overflows size_t");
+    const std::vector<uint64_t> raw = scan_u64_array(text, "values", "values");
+    if (raw.size() != b.rows * b.columns)
+        throw std::runtime_error("values has " + std::to_string(raw.size()) + " entries; expected " +
+                                 std::to_string(b.rows * b.columns));
+    b.values.reserve(raw.size());
+    for (uint64_t v : raw) {
+        if (v >= expected_prime) throw std::runtime_error("values entry is not reduced modulo the instance modulus");
+        if (v > 65535) throw std::runtime_error("values entry does not fit uint16_t CUDA storage");
+        b.values.push_back(static_cast<uint32_t>(v));
+    }
+    return b;
+}
+
+std::vector<uint32_t> load_drop_columns_file(const std::string& path, size_t expected_count, size_t base_columns) {
+    const std::string text = read_file(path);
+    const std::vector<uint64_t> raw = scan_u64_array(text, "indices", "drop-column indices");
+    if (raw.size() != expected_count) throw std::runtime_error("drop-column file has the wrong number of indices");
+    std::vector<uint32_t> out;
+    for (uint64_t v : raw) {
+        if (v >= base_columns || v > std::numeric_limits<uint32_t>::max())
+            throw std::runtime_error("drop-column index is outside the base column range");
+        out.push_back(static_cast<uint32_t>(v));
+    }
+    std::sort(out.begin(), out.end());
+    for (size_t i = 1; i < out.size(); ++i)
+        if (out[i] == out[i - 1]) throw std::runtime_error("drop-column indices must be distinct");
+    return out;
 }
 
 }  // namespace cyclic

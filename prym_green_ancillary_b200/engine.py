@@ -68,8 +68,8 @@ SIGNATURES = {
     "bw_koszul_sequence_host": (_INT, [_VP, _VP, _VP, _U64, _VP, _VP]),
     "bw_koszul_seq_step_timed": (_INT, [_VP, _U64, ctypes.POINTER(ctypes.c_float), _VP]),
     "bw_koszul_launch_count": (_U64, [_VP]),
-    "bw_cyclic_open": (_INT, [ctypes.c_char_p, ctypes.c_char_p, _U32, _U32, _U64, _U32, _U64, _INT,
-                              ctypes.POINTER(_VP)]),
+    "bw_cyclic_open": (_INT, [ctypes.c_char_p, ctypes.c_char_p, _U32, _U32, _U64, _U32, _U64, ctypes.c_char_p,
+                              ctypes.c_char_p, _INT, ctypes.POINTER(_VP)]),
     "bw_cyclic_info_get": (_INT, [_VP, _VP]),
     "bw_cyclic_close": (None, [_VP]),
     "bw_cyclic_apply_host": (_INT, [_VP, _INT, _VP, _VP]),
@@ -84,8 +84,8 @@ SIGNATURES = {
     "bw_file_read_text": (_INT, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "bw_project_noalloc": (_INT, [_VP, _VP, _U64, _U32, _U32, _U32, _VP, _INT, _VP]),
     "bw_cyclic_recover": (_INT, [ctypes.c_char_p, ctypes.c_char_p, _U32, ctypes.c_char_p, ctypes.c_char_p,
-                                 ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64, _U64, _INT,
-                                 _INT, _INT, _INT]),
+                                 ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                 ctypes.c_char_p, ctypes.c_int64, _U64, _INT, _INT, _INT, _INT]),
 }
 
 
@@ -254,18 +254,22 @@ def read_text(path):
 
 
 class CyclicEngine:
-    """Eliminated cyclic operator of one sector (paper mode, include/bw_engine.h).
+    """Paper-mode operator of one sector (include/bw_engine.h): the eliminated
+    cyclic operator, or with ``op="augmented"`` / ``"replacement"`` its
+    deformation variants (``dense_file``, and ``drop_columns`` for replacement).
 
     ``device=-1`` opens a host-only context (assembly, seeded data, row-mixing
     plan and sidecar; no device calls).
     """
 
     def __init__(self, instance, sector, op="eliminated", num_v=4, seed=1, rowmix_rounds=2, rowmix_seed=10001,
-                 device=0):
+                 device=0, dense_file=None, drop_columns=None):
         lib = load()
         handle = ctypes.c_void_p()
         _check(lib.bw_cyclic_open(str(instance).encode(), op.encode(), sector, num_v, seed, rowmix_rounds,
-                                  rowmix_seed, device, ctypes.byref(handle)))
+                                  rowmix_seed, str(dense_file).encode() if dense_file else None,
+                                  str(drop_columns).encode() if drop_columns else None, device,
+                                  ctypes.byref(handle)))
         self._h = handle
         self.refresh()
 

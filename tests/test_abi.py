@@ -40,7 +40,7 @@ def test_binding_covers_header():
 
 
 def test_abi_version():
-    assert engine.load().bw_abi_version() == 1
+    assert engine.load().bw_abi_version() == 2
 
 
 def test_seeded_host_matches_oracle():

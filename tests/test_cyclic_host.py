@@ -51,7 +51,8 @@ def test_host_only_context_refuses_device_work():
 
 
 @pytest.mark.parametrize("kw, msg", [
-    (dict(op="augmented"), "--operator must be eliminated"),
+    (dict(op="sideways"), "--operator must be one of: eliminated, augmented, replacement."),
+    (dict(op="augmented"), "deformation operators require --dense-file"),
     (dict(num_v=8), "exactly 4 block vectors"),
     (dict(sector=6), "--sector must be in 0..5"),
 ])
@@ -72,3 +73,82 @@ def test_tampered_instance_is_rejected(tmp_path):
     bad.write_text(json.dumps(doc))
     with pytest.raises(EngineError, match="mu_w\\*R=I failed"):
         CyclicEngine(bad, 0, device=-1)
+
+
+# ----- deformation inputs (host-only contexts; the reference's refusals)
+
+def _dense(tmp_path, n_rows, p=661, over=None):
+    from paper_helpers import write_dense_block
+    path = tmp_path / "dense.json"
+    write_dense_block(path, n_rows, p, 5)
+    if over:
+        doc = json.loads(path.read_text())
+        doc.update(over)
+        path.write_text(json.dumps(doc))
+    return path
+
+
+def _shape(sector=0):
+    with CyclicEngine(GOLDEN / "g12_p661.json", sector, device=-1) as eng:
+        return eng.info["rows"], eng.info["cols"]
+
+
+def test_deformation_operator_columns(tmp_path):
+    rows, base = _shape()
+    dense = _dense(tmp_path, rows)
+    with CyclicEngine(GOLDEN / "g12_p661.json", 0, op="augmented", dense_file=dense, device=-1) as eng:
+        assert (eng.info["rows"], eng.info["cols"]) == (rows, base + 2)
+        assert eng.info["default_nlen"] == 2 * (base + 2) // 4 + 50
+    drop = tmp_path / "drop.json"
+    drop.write_text(json.dumps({"indices": [base - 1, 3]}))
+    with CyclicEngine(GOLDEN / "g12_p661.json", 0, op="replacement", dense_file=dense, drop_columns=drop,
+                      device=-1) as eng:
+        assert eng.info["cols"] == base
+
+
+@pytest.mark.parametrize("over, drop, msg", [
+    (dict(prime=109), None, "dense block prime does not match instance modulus"),
+    (dict(columns=3), None, "values has"),
+    (dict(rows=5), None, "values has"),
+    (dict(values=[700, 1]), None, "values has"),
+    (None, [1], "drop-column file has the wrong number of indices"),
+    (None, [4, 4], "drop-column indices must be distinct"),
+    (None, [0, 10 ** 6], "drop-column index is outside the base column range"),
+])
+def test_deformation_input_refusals(tmp_path, over, drop, msg):
+    rows, _ = _shape()
+    dense = _dense(tmp_path, rows, over=over)
+    kw = dict(op="augmented")
+    if drop is not None:
+        path = tmp_path / "drop.json"
+        path.write_text(json.dumps({"indices": drop}))
+        kw = dict(op="replacement", drop_columns=path)
+    with pytest.raises(EngineError, match=msg):
+        CyclicEngine(GOLDEN / "g12_p661.json", 0, dense_file=dense, device=-1, **kw)
+
+
+def test_dense_values_must_be_reduced(tmp_path):
+    rows, _ = _shape()
+    vals = [[1, 2]] * (rows - 1) + [[661, 0]]
+    path = tmp_path / "dense.json"
+    path.write_text(json.dumps({"rows": rows, "columns": 2, "prime": 661, "values": vals}))
+    with pytest.raises(EngineError, match="not reduced modulo the instance modulus"):
+        CyclicEngine(GOLDEN / "g12_p661.json", 0, op="augmented", dense_file=path, device=-1)
+
+
+def test_drop_columns_only_for_replacement(tmp_path):
+    rows, _ = _shape()
+    dense = _dense(tmp_path, rows)
+    drop = tmp_path / "drop.json"
+    drop.write_text(json.dumps({"indices": [0, 1]}))
+    with pytest.raises(EngineError, match="only meaningful for replacement"):
+        CyclicEngine(GOLDEN / "g12_p661.json", 0, op="augmented", dense_file=dense, drop_columns=drop, device=-1)
+    with pytest.raises(EngineError, match="replacement operator requires --drop-columns"):
+        CyclicEngine(GOLDEN / "g12_p661.json", 0, op="replacement", dense_file=dense, device=-1)
+
+
+def test_dense_dimensions_must_match_sector(tmp_path):
+    rows, _ = _shape()
+    dense = _dense(tmp_path, rows - 1)
+    with pytest.raises(EngineError, match="dense block dimensions do not match the eliminated target sector"):
+        CyclicEngine(GOLDEN / "g12_p661.json", 0, op="augmented", dense_file=dense, device=-1)

@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from prym_green_ancillary_b200 import CyclicEngine
-from prym_green_ancillary_b200.engine import APPLY_SQUARE
+from paper_helpers import kernel_generator, square_matrix, write_generator
 
 pytestmark = pytest.mark.gpu
 
@@ -27,60 +27,6 @@ OUR_REC = ROOT / "prym_green_ancillary_b200" / "bin" / "cuprym_cyclic_kernel_vec
 REF_REC = ROOT / "oracle" / "_ref" / "bin" / "cuprym_cyclic_kernel_vectors"
 RECIPE = ["--operator", "eliminated", "-v", "4", "--seed", "1", "--rowmix-rounds", "2", "--rowmix-seed", "10001"]
 STEM = "eliminated-sector{:02d}-v4-rowmix-r2-s10001"
-
-
-def _square_matrix(eng, p):
-    n = eng.info["cols"]
-    cols = []
-    for c0 in range(0, n, 4):
-        block = np.zeros((n, 4), dtype=np.uint32)
-        for j in range(4):
-            if c0 + j < n:
-                block[c0 + j, j] = 1
-        out = eng.apply(APPLY_SQUARE, block).astype(np.int64)
-        for j in range(4):
-            if c0 + j < n:
-                cols.append(out[:, j])
-    return np.stack(cols, axis=1) % p
-
-
-def _minimal_polynomial(S, p, seed=3):
-    """Monic minimal polynomial of a random vector under S (exact, Python ints)."""
-    n = S.shape[0]
-    v = np.random.default_rng(seed).integers(0, p, n).astype(object)
-    krylov = [v]
-    Sobj = S.astype(object)
-    basis, pivots = [], []   # reduced echelon rows with combination coefficients
-    for d in range(n + 1):
-        w = krylov[-1]
-        # reduce w against the basis, tracking the combination of Krylov vectors
-        comb = [0] * (d + 1)
-        comb[d] = 1
-        w = list(w)
-        for (row, rcomb), pc in zip(basis, pivots):
-            f = w[pc] % p
-            if f:
-                w = [(a - f * b) % p for a, b in zip(w, row)]
-                for i, c in enumerate(rcomb):
-                    comb[i] = (comb[i] - f * c) % p
-        nz = next((i for i, a in enumerate(w) if a % p), None)
-        if nz is None:
-            return [c % p for c in comb]    # sum comb[i] S^i v = 0, comb[d] = 1
-        inv = pow(int(w[nz]), -1, p)
-        basis.append(([a * inv % p for a in w], [c * inv % p for c in comb]))
-        pivots.append(nz)
-        krylov.append(np.array([int(x) for x in Sobj.dot(np.array(krylov[-1], dtype=object)) % p], dtype=object))
-    raise AssertionError("no minimal polynomial found")
-
-
-def _write_generator(path, coeffs, p):
-    with open(path, "w") as f:
-        for c in coeffs:
-            m = np.zeros((4, 4), dtype=np.int64)
-            np.fill_diagonal(m, c % p)
-            # exported generator entries may be negative: write some as c - p
-            row = [int(x) if (i % 5) else int(x) - p if x else 0 for i, x in enumerate(m.reshape(-1))]
-            f.write(" ".join(str(x) for x in row) + "\n")
 
 
 def _run(cmd):
@@ -97,11 +43,9 @@ def test_recovery_matches_reference_binary(sector, tmp_path):
     res = _run([str(OUR_SEQ), str(inst), "--sector", str(sector), "--out", str(seq_dir), *RECIPE])
     assert res.returncode == 0, res.stderr
     with CyclicEngine(inst, sector) as eng:
-        S = _square_matrix(eng, p)
-    mu = _minimal_polynomial(S, p)
-    e = next(i for i, c in enumerate(mu) if c)
+        S = square_matrix(eng, p)
     # x^(e-1) q(x) for mu = x^e q(x); mu itself when S is invertible (then D = mu(S) V = 0)
-    gen = [0] * (e - 1) + mu[e:] if e >= 1 else mu
+    gen = kernel_generator(S, p)
     stem = STEM.format(sector)
     outs = {}
     for name, exe in (("ours", OUR_REC), ("ref", REF_REC)):
@@ -109,7 +53,7 @@ def test_recovery_matches_reference_binary(sector, tmp_path):
         d.mkdir()
         for suffix in (".wdm.zst", ".rowmix.json"):
             shutil.copy(seq_dir / (stem + suffix), d / (stem + suffix))
-        _write_generator(d / (stem + "_generators.txt"), gen, p)
+        write_generator(d / (stem + "_generators.txt"), gen, p)
         wdm = d / (stem + ".wdm.zst")
         res = _run([str(exe), str(inst), "-f", str(wdm), "--operator", "eliminated", "--sector", str(sector),
                     "-d", "0"])
