@@ -37,7 +37,8 @@
 //               proxy fence: the stage was written through the generic proxy);
 //   warps 5-12  epilogue, two warps per TMEM lane quadrant: tcgen05.ld the four
 //               partials, recombine, reduce mod p, scale by D (d^T only), split
-//               into limbs and store.
+//               into limbs, transpose 16 x 16 bytes per half-warp and store one
+//               16-byte plane row per lane.
 // Stages are tracked with mbarriers; accumulators are double-buffered in TMEM.
 // Every wait is bounded and polls only a shared-memory give-up flag: on a
 // timeout the kernel records an error code, all roles wind down, in-flight
@@ -98,6 +99,35 @@ __host__ __device__ __forceinline__ void split_limbs(int32_t v, int8_t& lo, int8
     const int32_t q = static_cast<int32_t>(static_cast<uint32_t>(v + 127 + 255 * 128) / 255u) - 128;
     lo = static_cast<int8_t>(v - 255 * q);
     hi = static_cast<int8_t>(q);
+}
+
+// 16 x 16 byte transpose inside each half-warp.  On entry lane L (L = lane & 15)
+// holds row L as four words (byte b of word q = element 4q + b); on exit it
+// holds column L the same way.  Two butterfly stages exchange words (lane bits
+// 2 and 3 against word-index bits), two exchange bytes (lane bits 0 and 1
+// against byte-index bits, recombined with byte permutes).
+__device__ __forceinline__ void transpose16(uint32_t (&w)[4], int lane) {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const bool upper = (lane >> (k + 2)) & 1;
+        const int step = 1 << k;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (q & step) continue;   // the pair (q, q + step)
+            const uint32_t send = upper ? w[q] : w[q + step];
+            const uint32_t recv = __shfl_xor_sync(0xffffffffu, send, 4 << k);
+            if (upper) w[q] = recv;
+            else w[q + step] = recv;
+        }
+    }
+    const bool b0 = lane & 1, b1 = (lane >> 1) & 1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uint32_t r = __shfl_xor_sync(0xffffffffu, w[q], 1);
+        w[q] = __byte_perm(w[q], r, b0 ? 0x3715 : 0x6240);
+        r = __shfl_xor_sync(0xffffffffu, w[q], 2);
+        w[q] = __byte_perm(w[q], r, b1 ? 0x3276 : 0x5410);
+    }
 }
 
 // Byte offset of element (row = blk * dim + u, column j) in a plane of width NB.
@@ -289,7 +319,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         const int t = m / NB, j = m % NB;
         const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
         const int chunks = P.half / 16;
-        const uint32_t j_off = static_cast<uint32_t>((j >> 4) * P.outer * 16 + (j & 15));
+        const uint32_t h_off = static_cast<uint32_t>((j >> 4) * P.outer * 16);   // this half-warp's column group
         long long tcount = 0;
         for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++tcount) {
             const int buf = static_cast<int>(tcount & 1);
@@ -323,22 +353,30 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                 tc::tmem_ld16(col0 + N + o0, hl);
                 tc::tmem_ld16(col0 + N + P.half + o0, hh);
                 tc::tmem_ld_wait();
-                if (valid) {
+                // this lane's 16 outputs (o0..o0+15 of its column j) as limb bytes; columns o >= outer
+                // hold zeros (zero rows of the maps, zero diagonal entries) and are not stored
+                uint32_t lw[4] = {0, 0, 0, 0}, hw[4] = {0, 0, 0, 0};
 #pragma unroll
-                    for (int oo = 0; oo < 16; ++oo) {
-                        const int o = o0 + oo;
-                        if (o < P.outer) {
-                            int32_t v = combine(ll[oo], lh[oo] + hl[oo], hh[oo], P.mod, P.c1, P.c2);
-                            if (P.diag) v = reduce_balanced(v * dg[oo], P.mod);
-                            int8_t lo, hi;
-                            split_limbs(v, lo, hi);
-                            const uint32_t off = j_off + static_cast<uint32_t>(o) * 16u;
-                            o_lo[off] = lo;
-                            o_hi[off] = hi;
-                            o_nlo[off] = static_cast<int8_t>(-lo);
-                            o_nhi[off] = static_cast<int8_t>(-hi);
-                        }
-                    }
+                for (int oo = 0; oo < 16; ++oo) {
+                    int32_t v = combine(ll[oo], lh[oo] + hl[oo], hh[oo], P.mod, P.c1, P.c2);
+                    if (P.diag) v = reduce_balanced(v * dg[oo], P.mod);
+                    int8_t lo, hi;
+                    split_limbs(v, lo, hi);
+                    lw[oo >> 2] |= static_cast<uint32_t>(static_cast<uint8_t>(lo)) << (8 * (oo & 3));
+                    hw[oo >> 2] |= static_cast<uint32_t>(static_cast<uint8_t>(hi)) << (8 * (oo & 3));
+                }
+                // transposed, lane L of the half-warp holds output row o0 + L: 16 bytes, one per j
+                transpose16(lw, lane);
+                transpose16(hw, lane);
+                const int o = o0 + (lane & 15);
+                if (valid && o < P.outer) {
+                    const uint32_t off = h_off + static_cast<uint32_t>(o) * 16u;
+                    *reinterpret_cast<uint4*>(o_lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                    *reinterpret_cast<uint4*>(o_hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    *reinterpret_cast<uint4*>(o_nlo + off) = make_uint4(__vsub4(0u, lw[0]), __vsub4(0u, lw[1]),
+                                                                        __vsub4(0u, lw[2]), __vsub4(0u, lw[3]));
+                    *reinterpret_cast<uint4*>(o_nhi + off) = make_uint4(__vsub4(0u, hw[0]), __vsub4(0u, hw[1]),
+                                                                        __vsub4(0u, hw[2]), __vsub4(0u, hw[3]));
                 }
             }
             tc::tc_fence_before();
