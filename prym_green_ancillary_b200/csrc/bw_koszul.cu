@@ -426,6 +426,7 @@ KoszulCtx* KoszulCtx::create(const bw_koszul_desc& d, int dev) {
     c->ci4 = (c->ci + 3) / 4 * 4;
     c->co4 = (c->co + 3) / 4 * 4;
     c->nb = static_cast<int>(d.block_width);
+    c->nbi = d.form == BW_FORM_INT8 ? (c->nb <= 16 ? 16 : 32) : c->nb;
     c->m = static_cast<int>(d.proj_width);
     c->p = d.prime;
     c->mod = make_mod(d.prime);
@@ -486,7 +487,7 @@ KoszulCtx* KoszulCtx::create(const bw_koszul_desc& d, int dev) {
     c->proj_grid = static_cast<unsigned>(std::min<uint64_t>(static_cast<uint64_t>(c->sms) * 4,
                                                             std::max<uint64_t>(1, (c->n_src + 255) / 256)));
     const uint64_t scratch_before = c->device_bytes;
-    c->d_partials = c->alloc<int32_t>(static_cast<uint64_t>(c->proj_grid) * c->m * c->nb);
+    c->d_partials = c->alloc<int32_t>(static_cast<uint64_t>(c->proj_grid) * c->m * std::max(c->nb, c->nbi));
     c->d_counter = c->alloc<unsigned int>(1);
     c->d_seq_index = c->alloc<unsigned long long>(1);
     c->scratch_bytes = c->device_bytes - scratch_before;

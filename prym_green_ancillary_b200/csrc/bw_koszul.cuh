@@ -13,6 +13,7 @@ struct KoszulCtx {
     // shape
     int device = 0, sms = 0;
     int r = 0, k = 0, ci = 0, co = 0, ci4 = 0, co4 = 0, nb = 0, m = 0;
+    int nbi = 0;   // block width inside the INT8 form (nb, or 16 for nb = 4 / 8: zero columns appended)
     uint32_t p = 0, form = BW_FORM_PLAIN;
     Mod mod{};
     uint64_t n_s = 0, n_t = 0, n_src = 0, n_tgt = 0;

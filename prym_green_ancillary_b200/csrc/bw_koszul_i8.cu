@@ -394,17 +394,18 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
 
 // ---- limb conversions and the projection on limb planes
 
-// canonical row-major (rows = n_blk * dim, NB columns) -> four planes
+// canonical row-major (rows = n_blk * dim, w_in columns) -> four planes of NB
+// columns (columns w_in..NB-1 are zero)
 template <int NB>
 __global__ void to_limbs_kernel(const uint32_t* __restrict__ in, int8_t* __restrict__ lo, int8_t* __restrict__ hi,
                                 int8_t* __restrict__ nlo, int8_t* __restrict__ nhi, long long count, int dim,
-                                Mod mod) {
+                                int w_in, Mod mod) {
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        int8_t a, b;
-        split_limbs(to_balanced(in[i] % static_cast<uint32_t>(mod.p), mod), a, b);
         const long long row = i / NB;
         const int j = static_cast<int>(i - row * NB);
+        int8_t a = 0, b = 0;
+        if (j < w_in) split_limbs(to_balanced(in[row * w_in + j] % static_cast<uint32_t>(mod.p), mod), a, b);
         const long long blk = row / dim;
         const long long off = plane_offset(blk, static_cast<int>(row - blk * dim), j, dim, NB);
         lo[off] = a;
@@ -414,13 +415,14 @@ __global__ void to_limbs_kernel(const uint32_t* __restrict__ in, int8_t* __restr
     }
 }
 
+// four planes of NB columns -> canonical row-major with the first w_out columns
 template <int NB>
 __global__ void from_limbs_kernel(const int8_t* __restrict__ lo, const int8_t* __restrict__ hi,
-                                  uint32_t* __restrict__ out, long long count, int dim, Mod mod) {
+                                  uint32_t* __restrict__ out, long long count, int dim, int w_out, Mod mod) {
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const long long row = i / NB;
-        const int j = static_cast<int>(i - row * NB);
+        const long long row = i / w_out;
+        const int j = static_cast<int>(i - row * w_out);
         const long long blk = row / dim;
         const long long off = plane_offset(blk, static_cast<int>(row - blk * dim), j, dim, NB);
         out[i] = to_canonical(255 * static_cast<int32_t>(hi[off]) + lo[off], mod);
@@ -460,6 +462,7 @@ struct I8Proj {
     int* err;
     long long n_blk;
     int dim, m, mg, sb, kp, n_stages, slots, drain;
+    int n_out;                  // columns of W that are the caller's (the rest are zero padding)
     uint32_t a_bytes, slot_bytes, pad_bytes;
     Mod mod;
     int32_t c1, c2;
@@ -633,12 +636,15 @@ __global__ void __launch_bounds__(kProjThreads, 1) i8_project_tc_kernel(I8Proj P
     __threadfence();
     const unsigned long long pos = *reinterpret_cast<volatile unsigned long long*>(P.seq_index);
     for (int e = threadIdx.x; e < entries; e += blockDim.x) {
+        const int x = e / NB, j = e - (e / NB) * NB;
+        if (j >= P.n_out) continue;
         int32_t sum = 0;
         for (unsigned b = 0; b < gridDim.x; ++b) {
             sum += reinterpret_cast<volatile int32_t*>(P.partials)[static_cast<size_t>(b) * entries + e];
             if ((b & 7) == 7) sum = reduce_partial(sum, P.mod);
         }
-        P.seq[pos * entries + e] = to_canonical(reduce_balanced(sum, P.mod), P.mod);
+        P.seq[pos * (static_cast<unsigned long long>(P.m) * P.n_out) + x * P.n_out + j] =
+            to_canonical(reduce_balanced(sum, P.mod), P.mod);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -787,10 +793,11 @@ void plan_projection(KoszulCtx& c, KoszulCtx::I8State& S) {
     I8Proj& P = S.proj;
     BW_REQUIRE(c.m >= 1 && c.m <= 64, "INT8 form: projection width must be 1..64");
     P.m = c.m;
+    P.n_out = c.nb;
     P.mg = (c.m + 15) / 16;
     P.dim = c.ci;
     P.n_blk = static_cast<long long>(c.n_s);
-    const int row_bytes = (2 * P.mg + 2 * (c.nb / 16)) * 16;
+    const int row_bytes = (2 * P.mg + 2 * (c.nbi / 16)) * 16;
     int best_sb = 1;
     double best_fill = 0;
     for (int sb = 1; sb <= 4096; ++sb) {
@@ -808,11 +815,11 @@ void plan_projection(KoszulCtx& c, KoszulCtx::I8State& S) {
     P.drain = std::max(1, 131072 / P.kp);
     const uint32_t group_bytes = static_cast<uint32_t>(P.kp) * 16;
     P.a_bytes = 2 * P.mg * group_bytes;
-    P.slot_bytes = P.a_bytes + 2 * (c.nb / 16) * group_bytes;
+    P.slot_bytes = P.a_bytes + 2 * (c.nbi / 16) * group_bytes;
     // the M = 128 A descriptor spans 8 groups from the tile start
     const uint32_t reach = 8 * group_bytes;
     P.pad_bytes = reach > P.slot_bytes ? reach - P.slot_bytes : 0;
-    const size_t extra = static_cast<size_t>(32) * P.mg * 2 * c.nb * 4 + (2 * 8 + 2 * 2 + 1) * 8 + 16;
+    const size_t extra = static_cast<size_t>(32) * P.mg * 2 * c.nbi * 4 + (2 * 8 + 2 * 2 + 1) * 8 + 16;
     const size_t limit = static_cast<size_t>(kMaxSmem) - 1024;   // headroom for the kernel's static flag
     int slots = 4;
     while (slots > 2 && static_cast<size_t>(slots) * P.slot_bytes + P.pad_bytes + extra > limit) --slots;
@@ -845,7 +852,7 @@ void KoszulCtx::i8_destroy() {
 }
 
 void KoszulCtx::i8_setup() {
-    BW_REQUIRE(nb == 16 || nb == 32, "INT8 form supports block widths 16 and 32");
+    BW_REQUIRE(nbi == 16 || nbi == 32, "INT8 form: internal block width must be 16 or 32");
     BW_REQUIRE(ci <= 128 && co <= 128, "INT8 form: dim_in and dim_out must be at most 128");
     BW_REQUIRE(static_cast<long long>(r) * std::max(ci, co) <= 1024, "INT8 form: r * dim above 1024 (int32 bound)");
     BW_REQUIRE(r <= 32, "INT8 form: at most 32 generators (one per lane)");
@@ -882,7 +889,7 @@ void KoszulCtx::i8_setup() {
     BW_CUDA(cudaMemcpyAsync(S.fwd.inc, fwd.data(), fwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
     BW_CUDA(cudaMemcpyAsync(S.bwd.inc, bwd.data(), bwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
     for (int b = 0; b < 3; ++b)
-        for (int pl = 0; pl < 4; ++pl) S.planes[b][pl] = alloc<int8_t>((b < 2 ? n_src : n_tgt) * nb);
+        for (int pl = 0; pl < 4; ++pl) S.planes[b][pl] = alloc<int8_t>((b < 2 ? n_src : n_tgt) * nbi);
     S.err = alloc<int>(1);
     BW_CUDA(cudaMemsetAsync(S.err, 0, sizeof(int), own_stream));
     plan_projection(*this, S);
@@ -895,14 +902,14 @@ void KoszulCtx::i8_setup() {
     S.bwd.p.inc = S.bwd.inc;
     S.fwd.p.n_blk = static_cast<long long>(n_t);
     S.bwd.p.n_blk = static_cast<long long>(n_s);
-    dispatch_i8_nb(nb, [&](auto NBc) {
+    dispatch_i8_nb(nbi, [&](auto NBc) {
         auto kern = i8_gather_gemm_kernel<decltype(NBc)::value>;
         const int need = static_cast<int>(std::max(S.fwd.smem, S.bwd.smem));
         BW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
         BW_CUDA(cudaFuncSetAttribute(i8_project_tc_kernel<decltype(NBc)::value>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S.proj_smem)));
     });
-    const int bt = 128 / nb;
+    const int bt = 128 / nbi;
     S.fwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_t + bt - 1) / bt, sms)));
     S.bwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_s + bt - 1) / bt, sms)));
     BW_CUDA(cudaStreamSynchronize(own_stream));
@@ -917,7 +924,7 @@ void KoszulCtx::i8_run(bool forward_dir, int in_buf, int out_buf, bool scale, cu
         D.p.out[pl] = i8->planes[out_buf][pl];
     }
     D.p.diag = (!forward_dir && scale) ? d_diag : nullptr;
-    dispatch_i8_nb(nb, [&](auto NBc) { launch_i8<decltype(NBc)::value>(*this, D, st); });
+    dispatch_i8_nb(nbi, [&](auto NBc) { launch_i8<decltype(NBc)::value>(*this, D, st); });
 }
 
 void KoszulCtx::i8_check_error() {
@@ -933,12 +940,12 @@ int KoszulCtx::i8_dim(int buf) const { return buf == I8_Z ? co : ci; }
 uint64_t KoszulCtx::i8_rows(int buf) const { return buf == I8_Z ? n_tgt : n_src; }
 
 void KoszulCtx::i8_to_limbs(const uint32_t* in, int buf, cudaStream_t st) {
-    const uint64_t count = i8_rows(buf) * nb;
+    const uint64_t count = i8_rows(buf) * nbi;
     unsigned grid = static_cast<unsigned>(std::min<uint64_t>((count + 255) / 256, static_cast<uint64_t>(sms) * 8));
     int8_t** pl = i8->planes[buf];
-    dispatch_i8_nb(nb, [&](auto NBc) {
+    dispatch_i8_nb(nbi, [&](auto NBc) {
         to_limbs_kernel<decltype(NBc)::value><<<std::max(grid, 1u), 256, 0, st>>>(
-            in, pl[0], pl[1], pl[2], pl[3], static_cast<long long>(count), i8_dim(buf), mod);
+            in, pl[0], pl[1], pl[2], pl[3], static_cast<long long>(count), i8_dim(buf), nb, mod);
     });
     BW_CHECK_LAUNCH();
     ++launches;
@@ -948,9 +955,9 @@ void KoszulCtx::i8_from_limbs(int buf, uint32_t* out, cudaStream_t st) {
     const uint64_t count = i8_rows(buf) * nb;
     unsigned grid = static_cast<unsigned>(std::min<uint64_t>((count + 255) / 256, static_cast<uint64_t>(sms) * 8));
     int8_t** pl = i8->planes[buf];
-    dispatch_i8_nb(nb, [&](auto NBc) {
+    dispatch_i8_nb(nbi, [&](auto NBc) {
         from_limbs_kernel<decltype(NBc)::value><<<std::max(grid, 1u), 256, 0, st>>>(
-            pl[0], pl[1], out, static_cast<long long>(count), i8_dim(buf), mod);
+            pl[0], pl[1], out, static_cast<long long>(count), i8_dim(buf), nb, mod);
     });
     BW_CHECK_LAUNCH();
     ++launches;
@@ -974,7 +981,7 @@ void KoszulCtx::i8_project(int buf, cudaStream_t st) {
     P.counter = d_counter;
     P.seq = d_seq;
     P.seq_index = d_seq_index;
-    dispatch_i8_nb(nb, [&](auto NBc) {
+    dispatch_i8_nb(nbi, [&](auto NBc) {
         i8_project_tc_kernel<decltype(NBc)::value><<<i8->proj_grid, kProjThreads, i8->proj_smem, st>>>(P);
     });
     BW_CHECK_LAUNCH();
