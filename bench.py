@@ -40,6 +40,8 @@ DESCRIPTIONS = {
     "config2": "synthetic Koszul genus-20-like: r=19 k=9 dim 20->28 p=32003 block 16x16 (N=1,847,560)",
     "config5": "synthetic Koszul genus-24/26-like: r=23 k=11 dim 32->40 p=32003 block 32x32 (N=43,266,496)",
     "config1": "synthetic Koszul small: r=10 k=4 dim 16->24 p=32003 block 8x8 (N=3,360)",
+    "config3": "batch of 24 synthetic sectors: r in {19,20,21}, k in {8,9,10}, dim R_q ~ U[12,40], "
+               "dim R_(q+1) = dim R_q + 8, block widths 8/16/32, p=32003, own seeded maps/D/X/Y each",
 }
 METRIC = "block-Wiedemann steps/s, INT8-limb TC vs plain CUDA-core, bit-exact; %HBM peak"
 
@@ -47,13 +49,17 @@ METRIC = "block-Wiedemann steps/s, INT8-limb TC vs plain CUDA-core, bit-exact; %
 def parse():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 2000; config5: 20; config3: 32 batch steps)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--form", choices=["int8", "plain", "auto"], default="auto")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["config3"], default="config2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.steps is None:
+        args.steps = {"config5": 20, "config3": 32}.get(args.workload, 2000)
+    return args
 
 
 def binom(n, k):
@@ -168,14 +174,27 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    sh = shape_of(args.workload)
     vals = []
     info = None
-    for i in range(args.warmup + args.steps):
-        v, threads, text = cpu_sample(sh)
-        if i >= args.warmup:
-            vals.append(v)
-            info = (threads, text)
+    if args.workload == "config3":
+        # every sector sampled at 1/64 of its subsets; value = sector-steps/s of the whole batch
+        secs = config3_sectors()
+        for i in range(args.warmup + min(args.steps, 3)):
+            total, threads = 0.0, 1
+            for sec in secs:
+                v, threads, _ = cpu_sample(sec, fraction=1 / 64)
+                total += 1.0 / v
+            if i >= args.warmup:
+                vals.append(len(secs) / total)
+                info = (threads, f"each of the {len(secs)} sectors: forward and transpose over 1/64 of its subsets, "
+                                 f"scaled to one full step; value = sectors / sum of full-step times")
+    else:
+        sh = shape_of(args.workload)
+        for i in range(args.warmup + args.steps if args.steps <= 40 else args.warmup + 40):
+            v, threads, text = cpu_sample(sh)
+            if i >= args.warmup:
+                vals.append(v)
+                info = (threads, text)
     value = statistics.median(vals)
     threads, text = info
     line = {
@@ -183,11 +202,150 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (u64 accumulate)",
         "data": "synthetic (seeded uniform residues)",
-        "config": {"workload": args.workload, "description": DESCRIPTIONS[args.workload], "parallelism": "cpu"},
+        "config": {"workload": args.workload, "description": DESCRIPTIONS[args.workload], "parallelism": "cpu",
+                   "samples": len(vals)},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port", "sample": text},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def config3_sectors(seed=300, count=24):
+    """The batched workload's sector shapes (seeded draw; each sector its own input seed)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        r = int(rng.choice([19, 20, 21]))
+        k = int(rng.choice([8, 9, 10]))
+        ci = int(rng.integers(12, 41))
+        nb = int(rng.choice([8, 16, 32]))
+        n_src, n_tgt = binom(r, k) * ci, binom(r, k - 1) * (ci + 8)
+        out.append(dict(r=r, k=k, ci=ci, co=ci + 8, p=32003, n=nb, m=nb, seed=3000 + i, n_src=n_src, n_tgt=n_tgt))
+    return out
+
+
+def run_batch(args):
+    """Config 3: 24 sectors advanced together (one CUDA graph per 16 batch steps)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from prym_green_ancillary_b200 import KoszulBatch, seeded_fill_device, seeded_fill_host, TAG_DIAG, TAG_MAPS, TAG_X, TAG_Y
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    secs = config3_sectors()
+    form = "int8" if args.form == "auto" else args.form
+    specs, xs, ys = [], [], []
+    for sec in secs:
+        seed = sec["seed"] + 100000 * rank
+        maps = seeded_fill_host(sec["r"] * sec["co"] * sec["ci"], seed, TAG_MAPS, sec["p"])
+        diag = torch.empty(sec["n_src"], dtype=torch.int32, device=dev)
+        seeded_fill_device(diag, seed, TAG_DIAG, sec["p"], 1)
+        x = torch.empty((sec["n_src"], sec["m"]), dtype=torch.int32, device=dev)
+        y = torch.empty((sec["n_src"], sec["n"]), dtype=torch.int32, device=dev)
+        seeded_fill_device(x, seed, TAG_X, sec["p"])
+        seeded_fill_device(y, seed, TAG_Y, sec["p"])
+        specs.append(dict(r=sec["r"], k=sec["k"], dim_in=sec["ci"], dim_out=sec["co"], prime=sec["p"],
+                          block_width=sec["n"], proj_width=sec["m"], maps=maps, diag=diag, form=form))
+        xs.append(x)
+        ys.append(y)
+    K, W = args.steps, args.warmup
+    batch = KoszulBatch(specs, device=local)
+    seqs = [torch.zeros((1 + W + K + 8, s["m"], s["n"]), dtype=torch.int32, device=dev) for s in secs]
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.synchronize()
+    batch.seq_start(xs, ys, seqs, stream=stream)
+    batch.seq_step(W, stream=stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches0 = batch.launch_count
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        batch.seq_step(K, stream=stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = batch.launch_count - launches0
+    batch.seq_finish(stream=stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # End to end: X and Y0 of every sector from pinned host memory, sequences back, K batch steps.
+    xh = [torch.empty(x.shape, dtype=torch.int32, pin_memory=True).copy_(x) for x in xs]
+    yh = [torch.empty(y.shape, dtype=torch.int32, pin_memory=True).copy_(y) for y in ys]
+    seqh = [torch.empty((K + 1,) + tuple(s.shape[1:]), dtype=torch.int32, pin_memory=True) for s in seqs]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for i in range(len(secs)):
+            xs[i].copy_(xh[i], non_blocking=True)
+            ys[i].copy_(yh[i], non_blocking=True)
+    batch.seq_start(xs, ys, seqs, stream=stream)
+    batch.seq_step(K, stream=stream)
+    batch.seq_finish(stream=stream)
+    with torch.cuda.stream(stream):
+        for i in range(len(secs)):
+            seqh[i].copy_(seqs[i][:K + 1], non_blocking=True)
+    stream.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = sum(x.numel() * 4 + y.numel() * 4 for x, y in zip(xh, yh)) / K
+    d2h = sum(s.numel() * 4 for s in seqh) / K
+
+    step_bytes = sum(algorithmic(s)["step_bytes"] for s in secs)
+    macs = sum(algorithmic(s)["macs"] for s in secs)
+    peak, peak_kind = measured_peaks()
+    step_ms = ms / K
+    n_sec = len(secs)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * K * n_sec / (ms / 1e3), "unit": "steps/s", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int8 limbs, int32 accumulate" if form == "int8" else "int32",
+            "data": "synthetic (seeded uniform residues, counter-based stream)",
+            "config": {"workload": "config3", "description": DESCRIPTIONS["config3"], "form": form,
+                       "sectors": n_sec, "step": "one batch step advances all sectors by one step; value counts "
+                                                 "sector-steps (batch steps/s x sectors)",
+                       "batch_steps_per_s": world * K / (ms / 1e3),
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "working set per batch step far exceeds the 126 MB L2; no flush needed",
+                       "shapes": [[s["r"], s["k"], s["ci"], s["co"], s["n"]] for s in secs]},
+            "step_bytes": step_bytes, "step_macs": macs,
+            "hbm_frac_step": step_bytes / (step_ms / 1e3) / 1e9 / peak,
+            "roofline": {"bound": "hbm", "kernel": "batch step (all sectors' kernels, one graph per 16 steps)",
+                         "achieved": step_bytes / (step_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+            "cpu_baseline": None,
+            "e2e": {"value": world * K * n_sec / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "note": "pinned host X, Y0 of every sector in, all sequences out, K batch steps"},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
@@ -334,6 +492,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "config3":
+        return run_batch(args)
     return run_engine(args)
 
 

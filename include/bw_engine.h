@@ -136,6 +136,27 @@ BW_API int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* ms_ou
 /* Number of engine kernel launches issued by this context since creation. */
 BW_API uint64_t bw_koszul_launch_count(const bw_koszul* ctx);
 
+/* Batch of synthetic operators ("sectors" of uneven shapes, block widths and
+ * forms) whose sequences advance together: every batch step advances every
+ * sector by one step, and 16 steps of all sectors run as one CUDA graph with
+ * one branch per sector.  Replaces the reference's one-process-per-sector
+ * scheduling of the sequence stage (scripts/reproduce.py:235-259) for the
+ * synthetic operator; each sector's arithmetic is that of bw_koszul_*.
+ * d_x[i], d_y0[i], d_seq[i] and d_y_out[i] are sector i's buffers as for
+ * bw_koszul_seq_*; seq_capacity applies to every sector. */
+typedef struct bw_koszul_batch bw_koszul_batch;
+BW_API int bw_koszul_batch_create(const bw_koszul_desc* descs, uint32_t count, int device, bw_koszul_batch** out);
+BW_API void bw_koszul_batch_destroy(bw_koszul_batch* batch);
+/* Borrowed handle of sector `index` (bw_koszul_info_get, single applications
+ * outside a session); valid until the batch is destroyed; do not destroy it. */
+BW_API int bw_koszul_batch_sector(bw_koszul_batch* batch, uint32_t index, bw_koszul** out);
+BW_API int bw_koszul_batch_seq_start(bw_koszul_batch* batch, const uint32_t* const* d_x, const uint32_t* const* d_y0,
+                                     uint32_t* const* d_seq, uint64_t seq_capacity, void* stream);
+BW_API int bw_koszul_batch_seq_step(bw_koszul_batch* batch, uint64_t steps, void* stream);
+BW_API int bw_koszul_batch_seq_finish(bw_koszul_batch* batch, uint32_t* const* d_y_out, uint64_t* nlen_out,
+                                      void* stream);
+BW_API uint64_t bw_koszul_batch_launch_count(const bw_koszul_batch* batch);
+
 /* ------------------------------------------------------------------------
  * Paper mode: the eliminated cyclic operator of one sector,
  *   F(x, z) = D_(m-1)(B z - R D_m x),  S = Dc F^t T^t Dr T F Dc,

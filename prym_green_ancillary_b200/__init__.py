@@ -9,6 +9,7 @@ from .engine import (  # noqa: F401
     EngineError,
     FORM_INT8,
     FORM_PLAIN,
+    KoszulBatch,
     KoszulEngine,
     CyclicEngine,
     read_text,

@@ -67,6 +67,12 @@ __global__ void seeded_fill_kernel(uint32_t* __restrict__ out, uint64_t count, u
         out[i] = seeded_residue_from_base(base, i, p, lo);
 }
 
+int max_dynamic_smem(int device) {
+    int v = 0;
+    BW_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    return v;
+}
+
 }  // namespace bw
 
 using namespace bw;

@@ -19,6 +19,9 @@ struct Error : std::runtime_error {
 
 void set_last_error(const std::string& msg);
 
+// Largest dynamic shared memory a block may opt into on `device`.
+int max_dynamic_smem(int device);
+
 #define BW_CUDA(call)                                                              \
     do {                                                                           \
         cudaError_t bw_err_ = (call);                                              \
@@ -34,6 +37,19 @@ void set_last_error(const std::string& msg);
     do {                                                                           \
         if (!(cond)) throw ::bw::Error(msg, 3);                                    \
     } while (0)
+
+// Kernels that use dynamic shared memory get the largest limit the device
+// allows them (the opt-in maximum less their static shared memory): the
+// per-function limit is process-wide, so setting one context's own size could
+// lower it under another context's launches of the same kernel.  Returns it.
+template <class Kernel>
+int allow_dynamic_smem(Kernel kernel, int device) {
+    cudaFuncAttributes a{};
+    BW_CUDA(cudaFuncGetAttributes(&a, kernel));
+    const int cap = max_dynamic_smem(device) - static_cast<int>(a.sharedSizeBytes);
+    BW_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+    return cap;
+}
 
 // Every C-ABI entry point runs its body through this wrapper: exceptions never
 // cross the ABI; the message goes to the thread-local last-error slot.

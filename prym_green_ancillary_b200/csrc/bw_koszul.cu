@@ -263,7 +263,8 @@ void launch_gather(KoszulCtx& c, const int32_t* in, int32_t* out, const uint32_t
     const int tpb = (outer4 / 4) * (NB / 4);
     BW_REQUIRE(tpb <= 256, "dimension too large for the plain gather kernel (dim/4 * n/4 > 256)");
     const int bpc = 256 / tpb;
-    BW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    BW_REQUIRE(static_cast<int>(smem) <= allow_dynamic_smem(kern, c.device),
+               "maps too large for shared memory staging");
     int occ = 0;
     BW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, smem));
     BW_REQUIRE(occ > 0, "plain gather kernel does not fit on an SM");
@@ -487,7 +488,8 @@ KoszulCtx* KoszulCtx::create(const bw_koszul_desc& d, int dev) {
     c->proj_grid = static_cast<unsigned>(std::min<uint64_t>(static_cast<uint64_t>(c->sms) * 4,
                                                             std::max<uint64_t>(1, (c->n_src + 255) / 256)));
     const uint64_t scratch_before = c->device_bytes;
-    c->d_partials = c->alloc<int32_t>(static_cast<uint64_t>(c->proj_grid) * c->m * std::max(c->nb, c->nbi));
+    // per-CTA partial sums: the plain projection's grid, or up to one CTA per SM for the INT8 form
+    c->d_partials = c->alloc<int32_t>(std::max<uint64_t>(c->proj_grid, c->sms) * c->m * std::max(c->nb, c->nbi));
     c->d_counter = c->alloc<unsigned int>(1);
     c->d_seq_index = c->alloc<unsigned long long>(1);
     c->scratch_bytes = c->device_bytes - scratch_before;
@@ -601,10 +603,6 @@ void KoszulCtx::seq_finish(uint32_t* y_out, uint64_t* nlen_out, cudaStream_t st)
 // ------------------------------------------------------------------ C ABI
 
 using namespace bw;
-
-struct bw_koszul {
-    KoszulCtx* impl;
-};
 
 // A NULL stream means "ordered like the legacy default stream": the call's
 // work runs on the context's own stream after everything issued before it on

@@ -95,3 +95,8 @@ struct KoszulCtx {
 };
 
 }  // namespace bw
+
+// Opaque handle of the C ABI (include/bw_engine.h).
+struct bw_koszul {
+    bw::KoszulCtx* impl;
+};

@@ -77,7 +77,7 @@ struct I8Dir {
     int r, inner, outer, half;   // N = 2 * half, half = outer rounded up to 16
     int gi;                      // generators per stage
     int stages_per_tile;         // ceil(r / gi)
-    int ks_full;                 // K-steps of a full stage (gi * inner / 32)
+    int ks_full;                 // K-steps of a full stage (gi * inner rows padded to a multiple of 32)
     int ks_last;                 // K-steps of the last stage
     int slots;                   // pipeline depth
     uint32_t b_bytes, slot_bytes, limb_bytes;
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         tc::tmem_alloc(tmem_slot, tmem_cols);
         tc::tmem_relinquish();
     }
-    const int KS = P.gi * P.inner;                       // K' rows of a slot
+    const int KS = P.ks_full * 32;                       // K' rows of a slot group (gi * inner, padded)
     for (int w = threadIdx.x; w < KS; w += blockDim.x) il_of_row[w] = static_cast<uint8_t>(w / P.inner);
     tc::tc_fence_before();
     __syncthreads();
@@ -681,15 +681,6 @@ __global__ void x_tiles_kernel(const uint32_t* __restrict__ X, int8_t* __restric
     }
 }
 
-int gcd_int(int a, int b) {
-    while (b) {
-        int t = a % b;
-        a = b;
-        b = t;
-    }
-    return a;
-}
-
 template <class F>
 void dispatch_i8_nb(int nb, F&& f) {
     switch (nb) {
@@ -729,19 +720,29 @@ void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     P.half = (outer + 15) / 16 * 16;
     const int N = 2 * P.half;
     BW_REQUIRE(N <= 256, "INT8 form: output dimension above 128 is not supported");
-    const int base_g = 32 / gcd_int(inner, 32);
-    // grow the stage towards ~40 KB of A per slot
-    int gi = base_g;
-    auto slot_bytes_for = [&](int g) { return static_cast<size_t>(2) * 8 * (g * inner) * 16; };
-    while (gi * 2 <= std::max(base_g, c.r) && slot_bytes_for(gi * 2) <= 48 * 1024) gi *= 2;
+    // Stage = gi generators: gi * inner K' rows, padded to whole K-steps of 32
+    // (the padding rows of B are zero, so the A rows there may hold anything).
+    // Pick the best-filled stage of at most 56 KB of A per slot, the largest
+    // such gi on ties.
+    int gi = 1;
+    double best_fill = -1;
+    for (int g = 1; g <= c.r; ++g) {
+        const int rows = g * inner, padded = (rows + 31) / 32 * 32;
+        if (g > 1 && static_cast<size_t>(2) * 8 * padded * 16 > 56 * 1024) break;
+        const double fill = static_cast<double>(rows) / padded;
+        if (fill > best_fill - 1e-9) {
+            best_fill = std::max(best_fill, fill);
+            gi = g;
+        }
+    }
     P.gi = gi;
     P.stages_per_tile = (c.r + gi - 1) / gi;
-    P.ks_full = gi * inner / 32;
+    P.ks_full = (gi * inner + 31) / 32;
     const int last_g = c.r - (P.stages_per_tile - 1) * gi;
     P.ks_last = (last_g * inner + 31) / 32;
     const int total_ks = (P.stages_per_tile - 1) * P.ks_full + P.ks_last;
     P.b_bytes = static_cast<uint32_t>(total_ks) * N * 32;
-    P.limb_bytes = static_cast<uint32_t>(8 * gi * inner * 16);
+    P.limb_bytes = static_cast<uint32_t>(8 * P.ks_full * 32 * 16);
     P.slot_bytes = 2 * P.limb_bytes;
     BW_REQUIRE(gi * inner <= kMaxRowTable, "INT8 form: stage too deep for the row table");
     const size_t extra = (2 * 8 + 2 * 2 + 1) * 8 + 16 + kMaxRowTable;
@@ -832,7 +833,8 @@ void plan_projection(KoszulCtx& c, KoszulCtx::I8State& S) {
     P.c2 = to_balanced(static_cast<uint32_t>((255ull * 255ull) % c.p), c.mod);
     P.err = S.err;
     S.proj_grid = static_cast<unsigned>(std::max(1, std::min(P.n_stages, c.sms)));
-    BW_REQUIRE(S.proj_grid <= c.proj_grid, "INT8 form: projection grid above the partials buffer");
+    BW_REQUIRE(S.proj_grid <= std::max<unsigned>(c.proj_grid, static_cast<unsigned>(c.sms)),
+               "INT8 form: projection grid above the partials buffer");
     S.xt = c.alloc<int8_t>(static_cast<uint64_t>(P.n_stages) * P.a_bytes);
     P.xt = S.xt;
 }
@@ -903,11 +905,11 @@ void KoszulCtx::i8_setup() {
     S.fwd.p.n_blk = static_cast<long long>(n_t);
     S.bwd.p.n_blk = static_cast<long long>(n_s);
     dispatch_i8_nb(nbi, [&](auto NBc) {
-        auto kern = i8_gather_gemm_kernel<decltype(NBc)::value>;
-        const int need = static_cast<int>(std::max(S.fwd.smem, S.bwd.smem));
-        BW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
-        BW_CUDA(cudaFuncSetAttribute(i8_project_tc_kernel<decltype(NBc)::value>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S.proj_smem)));
+        const int cap_g = allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value>, device);
+        const int cap_p = allow_dynamic_smem(i8_project_tc_kernel<decltype(NBc)::value>, device);
+        BW_REQUIRE(static_cast<int>(std::max(S.fwd.smem, S.bwd.smem)) <= cap_g &&
+                       static_cast<int>(S.proj_smem) <= cap_p,
+                   "INT8 form: shared-memory plan above the device limit");
     });
     const int bt = 128 / nbi;
     S.fwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_t + bt - 1) / bt, sms)));

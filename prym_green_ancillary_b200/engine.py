@@ -68,6 +68,13 @@ SIGNATURES = {
     "bw_koszul_sequence_host": (_INT, [_VP, _VP, _VP, _U64, _VP, _VP]),
     "bw_koszul_seq_step_timed": (_INT, [_VP, _U64, ctypes.POINTER(ctypes.c_float), _VP]),
     "bw_koszul_launch_count": (_U64, [_VP]),
+    "bw_koszul_batch_create": (_INT, [_VP, _U32, _INT, ctypes.POINTER(_VP)]),
+    "bw_koszul_batch_destroy": (None, [_VP]),
+    "bw_koszul_batch_sector": (_INT, [_VP, _U32, ctypes.POINTER(_VP)]),
+    "bw_koszul_batch_seq_start": (_INT, [_VP, _VP, _VP, _VP, _U64, _VP]),
+    "bw_koszul_batch_seq_step": (_INT, [_VP, _U64, _VP]),
+    "bw_koszul_batch_seq_finish": (_INT, [_VP, _VP, ctypes.POINTER(_U64), _VP]),
+    "bw_koszul_batch_launch_count": (_U64, [_VP]),
     "bw_cyclic_open": (_INT, [ctypes.c_char_p, ctypes.c_char_p, _U32, _U32, _U64, _U32, _U64, ctypes.c_char_p,
                               ctypes.c_char_p, _INT, ctypes.POINTER(_VP)]),
     "bw_cyclic_info_get": (_INT, [_VP, _VP]),
@@ -151,6 +158,19 @@ def seeded_fill_device(out, seed, tag, p, lo=0, stream=None):
     return out
 
 
+def _koszul_desc(r, k, dim_in, dim_out, prime, block_width, proj_width, form, maps, diag):
+    """bw_koszul_desc for the arguments, and the arrays it points into (keep them alive)."""
+    maps = np.ascontiguousarray(maps, dtype=np.uint32).reshape(-1)
+    desc = KoszulDesc(r, k, dim_in, dim_out, prime, block_width, proj_width, FORMS[form], maps.ctypes.data, 0, 0)
+    if isinstance(diag, np.ndarray):
+        diag = np.ascontiguousarray(diag, dtype=np.uint32)
+        desc.diag = diag.ctypes.data
+    else:
+        desc.diag = diag.data_ptr()
+        desc.diag_on_device = 1
+    return desc, (maps, diag)
+
+
 class KoszulEngine:
     """Synthetic Koszul operator S = D d^T d on one GPU (see include/bw_engine.h).
 
@@ -166,28 +186,33 @@ class KoszulEngine:
         self.m = block_width if proj_width is None else proj_width
         self.form = form
         self.device = device
-        maps = np.ascontiguousarray(maps, dtype=np.uint32).reshape(-1)
-        desc = KoszulDesc(r, k, dim_in, dim_out, prime, self.nb, self.m, FORMS[form],
-                          maps.ctypes.data, 0, 0)
-        if isinstance(diag, np.ndarray):
-            diag = np.ascontiguousarray(diag, dtype=np.uint32)
-            desc.diag = diag.ctypes.data
-        else:
-            desc.diag = diag.data_ptr()
-            desc.diag_on_device = 1
+        desc, self._keep = _koszul_desc(r, k, dim_in, dim_out, prime, self.nb, self.m, form, maps, diag)
         handle = ctypes.c_void_p()
         _check(lib.bw_koszul_create(ctypes.byref(desc), device, ctypes.byref(handle)))
         self._h = handle
+        self._read_info()
+
+    @classmethod
+    def _borrowed(cls, handle, r, k, dim_in, dim_out, prime, block_width, proj_width, form, device):
+        """A view of a batch sector (the batch owns the context)."""
+        eng = cls.__new__(cls)
+        eng.r, eng.k, eng.dim_in, eng.dim_out, eng.p = r, k, dim_in, dim_out, prime
+        eng.nb, eng.m, eng.form, eng.device = block_width, proj_width, form, device
+        eng._h, eng._owned = handle, False
+        eng._read_info()
+        return eng
+
+    def _read_info(self):
         info = KoszulInfo()
-        _check(lib.bw_koszul_info_get(self._h, ctypes.byref(info)))
+        _check(load().bw_koszul_info_get(self._h, ctypes.byref(info)))
         self.n_src, self.n_tgt = int(info.n_src), int(info.n_tgt)
         self.device_bytes, self.scratch_bytes = int(info.device_bytes), int(info.scratch_bytes)
         self.sm_count = int(info.sm_count)
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and getattr(self, "_owned", True):
             load().bw_koszul_destroy(self._h)
-            self._h = None
+        self._h = None
 
     __del__ = close
 
@@ -241,6 +266,74 @@ class KoszulEngine:
     @property
     def launch_count(self):
         return int(load().bw_koszul_launch_count(self._h))
+
+
+class KoszulBatch:
+    """Sectors of uneven shapes advanced together (bw_koszul_batch_*).
+
+    ``sectors`` is a list of dicts with the KoszulEngine arguments (r, k,
+    dim_in, dim_out, prime, block_width, proj_width, maps, diag, form).
+    """
+
+    def __init__(self, sectors, device=0):
+        lib = load()
+        descs = (KoszulDesc * len(sectors))()
+        self._keep = []
+        for i, sec in enumerate(sectors):
+            sec = dict(sec)
+            sec.setdefault("proj_width", sec["block_width"])
+            sec.setdefault("form", "int8")
+            d, keep = _koszul_desc(sec["r"], sec["k"], sec["dim_in"], sec["dim_out"], sec["prime"],
+                                   sec["block_width"], sec["proj_width"], sec["form"], sec["maps"], sec["diag"])
+            descs[i] = d
+            self._keep.append(keep)
+        handle = ctypes.c_void_p()
+        _check(lib.bw_koszul_batch_create(descs, len(sectors), device, ctypes.byref(handle)))
+        self._h = handle
+        self.engines = []
+        for i, sec in enumerate(sectors):
+            h = ctypes.c_void_p()
+            _check(lib.bw_koszul_batch_sector(self._h, i, ctypes.byref(h)))
+            self.engines.append(KoszulEngine._borrowed(
+                h, sec["r"], sec["k"], sec["dim_in"], sec["dim_out"], sec["prime"], sec["block_width"],
+                sec.get("proj_width", sec["block_width"]), sec.get("form", "int8"), device))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for e in self.engines:
+                e._h = None
+            load().bw_koszul_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def _ptrs(tensors):
+        return (ctypes.c_void_p * len(tensors))(*[t.data_ptr() if t is not None else None for t in tensors])
+
+    def seq_start(self, xs, ys, seqs, stream=None):
+        cap = min(s.numel() // (e.m * e.nb) for s, e in zip(seqs, self.engines))
+        self._arrays = (self._ptrs(xs), self._ptrs(ys), self._ptrs(seqs))
+        _check(load().bw_koszul_batch_seq_start(self._h, *self._arrays, cap, _stream_ptr(stream)))
+
+    def seq_step(self, steps, stream=None):
+        _check(load().bw_koszul_batch_seq_step(self._h, steps, _stream_ptr(stream)))
+
+    def seq_finish(self, y_outs=None, stream=None):
+        n = ctypes.c_uint64()
+        ptrs = self._ptrs(y_outs) if y_outs is not None else None
+        _check(load().bw_koszul_batch_seq_finish(self._h, ptrs, ctypes.byref(n), _stream_ptr(stream)))
+        return int(n.value)
+
+    @property
+    def launch_count(self):
+        return int(load().bw_koszul_batch_launch_count(self._h))
 
 
 def read_text(path):

@@ -193,3 +193,26 @@ def test_session_graph_path_matches_direct(form):
         # a second session on the same context (graphs are rebuilt)
         seq2, _ = eng.sequence_host(X, Y, nlen)
         np.testing.assert_array_equal(seq2, want)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_contexts_of_different_shapes_coexist(form):
+    """Per-kernel launch limits are process-wide: a context created after a
+    larger one must not break the larger one's launches."""
+    big = oracle.KoszulShape(6, 3, 40, 48, 32003, 32, 32)
+    small = oracle.KoszulShape(7, 3, 5, 6, 32003, 16, 16)
+    dev = torch.device("cuda", 0)
+    engines = []
+    for shape in (big, small):
+        maps, diag, X, Y = oracle.seeded_problem(shape, 21)
+        engines.append((shape, maps, diag, Y, _engine(shape, maps, diag, form)))
+    try:
+        for shape, maps, diag, Y, eng in engines:   # the large context runs after the small one was created
+            y = torch.from_numpy(Y.view(np.int32)).to(dev)
+            out = torch.empty_like(y)
+            eng.apply(y, out)
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), oracle.apply(shape, maps, diag, Y))
+    finally:
+        for *_, eng in engines:
+            eng.close()
