@@ -44,6 +44,9 @@ DESCRIPTIONS = {
                "dim R_(q+1) = dim R_q + 8, block widths 8/16/32, p=32003, own seeded maps/D/X/Y each",
 }
 METRIC = "block-Wiedemann steps/s, INT8-limb TC vs plain CUDA-core, bit-exact; %HBM peak"
+# Paper mode (the eliminated cyclic operator of one sector of the shipped instances, block width 4):
+# name -> default timed steps (applications of S; two per round of 4 moments)
+PAPER = {"g20": 2000, "g22": 2000, "g24": 2000, "g26": 800, "g28": 200, "g30": 40}
 
 
 def parse():
@@ -54,11 +57,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--form", choices=["int8", "plain", "auto"], default="auto")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["config3"], default="config2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["config3"] + sorted(PAPER), default="config2")
+    ap.add_argument("--sector", type=int, default=0, help="paper workloads: the sector")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"config5": 20, "config3": 32}.get(args.workload, 2000)
+        args.steps = {"config5": 20, "config3": 32}.get(args.workload, PAPER.get(args.workload, 2000))
     return args
 
 
@@ -349,6 +353,79 @@ def run_batch(args):
     return 0
 
 
+def run_paper(args):
+    """Paper mode: the eliminated operator of one sector of a shipped instance.
+
+    A step is one application of S = Dc F^t T^t Dr T F Dc to the 4-wide block
+    with its Gram moments (two steps per round of four moments, as the
+    reference's loop); K steps are K/2 rounds from the seeded initial block.
+    """
+    import torch
+    from prym_green_ancillary_b200 import CyclicEngine
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    path = ROOT / "prym_green_ancillary_b200" / "_data" / f"{args.workload}.json"
+    if not path.exists():
+        raise SystemExit(f"{path} missing: build() stages the shipped instances from a reference checkout")
+    sector = args.sector + rank   # every rank its own sector (no collective)
+    t_open = time.perf_counter()
+    eng = CyclicEngine(path, sector, device=local)
+    t_open = time.perf_counter() - t_open
+    info = eng.info
+    rounds_w, rounds_k = max(1, args.warmup // 2), max(1, args.steps // 2)
+    K = 2 * rounds_k
+    eng.generate_timed(1 + 4 * rounds_w)   # warm-up (also captures the round graph)
+    l0 = eng.launch_count
+    with ClockSampler(local) as clocks:
+        ms = eng.generate_timed(1 + 4 * rounds_k)
+    launches = eng.launch_count - l0
+    t0 = time.perf_counter()
+    eng.generate(1 + 4 * rounds_k)
+    seq, cur = eng.download()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dev = torch.device("cuda", local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_s = float(t[0].item()), float(t[1].item())
+    rows, cols = info["rows"], info["cols"]
+    step_bytes = 2 * (rows + cols) * 4 * 4
+    peak, peak_kind = measured_peaks()
+    achieved = step_bytes / (ms / K / 1e3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * K / (ms / 1e3), "unit": "steps/s", "n_gpus": world, "steps": K,
+            "warmup": 2 * rounds_w, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32 balanced residues (canonical u32 in the WDM)",
+            "data": f"shipped instance {args.workload}.json, seeded preconditioners and block (paper recipe)",
+            "config": {"workload": args.workload, "sector": sector, "form": "paper (eliminated operator, v=4)",
+                       "rows": rows, "cols": cols, "rounds_timed": rounds_k, "open_s": t_open,
+                       "parallelism": f"sectors{world}" if world > 1 else "single",
+                       "l2": "per-step working set " + ("exceeds" if 3 * step_bytes > 126e6 else "fits in") +
+                             " the 126 MB L2 (no flush: successive steps touch every vector)"},
+            "step_bytes": step_bytes,
+            "hbm_frac_step": achieved / peak,
+            "roofline": {"bound": "hbm", "kernel": "apply of S + moments (one CUDA graph per round)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None,
+                         "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+            "cpu_baseline": None,
+            "e2e": {"value": world * K / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": cols * 4 * 4 / K,
+                    "d2h_bytes_per_step": (seq.nbytes + cur.nbytes) / K,
+                    "note": "bw_cyclic_generate + bw_cyclic_download (initial block in, moments and block out)"},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    return 0
+
+
 def run_engine(args):
     import numpy as np
     import torch
@@ -494,6 +571,8 @@ def main():
         return run_reference(args)
     if args.workload == "config3":
         return run_batch(args)
+    if args.workload in PAPER:
+        return run_paper(args)
     return run_engine(args)
 
 

@@ -211,6 +211,10 @@ BW_API int bw_cyclic_apply_host(bw_cyclic* ctx, int what, const uint32_t* in, ui
  * default 2 N_c / 4 + 50), rounded up to whole rounds of 4 moments like the
  * reference's hot loop (cuda/cuprym_cyclic.cu:2420-2450). */
 BW_API int bw_cyclic_generate(bw_cyclic* ctx, uint64_t nlen);
+/* bw_cyclic_generate that also returns the device time of the rounds (CUDA
+ * events around the round graphs on the context's stream, in ms); for
+ * measurement. */
+BW_API int bw_cyclic_generate_timed(bw_cyclic* ctx, uint64_t nlen, float* device_ms);
 
 /* Copies the packed moments (seq_len x 10, upper triangles in WDM order) and
  * the current block (cols x 4, row-major) to host buffers (either may be NULL). */

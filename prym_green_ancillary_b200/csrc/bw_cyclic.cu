@@ -842,7 +842,7 @@ void CyclicCtx::round() {
     gram(d_b, d_d, d_b, d_b, 2);
 }
 
-void CyclicCtx::generate(size_t nlen_target) {
+void CyclicCtx::generate(size_t nlen_target, float* device_ms) {
     const size_t nc = op_cols;
     const size_t default_nlen = (2 * nc) / num_v + 50;
     const size_t max_nlen = nlen_target == 0 ? default_nlen : nlen_target;
@@ -881,10 +881,25 @@ void CyclicCtx::generate(size_t nlen_target) {
             BW_CUDA(cudaGraphInstantiate(&graphs[0], graph, 0));
             cudaGraphDestroy(graph);
         }
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (device_ms) {
+            BW_CUDA(cudaEventCreate(&e0));
+            BW_CUDA(cudaEventCreate(&e1));
+            BW_CUDA(cudaEventRecord(e0, stream));
+        }
         for (size_t r = 0; r < rounds; ++r) {
             BW_CUDA(cudaGraphLaunch(graphs[0], stream));
             launches += graph_kernels;
         }
+        if (device_ms) {
+            BW_CUDA(cudaEventRecord(e1, stream));
+            BW_CUDA(cudaEventSynchronize(e1));
+            BW_CUDA(cudaEventElapsedTime(device_ms, e0, e1));
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+        }
+    } else if (device_ms) {
+        *device_ms = 0;
     }
     seq_len = 1 + 4 * rounds;
     BW_CUDA(cudaStreamSynchronize(stream));

@@ -120,7 +120,7 @@ struct CyclicCtx {
     void apply_square(const int32_t* in, int32_t* out);
     void gram(const int32_t* a1, const int32_t* c1, const int32_t* a2, const int32_t* c2, int count);
     void round();
-    void generate(size_t nlen_target);
+    void generate(size_t nlen_target, float* device_ms = nullptr);
     void download_state(std::vector<uint32_t>& current, std::vector<uint32_t>& packed);
     void apply_host(int what, const uint32_t* in, uint32_t* out);
     // kernel-vector recovery (bw_cyclic_recover.cu)

@@ -76,6 +76,15 @@ extern "C" int bw_cyclic_generate(bw_cyclic* ctx, uint64_t nlen) {
     });
 }
 
+extern "C" int bw_cyclic_generate_timed(bw_cyclic* ctx, uint64_t nlen, float* device_ms) {
+    return guarded([&] {
+        BW_REQUIRE(ctx && device_ms, "bw_cyclic_generate_timed: null argument");
+        ctx->impl->require_device();
+        BW_CUDA(cudaSetDevice(ctx->impl->device));
+        ctx->impl->generate(nlen, device_ms);
+    });
+}
+
 extern "C" int bw_cyclic_download(bw_cyclic* ctx, uint32_t* packed_seq, uint64_t seq_capacity, uint32_t* current) {
     return guarded([&] {
         BW_REQUIRE(ctx, "bw_cyclic_download: null context");

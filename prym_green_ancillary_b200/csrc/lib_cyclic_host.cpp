@@ -12,6 +12,7 @@
 #include <map>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 
 namespace bw {
 namespace cyclic {
@@ -125,13 +126,71 @@ uint64_t fnv_str(uint64_t h, const std::string& s) {
     return h;
 }
 
+// C(n, k) for n, k < 64 (0 when k > n; saturates at 2^64 - 1, never reached by
+// the subset counts that pass the u32 checks).
+struct BinomTable {
+    uint64_t c[64][64];
+    BinomTable() {
+        for (int n = 0; n < 64; ++n)
+            for (int k = 0; k < 64; ++k) {
+                if (k == 0) c[n][k] = 1;
+                else if (n == 0) c[n][k] = 0;
+                else {
+                    const uint64_t a = c[n - 1][k - 1], b = c[n - 1][k];
+                    c[n][k] = a > ~b ? ~0ULL : a + b;
+                }
+            }
+    }
+};
+const BinomTable& binoms() {
+    static const BinomTable t;
+    return t;
+}
+
+// Lexicographic rank of a k-subset of {0..n-1} given as a bit mask:
+// rank = C(n,k) - 1 - sum_pos C(n-1-s_pos, k-pos).
 uint64_t lex_rank_mask(uint64_t mask, size_t n, size_t k) {
-    // rank = C(n,k) - 1 - sum_pos C(n-1-s_pos, k-pos)
+    const BinomTable& B = binoms();
     uint64_t acc = 0;
     size_t pos = 0;
-    for (size_t v = 0; v < n && pos < k; ++v)
-        if (mask & (1ULL << v)) acc += binom64(n - 1 - v, k - pos++);
-    return binom64(n, k) - 1 - acc;
+    for (uint64_t m = mask; m && pos < k; m &= m - 1) {
+        const size_t v = static_cast<size_t>(__builtin_ctzll(m));
+        acc += B.c[n - 1 - v][k - pos++];
+    }
+    return B.c[n][k] - 1 - acc;
+}
+
+// The k-subset of {0..n-1} with lexicographic rank `rank` (inverse of lex_rank_mask).
+void lex_unrank_into(uint64_t rank, size_t n, size_t k, std::vector<size_t>& s) {
+    const BinomTable& B = binoms();
+    uint64_t rev = B.c[n][k] - 1 - rank;   // co-lexicographic index of the complement order
+    s.resize(k);
+    size_t v = 0;
+    for (size_t pos = 0; pos < k; ++pos) {
+        // smallest v with C(n-1-v, k-pos) <= rev
+        while (B.c[n - 1 - v][k - pos] > rev) ++v;
+        s[pos] = v;
+        rev -= B.c[n - 1 - v][k - pos];
+        ++v;
+    }
+}
+
+// Runs f(begin, end) over [0, n) in contiguous chunks on the host's cores.
+template <class F>
+void parallel_chunks(size_t n, F&& f) {
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t threads = std::min(hw, std::max<size_t>(1, n / 16384));
+    if (threads <= 1) {
+        f(size_t{0}, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t chunk = (n + threads - 1) / threads;
+    for (size_t t = 0; t < threads; ++t) {
+        const size_t b = t * chunk, e = std::min(n, b + chunk);
+        if (b < e) pool.emplace_back([&f, b, e] { f(b, e); });
+    }
+    for (auto& th : pool) th.join();
 }
 
 }  // namespace
@@ -236,65 +295,76 @@ Incidence build_incidences(size_t local_n, size_t degree, size_t r, const std::v
     inc.column_width = degree;
     inc.row_subset_weights.resize(inc.row_subsets);
     inc.column_subset_weights.resize(inc.column_subsets);
-    inc.row_i.reserve(inc.row_subsets * inc.row_width);
-    inc.row_col.reserve(inc.row_subsets * inc.row_width);
-    inc.row_neg.reserve(inc.row_subsets * inc.row_width);
-    inc.col_i.reserve(inc.column_subsets * degree);
-    inc.col_row.reserve(inc.column_subsets * degree);
-    inc.col_neg.reserve(inc.column_subsets * degree);
+    checked_u32(inc.column_subsets, "column rank");
+    checked_u32(inc.row_subsets, "row rank");
+    for (size_t li = 0; li < local_n; ++li) checked_u32(original[li], "incidence i");
+    inc.row_i.resize(inc.row_subsets * inc.row_width);
+    inc.row_col.resize(inc.row_subsets * inc.row_width);
+    inc.row_neg.resize(inc.row_subsets * inc.row_width);
+    inc.col_i.resize(inc.column_subsets * degree);
+    inc.col_row.resize(inc.column_subsets * degree);
+    inc.col_neg.resize(inc.column_subsets * degree);
 
-    // Enumerate (d-1)-subsets in lexicographic order.
-    std::vector<size_t> s(td);
-    for (size_t i = 0; i < td; ++i) s[i] = i;
-    for (uint64_t rank = 0; rank < inc.row_subsets; ++rank) {
-        uint64_t mask = 0;
-        size_t wsum = 0;
-        for (size_t v : s) {
-            mask |= 1ULL << v;
-            wsum += local_weights[v];
-        }
-        inc.row_subset_weights[rank] = static_cast<uint16_t>(wsum % r);
-        size_t position = 0;
-        for (size_t li = 0; li < local_n; ++li) {
-            if (mask & (1ULL << li)) {
-                ++position;
-                continue;
+    // (d-1)-subsets T in lexicographic order: for every i not in T, the column
+    // subset T u {i} and the sign (-1)^(number of elements of T below i).
+    // Chunks of ranks run on the host's cores; each starts from its first
+    // subset (unranked) and walks to the next combination.
+    parallel_chunks(inc.row_subsets, [&](size_t begin, size_t end) {
+        std::vector<size_t> s;
+        lex_unrank_into(begin, local_n, td, s);
+        for (uint64_t rank = begin; rank < end; ++rank) {
+            uint64_t mask = 0;
+            size_t wsum = 0;
+            for (size_t v : s) {
+                mask |= 1ULL << v;
+                wsum += local_weights[v];
             }
-            inc.row_i.push_back(checked_u32(original[li], "row incidence i"));
-            inc.row_col.push_back(checked_u32(lex_rank_mask(mask | (1ULL << li), local_n, degree), "column rank"));
-            inc.row_neg.push_back(static_cast<uint8_t>(position % 2 == 1));
+            inc.row_subset_weights[rank] = static_cast<uint16_t>(wsum % r);
+            size_t position = 0, q = rank * inc.row_width;
+            for (size_t li = 0; li < local_n; ++li) {
+                if (mask & (1ULL << li)) {
+                    ++position;
+                    continue;
+                }
+                inc.row_i[q] = static_cast<uint32_t>(original[li]);
+                inc.row_col[q] = static_cast<uint32_t>(lex_rank_mask(mask | (1ULL << li), local_n, degree));
+                inc.row_neg[q] = static_cast<uint8_t>(position % 2 == 1);
+                ++q;
+            }
+            if (td > 0 && rank + 1 < end) {   // next combination
+                size_t i = td;
+                while (i > 0 && s[i - 1] == local_n - td + i - 1) --i;
+                ++s[i - 1];
+                for (size_t j = i; j < td; ++j) s[j] = s[j - 1] + 1;
+            }
         }
-        // next combination
-        if (td > 0) {
-            size_t i = td;
-            while (i > 0 && s[i - 1] == local_n - td + i - 1) --i;
-            if (i == 0) break;
-            ++s[i - 1];
-            for (size_t j = i; j < td; ++j) s[j] = s[j - 1] + 1;
+    });
+    // d-subsets S: for every position of S, the row subset S \ {S_pos} and the sign (-1)^pos.
+    parallel_chunks(inc.column_subsets, [&](size_t begin, size_t end) {
+        std::vector<size_t> c;
+        lex_unrank_into(begin, local_n, degree, c);
+        for (uint64_t rank = begin; rank < end; ++rank) {
+            uint64_t mask = 0;
+            size_t wsum = 0;
+            for (size_t v : c) {
+                mask |= 1ULL << v;
+                wsum += local_weights[v];
+            }
+            inc.column_subset_weights[rank] = static_cast<uint16_t>(wsum % r);
+            for (size_t position = 0; position < degree; ++position) {
+                const size_t li = c[position], q = rank * degree + position;
+                inc.col_i[q] = static_cast<uint32_t>(original[li]);
+                inc.col_row[q] = static_cast<uint32_t>(lex_rank_mask(mask & ~(1ULL << li), local_n, td));
+                inc.col_neg[q] = static_cast<uint8_t>(position % 2 == 1);
+            }
+            if (rank + 1 < end) {
+                size_t i = degree;
+                while (i > 0 && c[i - 1] == local_n - degree + i - 1) --i;
+                ++c[i - 1];
+                for (size_t j = i; j < degree; ++j) c[j] = c[j - 1] + 1;
+            }
         }
-    }
-    std::vector<size_t> c(degree);
-    for (size_t i = 0; i < degree; ++i) c[i] = i;
-    for (uint64_t rank = 0; rank < inc.column_subsets; ++rank) {
-        uint64_t mask = 0;
-        size_t wsum = 0;
-        for (size_t v : c) {
-            mask |= 1ULL << v;
-            wsum += local_weights[v];
-        }
-        inc.column_subset_weights[rank] = static_cast<uint16_t>(wsum % r);
-        for (size_t position = 0; position < degree; ++position) {
-            const size_t li = c[position];
-            inc.col_i.push_back(checked_u32(original[li], "column incidence i"));
-            inc.col_row.push_back(checked_u32(lex_rank_mask(mask & ~(1ULL << li), local_n, td), "row rank"));
-            inc.col_neg.push_back(static_cast<uint8_t>(position % 2 == 1));
-        }
-        size_t i = degree;
-        while (i > 0 && c[i - 1] == local_n - degree + i - 1) --i;
-        if (i == 0) break;
-        ++c[i - 1];
-        for (size_t j = i; j < degree; ++j) c[j] = c[j - 1] + 1;
-    }
+    });
     return inc;
 }
 
@@ -528,48 +598,117 @@ void validate_rowmix_transpose_identity(const RowMixPlan& plan, size_t cols, uin
 Csr composite_target_preconditioner(const RowMixPlan& plan, const std::vector<uint32_t>& dr, uint32_t prime) {
     const size_t n = plan.target_rows;
     if (dr.size() != n) throw std::runtime_error("row preconditioner length does not match the rowmix plan");
-    // Sparse rows of T, built round by round: T <- T_k T.
-    std::vector<std::vector<std::pair<uint32_t, uint64_t>>> t(n);
-    for (size_t i = 0; i < n; ++i) t[i] = {{static_cast<uint32_t>(i), 1}};
-    auto combine = [&](const std::vector<std::pair<uint32_t, uint64_t>>& u, uint64_t cu,
-                       const std::vector<std::pair<uint32_t, uint64_t>>& v, uint64_t cv) {
-        std::map<uint32_t, uint64_t> acc;
-        for (auto& e : u) acc[e.first] = (acc[e.first] + cu * e.second) % prime;
-        for (auto& e : v) acc[e.first] = (acc[e.first] + cv * e.second) % prime;
-        std::vector<std::pair<uint32_t, uint64_t>> out;
-        for (auto& e : acc)
-            if (e.second) out.push_back(e);
-        return out;
+    if (plan.rounds > 6) throw std::runtime_error("at most 6 row-mixing rounds can be folded");
+    // T = T_R ... T_1 row by row: a round pairs disjoint rows, so every row has
+    // at most W = 2^R entries; rows are kept sorted by column.
+    const size_t W = size_t(1) << plan.rounds;
+    std::vector<uint32_t> tc(n * W), tv(n * W);
+    std::vector<uint8_t> tn(n, 1);
+    for (size_t i = 0; i < n; ++i) {
+        tc[i * W] = static_cast<uint32_t>(i);
+        tv[i * W] = 1;
+    }
+    const uint64_t p = prime;
+    // out = cu * row u + cv * row v (sorted merge, zeros dropped); returns the count
+    auto combine = [&](size_t u, uint64_t cu, size_t v, uint64_t cv, uint32_t* oc, uint32_t* ov) {
+        size_t a = 0, b = 0, k = 0;
+        const uint32_t *uc = &tc[u * W], *uv = &tv[u * W], *vc = &tc[v * W], *vv = &tv[v * W];
+        while (a < tn[u] || b < tn[v]) {
+            uint32_t col;
+            uint64_t val = 0;
+            if (b >= tn[v] || (a < tn[u] && uc[a] < vc[b])) {
+                col = uc[a];
+                val = cu * uv[a++] % p;
+            } else if (a >= tn[u] || vc[b] < uc[a]) {
+                col = vc[b];
+                val = cv * vv[b++] % p;
+            } else {
+                col = uc[a];
+                val = (cu * uv[a++] + cv * vv[b++]) % p;
+            }
+            if (val) {
+                oc[k] = col;
+                ov[k++] = static_cast<uint32_t>(val);
+            }
+        }
+        return k;
     };
     for (const auto& round : plan.round_pairs) {
-        for (const auto& pr : round) {
-            const uint64_t a = pr.a, b = pr.b, oab = (1 + a * b) % prime;
-            auto f = combine(t[pr.first], 1, t[pr.second], a);
-            auto s = combine(t[pr.first], b, t[pr.second], oab);
-            t[pr.first] = std::move(f);
-            t[pr.second] = std::move(s);
-        }
-    }
-    // P[i][j] = sum_k T[k][i] Dr[k] T[k][j]
-    std::vector<std::map<uint32_t, uint64_t>> rows(n);
-    for (size_t k = 0; k < n; ++k)
-        for (auto& ei : t[k])
-            for (auto& ej : t[k]) {
-                uint64_t v = ei.second * dr[k] % prime * ej.second % prime;
-                auto& slot = rows[ei.first][ej.first];
-                slot = (slot + v) % prime;
+        parallel_chunks(round.size(), [&](size_t begin, size_t end) {
+            std::vector<uint32_t> fc(W), fv(W), sc(W), sv(W);
+            for (size_t q = begin; q < end; ++q) {
+                const auto& pr = round[q];
+                const uint64_t a = pr.a, b = pr.b, oab = (1 + a * b) % p;
+                const size_t nf = combine(pr.first, 1, pr.second, a, fc.data(), fv.data());
+                const size_t ns = combine(pr.first, b, pr.second, oab, sc.data(), sv.data());
+                std::copy(fc.begin(), fc.begin() + nf, &tc[pr.first * W]);
+                std::copy(fv.begin(), fv.begin() + nf, &tv[pr.first * W]);
+                std::copy(sc.begin(), sc.begin() + ns, &tc[pr.second * W]);
+                std::copy(sv.begin(), sv.begin() + ns, &tv[pr.second * W]);
+                tn[pr.first] = static_cast<uint8_t>(nf);
+                tn[pr.second] = static_cast<uint8_t>(ns);
             }
+        });
+    }
+    // columns of T: for column i, the rows k with T[k][i] != 0
+    std::vector<uint32_t> cptr(n + 1, 0);
+    for (size_t k = 0; k < n; ++k)
+        for (size_t e = 0; e < tn[k]; ++e) ++cptr[tc[k * W + e] + 1];
+    for (size_t i = 0; i < n; ++i) cptr[i + 1] += cptr[i];
+    std::vector<uint32_t> crow(cptr[n]), cval(cptr[n]);
+    {
+        std::vector<uint32_t> fill(cptr.begin(), cptr.end() - 1);
+        for (size_t k = 0; k < n; ++k)
+            for (size_t e = 0; e < tn[k]; ++e) {
+                const uint32_t i = tc[k * W + e];
+                crow[fill[i]] = static_cast<uint32_t>(k);
+                cval[fill[i]++] = tv[k * W + e];
+            }
+    }
+    // P[i][j] = sum_k T[k][i] Dr[k] T[k][j]: row i merges the rows k of column i
+    const size_t PW = W * W;
+    std::vector<uint32_t> pc(n * PW), pv(n * PW);
+    std::vector<uint16_t> pn(n);
+    parallel_chunks(n, [&](size_t begin, size_t end) {
+        std::vector<std::pair<uint32_t, uint64_t>> acc;
+        for (size_t i = begin; i < end; ++i) {
+            acc.clear();
+            for (uint32_t e = cptr[i]; e < cptr[i + 1]; ++e) {
+                const size_t k = crow[e];
+                const uint64_t coef = static_cast<uint64_t>(cval[e]) * dr[k] % p;
+                for (size_t f = 0; f < tn[k]; ++f) acc.emplace_back(tc[k * W + f], coef * tv[k * W + f] % p);
+            }
+            std::sort(acc.begin(), acc.end(),
+                      [](const auto& x, const auto& y) { return x.first < y.first; });
+            size_t cnt = 0;
+            for (size_t a = 0; a < acc.size();) {
+                uint64_t sum = 0;
+                const uint32_t col = acc[a].first;
+                for (; a < acc.size() && acc[a].first == col; ++a) sum = (sum + acc[a].second) % p;
+                if (sum) {
+                    pc[i * PW + cnt] = col;
+                    pv[i * PW + cnt++] = static_cast<uint32_t>(sum);
+                }
+            }
+            pn[i] = static_cast<uint16_t>(cnt);
+        }
+    });
     Csr out;
     out.row_ptr.resize(n + 1);
+    size_t total = 0;
     for (size_t i = 0; i < n; ++i) {
-        out.row_ptr[i] = checked_u32(out.col.size(), "preconditioner nnz");
-        for (auto& e : rows[i])
-            if (e.second) {
-                out.col.push_back(e.first);
-                out.val.push_back(static_cast<uint32_t>(e.second));
-            }
+        out.row_ptr[i] = checked_u32(total, "preconditioner nnz");
+        total += pn[i];
     }
-    out.row_ptr[n] = checked_u32(out.col.size(), "preconditioner nnz");
+    out.row_ptr[n] = checked_u32(total, "preconditioner nnz");
+    out.col.resize(total);
+    out.val.resize(total);
+    parallel_chunks(n, [&](size_t begin, size_t end) {
+        for (size_t i = begin; i < end; ++i) {
+            std::copy(&pc[i * PW], &pc[i * PW] + pn[i], &out.col[out.row_ptr[i]]);
+            std::copy(&pv[i * PW], &pv[i * PW] + pn[i], &out.val[out.row_ptr[i]]);
+        }
+    });
     return out;
 }
 

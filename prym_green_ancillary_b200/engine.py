@@ -81,6 +81,7 @@ SIGNATURES = {
     "bw_cyclic_close": (None, [_VP]),
     "bw_cyclic_apply_host": (_INT, [_VP, _INT, _VP, _VP]),
     "bw_cyclic_generate": (_INT, [_VP, _U64]),
+    "bw_cyclic_generate_timed": (_INT, [_VP, _U64, ctypes.POINTER(ctypes.c_float)]),
     "bw_cyclic_download": (_INT, [_VP, _VP, _U64, _VP]),
     "bw_cyclic_output_path": (_INT, [_VP, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t]),
     "bw_cyclic_check_outputs_absent": (_INT, [ctypes.c_char_p]),
@@ -395,6 +396,13 @@ class CyclicEngine:
     def generate(self, nlen=0):
         _check(load().bw_cyclic_generate(self._h, nlen))
         return self.refresh()["seq_len"]
+
+    def generate_timed(self, nlen=0):
+        """generate() plus the device time of its rounds in ms (CUDA events on the engine's stream)."""
+        ms = ctypes.c_float()
+        _check(load().bw_cyclic_generate_timed(self._h, nlen, ctypes.byref(ms)))
+        self.refresh()
+        return float(ms.value)
 
     def download(self):
         n = self.info["seq_len"]
