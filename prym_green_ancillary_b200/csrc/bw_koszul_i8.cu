@@ -55,10 +55,10 @@ namespace bw {
 namespace {
 
 constexpr uint32_t kAbsent = 0xFFFFFFFFu;
-constexpr int kProducerWarps = 4;
-constexpr int kMmaWarp = 4;
-constexpr int kEpilogueWarp0 = 5;
-constexpr int kEpilogueWarps = 8;                 // two per TMEM lane quadrant
+constexpr int kProducerWarps = 8;
+constexpr int kMmaWarp = kProducerWarps;
+constexpr int kEpilogueWarp0 = kProducerWarps + 1;
+constexpr int kEpilogueWarps = 8;                 // per TMEM lane quadrant: kEpilogueWarps / 4
 constexpr int kI8Threads = (kProducerWarps + 1 + kEpilogueWarps) * 32;
 constexpr int kMaxSmem = 227 * 1024;
 constexpr int kMaxRowTable = 2048;    // bytes of the K'-row -> generator table
@@ -83,6 +83,21 @@ struct I8Dir {
     uint32_t b_bytes, slot_bytes, limb_bytes;
     Mod mod;
     int32_t c1, c2;              // 255 and 255^2 mod p, balanced
+};
+
+// Position in a ring of pipeline slots: slot index and the parity of its
+// current phase, advanced without dividing (a 64-bit division per stage would
+// sit on the producers' and the MMA thread's critical paths).
+struct SlotRing {
+    int slot = 0, n = 1;
+    uint32_t phase = 0;
+    __device__ explicit SlotRing(int count) : n(count) {}
+    __device__ void next() {
+        if (++slot == n) {
+            slot = 0;
+            phase ^= 1u;
+        }
+    }
 };
 
 // ll + 255 (lh + hl) + 255^2 hh mod p (balanced); c1 = 255, c2 = 255^2 mod p, balanced.
@@ -161,7 +176,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
     tc::fence_proxy_async_smem();
     if (threadIdx.x == 0) {
         for (int s = 0; s < P.slots; ++s) {
-            tc::mbar_init(&full[s], 2 * kProducerWarps * 32);   // per thread: copies landed + own stores
+            tc::mbar_init(&full[s], kProducerWarps * 32);   // per thread: its copies have landed
             tc::mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -195,17 +210,21 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         // or a zero store for an absent generator.  Each thread arrives on the
         // stage barrier twice: once through cp.async.mbarrier.arrive.noinc when
         // its copies have landed, once with release semantics for its stores.
-        constexpr int TPW = (BT + kProducerWarps - 1) / kProducerWarps;   // blocks per producer warp
+        // More producer warps than blocks: RPW warps share a block, interleaving its rows.
+        constexpr int RPW = kProducerWarps > BT ? kProducerWarps / BT : 1;
+        constexpr int GROUPS = kProducerWarps / RPW;                     // distinct block positions
+        constexpr int TPW = (BT + GROUPS - 1) / GROUPS;                  // blocks per producer warp
+        const int group = warp % GROUPS, sub = warp / GROUPS;
         auto load_inc = [&](long long tile, uint32_t (&dst)[TPW]) {
 #pragma unroll
             for (int k = 0; k < TPW; ++k) {
-                const int t = warp + k * kProducerWarps;
+                const int t = group + k * GROUPS;
                 const long long blk = tile * BT + t;
                 dst[k] = (tile < n_tiles && t < BT && blk < P.n_blk && lane < P.r) ? __ldg(P.inc + blk * P.r + lane)
                                                                                   : kAbsent;
             }
         };
-        long long it = 0;
+        SlotRing ring(P.slots);
         bool ok = true;
         uint32_t incr[TPW], incn[TPW];
         load_inc(blockIdx.x, incn);
@@ -213,9 +232,9 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
 #pragma unroll
             for (int k = 0; k < TPW; ++k) incr[k] = incn[k];
             load_inc(tile + gridDim.x, incn);
-            for (int s = 0; s < P.stages_per_tile; ++s, ++it) {
-                const int slot = static_cast<int>(it % P.slots);
-                const uint32_t ph = static_cast<uint32_t>((it / P.slots) & 1);
+            for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
+                const int slot = ring.slot;
+                const uint32_t ph = ring.phase;
                 int got = 1;
                 if (lane == 0) got = tc::mbar_wait(&empty[slot], ph ^ 1u, abort, P.err, tc::ERR_WAIT_EMPTY) ? 1 : 0;
                 got = __shfl_sync(0xffffffffu, got, 0);
@@ -228,39 +247,32 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                 uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
 #pragma unroll
                 for (int k = 0; k < TPW; ++k) {
-                    const int t = warp + k * kProducerWarps;
+                    const int t = group + k * GROUPS;
                     if (t >= BT) break;
-                    for (int w0 = 0; w0 < rows; w0 += 32) {
+                    for (int w0 = sub * 32; w0 < rows; w0 += RPW * 32) {
                         const int w = w0 + lane;
                         const int il = il_of_row[min(w, rows - 1)];
                         const uint32_t e = __shfl_sync(0xffffffffu, incr[k], s * P.gi + il);
                         if (w >= rows) continue;
                         const int b = w - il * P.inner;
                         uint8_t* dst0 = slotA + static_cast<size_t>(t * HG) * KS * 16 + static_cast<size_t>(w) * 16;
-                        if (e == kAbsent) {
-                            // absent generator: zero rows written here (a shared zero source in
-                            // global memory would send every SM's reads to one L2 slice)
+                        // one code path for every lane: an absent generator's rows are zero-filled by
+                        // the copy itself (source size 0: nothing is read), so the warp does not diverge
+                        const bool present = e != kAbsent;
+                        const long long nbr = present ? static_cast<long long>(e & 0x7FFFFFFFu) : 0;
+                        const int neg = (present && (e >> 31)) ? 2 : 0;
+                        const uint32_t nbytes = present ? 16u : 0u;
 #pragma unroll
-                            for (int limb = 0; limb < 2; ++limb)
+                        for (int limb = 0; limb < 2; ++limb)
 #pragma unroll
-                                for (int h = 0; h < HG; ++h)
-                                    *reinterpret_cast<int4*>(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
-                                                             static_cast<size_t>(h) * KS * 16) = make_int4(0, 0, 0, 0);
-                        } else {
-                            const long long nbr = static_cast<long long>(e & 0x7FFFFFFFu);
-                            const int neg = (e >> 31) ? 2 : 0;
-#pragma unroll
-                            for (int limb = 0; limb < 2; ++limb)
-#pragma unroll
-                                for (int h = 0; h < HG; ++h)
-                                    tc::cp_async16(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
-                                                       static_cast<size_t>(h) * KS * 16,
-                                                   P.in[limb + neg] + (nbr * HG + h) * block_bytes + b * 16);
-                        }
+                            for (int h = 0; h < HG; ++h)
+                                tc::cp_async16_zfill(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
+                                                         static_cast<size_t>(h) * KS * 16,
+                                                     P.in[limb + neg] + (nbr * HG + h) * block_bytes + b * 16,
+                                                     nbytes);
                     }
                 }
                 tc::cp_async_arrive_noinc(&full[slot]);   // when this thread's copies have landed
-                tc::mbar_arrive(&full[slot]);              // release: this thread's zero stores
             }
         }
         tc::cp_async_wait_all();   // no copy may still be landing when the CTA exits
@@ -269,7 +281,8 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_i8(128, N, true, false);
             const uint32_t sA0 = tc::smem_u32(sA), sB0 = tc::smem_u32(sB);
-            long long it = 0, tcount = 0;
+            long long tcount = 0;
+            SlotRing ring(P.slots);
             bool ok = true;
             for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
                 const int buf = static_cast<int>(tcount & 1);
@@ -277,9 +290,9 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                 if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, abort, P.err, tc::ERR_WAIT_ACCUM_FREE)) break;
                 tc::tc_fence_after();
                 const uint32_t dbase = tmem + static_cast<uint32_t>(buf * 2 * N);
-                for (int s = 0; s < P.stages_per_tile; ++s, ++it) {
-                    const int slot = static_cast<int>(it % P.slots);
-                    const uint32_t ph = static_cast<uint32_t>((it / P.slots) & 1);
+                for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
+                    const int slot = ring.slot;
+                    const uint32_t ph = ring.phase;
                     if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL)) {
                         ok = false;
                         break;
@@ -314,7 +327,8 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         // Warps 5..12: warp & 3 is the TMEM lane quadrant it may read; the two
         // warps of a quadrant split the 16-column output chunks between them.
         const int q = warp & 3;
-        const int half_id = (warp - kEpilogueWarp0) >> 2;      // 0 or 1
+        constexpr int EPQ = kEpilogueWarps / 4;                 // epilogue warps per quadrant
+        const int half_id = (warp - kEpilogueWarp0) >> 2;      // this warp's part of the chunks
         const int m = q * 32 + lane;               // tile row = (block t, column j)
         const int t = m / NB, j = m % NB;
         const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
@@ -344,7 +358,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
             int8_t* o_hi = P.out[PL_HI] + base;
             int8_t* o_nlo = P.out[PL_NLO] + base;
             int8_t* o_nhi = P.out[PL_NHI] + base;
-            for (int c = half_id; c < chunks; c += 2) {
+            for (int c = half_id; c < chunks; c += EPQ) {
                 const int o0 = c * 16;
                 if (c != half_id) load_diag(c);
                 int32_t ll[16], lh[16], hl[16], hh[16];
@@ -512,9 +526,10 @@ __global__ void __launch_bounds__(kProjThreads, 1) i8_project_tc_kernel(I8Proj P
 
     if (warp == 0) {
         // ------------------------------------------------------------ producer
-        for (long long i = 0; i < n_my; ++i) {
-            const int slot = static_cast<int>(i % P.slots);
-            const uint32_t ph = static_cast<uint32_t>((i / P.slots) & 1);
+        SlotRing ring(P.slots);
+        for (long long i = 0; i < n_my; ++i, ring.next()) {
+            const int slot = ring.slot;
+            const uint32_t ph = ring.phase;
             const long long st = blockIdx.x + i * gridDim.x;
             const long long blk0 = st * P.sb;
             const int nbh = static_cast<int>(min(static_cast<long long>(P.sb), P.n_blk - blk0));
@@ -551,6 +566,7 @@ __global__ void __launch_bounds__(kProjThreads, 1) i8_project_tc_kernel(I8Proj P
             const uint32_t gb = static_cast<uint32_t>(P.kp) * 16;
             const int ksteps = P.kp / 32;
             long long i = 0;
+            SlotRing ring(P.slots);
             bool ok = true;
             for (long long c = 0; c < n_chunks && ok; ++c) {
                 const int buf = static_cast<int>(c & 1);
@@ -559,9 +575,9 @@ __global__ void __launch_bounds__(kProjThreads, 1) i8_project_tc_kernel(I8Proj P
                 tc::tc_fence_after();
                 const uint32_t dcol = tmem + static_cast<uint32_t>(buf * N);
                 const long long i_end = min(n_my, (c + 1) * P.drain);
-                for (bool first = true; i < i_end; ++i, first = false) {
-                    const int slot = static_cast<int>(i % P.slots);
-                    const uint32_t ph = static_cast<uint32_t>((i / P.slots) & 1);
+                for (bool first = true; i < i_end; ++i, first = false, ring.next()) {
+                    const int slot = ring.slot;
+                    const uint32_t ph = ring.phase;
                     if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL)) {
                         ok = false;
                         break;

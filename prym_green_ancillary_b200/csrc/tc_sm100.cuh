@@ -89,6 +89,13 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 
+// 16-byte cp.async that reads src_size (0 or 16) bytes and zero-fills the rest:
+// src_size 0 writes 16 zero bytes without reading global memory.
+__device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, uint32_t src_size) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_size)
+                 : "memory");
+}
+
 // Arrive on `bar` once every cp.async issued so far by this thread has landed
 // (the arrival is one of the barrier's expected arrivals).
 __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
