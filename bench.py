@@ -245,11 +245,12 @@ def run_batch(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    from prym_green_ancillary_b200.sharding import max_over_ranks, rank_seed
     secs = config3_sectors()
     form = "int8" if args.form == "auto" else args.form
     specs, xs, ys = [], [], []
     for sec in secs:
-        seed = sec["seed"] + 100000 * rank
+        seed = rank_seed(sec["seed"], rank, stride=100000)
         maps = seeded_fill_host(sec["r"] * sec["co"] * sec["ci"], seed, TAG_MAPS, sec["p"])
         diag = torch.empty(sec["n_src"], dtype=torch.int32, device=dev)
         seeded_fill_device(diag, seed, TAG_DIAG, sec["p"], 1)
@@ -282,10 +283,7 @@ def run_batch(args):
     launches = batch.launch_count - launches0
     batch.seq_finish(stream=stream)
     torch.cuda.synchronize()
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    (ms,) = max_over_ranks([ms], device=dev)
 
     # End to end: X and Y0 of every sector from pinned host memory, sequences back, K batch steps.
     xh = [torch.empty(x.shape, dtype=torch.int32, pin_memory=True).copy_(x) for x in xs]
@@ -307,10 +305,7 @@ def run_batch(args):
             seqh[i].copy_(seqs[i][:K + 1], non_blocking=True)
     stream.synchronize()
     e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    (e2e_s,) = max_over_ranks([e2e_s], device=dev)
     h2d = sum(x.numel() * 4 + y.numel() * 4 for x, y in zip(xh, yh)) / K
     d2h = sum(s.numel() * 4 for s in seqh) / K
 
@@ -369,7 +364,8 @@ def run_paper(args):
     path = ROOT / "prym_green_ancillary_b200" / "_data" / f"{args.workload}.json"
     if not path.exists():
         raise SystemExit(f"{path} missing: build() stages the shipped instances from a reference checkout")
-    sector = args.sector + rank   # every rank its own sector (no collective)
+    from prym_green_ancillary_b200.sharding import max_over_ranks
+    sector = args.sector + rank   # every rank its own sector (no collective on the data path)
     t_open = time.perf_counter()
     eng = CyclicEngine(path, sector, device=local)
     t_open = time.perf_counter() - t_open
@@ -390,9 +386,8 @@ def run_paper(args):
         from datetime import timedelta
         dev = torch.device("cuda", local)
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
-        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_s = float(t[0].item()), float(t[1].item())
+        ms, e2e_s = max_over_ranks([ms, e2e_s], device=dev)
+        dist.destroy_process_group()
     rows, cols = info["rows"], info["cols"]
     step_bytes = 2 * (rows + cols) * 4 * 4
     peak, peak_kind = measured_peaks()
@@ -442,8 +437,9 @@ def run_engine(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
+    from prym_green_ancillary_b200.sharding import max_over_ranks, rank_seed
     sh = shape_of(args.workload)
-    seed = sh["seed"] + 1000 * rank       # every rank: its own sector
+    seed = rank_seed(sh["seed"], rank)    # every rank: its own sequence
     p, n, m = sh["p"], sh["n"], sh["m"]
     maps = seeded_fill_host(sh["r"] * sh["co"] * sh["ci"], seed, TAG_MAPS, p)
     diag = torch.empty(sh["n_src"], dtype=torch.int32, device=dev)
@@ -486,9 +482,7 @@ def run_engine(args):
     launches = eng.launch_count - launches0
     if world > 1:
         dist.barrier()
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    (ms,) = max_over_ranks([ms], device=dev)
     value = world * K / (ms / 1e3)
 
     # Per-kernel device times (CUDA events around each launch on the session stream).
@@ -508,10 +502,7 @@ def run_engine(args):
     t0 = time.perf_counter()
     seq_h, yf_h = eng.sequence_host(xh_np, yh_np, K + 1)
     e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    (e2e_s,) = max_over_ranks([e2e_s], device=dev)
     e2e_value = world * K / e2e_s
     h2d = (xh_np.nbytes + yh_np.nbytes) / K
     d2h = (seq_h.nbytes + yf_h.nbytes) / K
