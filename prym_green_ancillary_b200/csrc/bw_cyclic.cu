@@ -15,6 +15,7 @@
 //     packs the upper triangles (no atomics, deterministic);
 //   * one half-round pair captured as a CUDA graph and replayed.
 #include "bw_cyclic.cuh"
+#include "bw_cyclic_dev.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -26,58 +27,12 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ int32_t red64(long long x, const Mod& m) {
-    long long r = x % m.p;
-    if (r > m.half) r -= m.p;
-    if (r < -m.half) r += m.p;
-    return static_cast<int32_t>(r);
-}
-
-// Four-column accumulator.  SMALL: int32 sums, exact because the host checked
-// that (terms per output) * ((p-1)/2)^2 + 2p < 2^31 for every kernel of this
-// sector (always true at the paper primes); otherwise int64 sums.
-template <bool SMALL>
-struct Acc4;
-
-template <>
-struct Acc4<true> {
-    int32_t x = 0, y = 0, z = 0, w = 0;
-    __device__ __forceinline__ void mac(int32_t c, const int4& v) {
-        x += c * v.x;
-        y += c * v.y;
-        z += c * v.z;
-        w += c * v.w;
-    }
-    __device__ __forceinline__ int4 reduce(const Mod& m) const {
-        return make_int4(reduce_balanced(x, m), reduce_balanced(y, m), reduce_balanced(z, m), reduce_balanced(w, m));
-    }
-};
-
-template <>
-struct Acc4<false> {
-    long long x = 0, y = 0, z = 0, w = 0;
-    __device__ __forceinline__ void mac(int32_t c, const int4& v) {
-        x += static_cast<long long>(c) * v.x;
-        y += static_cast<long long>(c) * v.y;
-        z += static_cast<long long>(c) * v.z;
-        w += static_cast<long long>(c) * v.w;
-    }
-    __device__ __forceinline__ int4 reduce(const Mod& m) const {
-        return make_int4(red64(x, m), red64(y, m), red64(z, m), red64(w, m));
-    }
-};
-
-__device__ __forceinline__ int4 ld4(const int32_t* base, long long row) {
-    return __ldg(reinterpret_cast<const int4*>(base) + row);
-}
-__device__ __forceinline__ void st4(int32_t* base, long long row, const int4& v) {
-    reinterpret_cast<int4*>(base)[row] = v;
-}
-__device__ __forceinline__ int4 scale4(const int4& v, int32_t s, const Mod& m) {
-    return make_int4(reduce_balanced(v.x * s, m), reduce_balanced(v.y * s, m), reduce_balanced(v.z * s, m),
-                     reduce_balanced(v.w * s, m));
-}
-__device__ __forceinline__ int4 neg4(const int4& v) { return make_int4(-v.x, -v.y, -v.z, -v.w); }
+using cyc::Acc4;
+using cyc::ld4;
+using cyc::neg4;
+using cyc::red64;
+using cyc::scale4;
+using cyc::st4;
 
 __device__ __forceinline__ void decode_inc(uint32_t e, uint32_t& sub, int& i, bool& neg) {
     sub = e & 0x3FFFFFFu;
@@ -95,11 +50,7 @@ __device__ __forceinline__ void decode_coef(int32_t e, int& local, int32_t& coef
 
 // Operator column of base column q: q itself, or (replacement) q less the
 // dropped columns before it, -1 for a dropped column.
-__device__ __forceinline__ long long op_col(const ElimDev& E, long long q) {
-    if (E.drop0 < 0) return q;
-    if (q == E.drop0 || q == E.drop1) return -1;
-    return q - (q > E.drop0 ? 1 : 0) - (q > E.drop1 ? 1 : 0);
-}
+__device__ __forceinline__ long long op_col(const ElimDev& E, long long q) { return cyc::op_col(E.drop0, E.drop1, q); }
 
 // xs = the scaled source in base order: rows [0, base_cols) take operator
 // column op_col(q) times dc (zero for a dropped column), rows base_cols + j
@@ -691,31 +642,6 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
     E.dm_col_width = static_cast<uint32_t>(es.dm.column_width);
     E.d2_row_width = static_cast<uint32_t>(es.d2.row_width);
     E.d2_col_width = static_cast<uint32_t>(es.d2.column_width);
-    E.t_off = c->upload(es.dm_layout.row_offsets);
-    E.t_beta = c->upload(es.dm_layout.row_beta);
-    E.t_sub = c->upload(es.dm_layout.row_subset);
-    E.x_off = c->upload(es.dm_layout.col_offsets);
-    E.x_sub = c->upload(es.dm_layout.col_subset);
-    E.x_a = c->upload(es.dm_layout.col_a);
-    E.dm_row_inc = c->upload(pack_incidence(es.dm.row_col, es.dm.row_i, es.dm.row_neg));
-    E.dm_col_inc = c->upload(pack_incidence(es.dm.col_row, es.dm.col_i, es.dm.col_neg));
-    E.y_off = c->upload(es.d2_layout.col_offsets);
-    E.y_sub = c->upload(es.d2_layout.col_subset);
-    E.y_a = c->upload(es.d2_layout.col_a);
-    E.u_off = c->upload(es.d2_layout.row_offsets);
-    E.u_sub = c->upload(es.d2_layout.row_subset);
-    E.u_beta = c->upload(es.d2_layout.row_beta);
-    E.d2_row_inc = c->upload(pack_incidence(es.d2.row_col, es.d2.row_i, es.d2.row_neg));
-    E.d2_col_inc = c->upload(pack_incidence(es.d2.col_row, es.d2.col_i, es.d2.col_neg));
-    E.z_off = c->upload(es.z_layout.offsets);
-    E.z_sub = c->upload(es.z_layout.subset);
-    E.z_k = c->upload(es.z_layout.index);
-    E.fl_off = c->upload(fl_off);
-    E.fl = c->upload(fl);
-    E.tl_off = c->upload(tl_off);
-    E.tl = c->upload(tl);
-    E.R = c->upload(balanced(inst.right_inverse, c->mod));
-    E.Bk = c->upload(balanced(inst.kernel_basis, c->mod));
     E.base_cols = c->base_cols;
     E.kept_cols = c->kept_cols;
     E.drop0 = c->drop.size() > 0 ? static_cast<long long>(c->drop[0]) : -1;
@@ -723,6 +649,36 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
     E.n_extra = static_cast<int>(c->dense.columns);
     E.dense_sign = op == "augmented" ? -1 : 1;
     E.dense = deformation ? c->upload(balanced(c->dense.values, c->mod)) : nullptr;
+    // Subset-major gathers where the sector fits their format, else the
+    // generic row kernels and their tables.
+    c->setup_subset_path();
+    if (!c->subset_path) {
+        E.t_off = c->upload(es.dm_layout.row_offsets);
+        E.t_beta = c->upload(es.dm_layout.row_beta);
+        E.t_sub = c->upload(es.dm_layout.row_subset);
+        E.x_off = c->upload(es.dm_layout.col_offsets);
+        E.x_sub = c->upload(es.dm_layout.col_subset);
+        E.x_a = c->upload(es.dm_layout.col_a);
+        E.dm_row_inc = c->upload(pack_incidence(es.dm.row_col, es.dm.row_i, es.dm.row_neg));
+        E.dm_col_inc = c->upload(pack_incidence(es.dm.col_row, es.dm.col_i, es.dm.col_neg));
+        E.y_off = c->upload(es.d2_layout.col_offsets);
+        E.y_sub = c->upload(es.d2_layout.col_subset);
+        E.y_a = c->upload(es.d2_layout.col_a);
+        E.u_off = c->upload(es.d2_layout.row_offsets);
+        E.u_sub = c->upload(es.d2_layout.row_subset);
+        E.u_beta = c->upload(es.d2_layout.row_beta);
+        E.d2_row_inc = c->upload(pack_incidence(es.d2.row_col, es.d2.row_i, es.d2.row_neg));
+        E.d2_col_inc = c->upload(pack_incidence(es.d2.col_row, es.d2.col_i, es.d2.col_neg));
+        E.z_off = c->upload(es.z_layout.offsets);
+        E.z_sub = c->upload(es.z_layout.subset);
+        E.z_k = c->upload(es.z_layout.index);
+        E.fl_off = c->upload(fl_off);
+        E.fl = c->upload(fl);
+        E.tl_off = c->upload(tl_off);
+        E.tl = c->upload(tl);
+        E.R = c->upload(balanced(inst.right_inverse, c->mod));
+        E.Bk = c->upload(balanced(inst.kernel_basis, c->mod));
+    }
     c->d_dc = c->upload(balanced(c->col_precond, c->mod));
     c->d_p_ptr = c->upload(c->precond.row_ptr);
     c->d_p_col = c->upload(c->precond.col);
@@ -731,12 +687,14 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
     const size_t nc = ncols, v = num_v;
     c->d_b = c->alloc<int32_t>(nc * v);
     c->d_d = c->alloc<int32_t>(nc * v);
-    c->d_xs = c->alloc<int32_t>((c->base_cols + c->dense.columns) * v);
-    c->d_y = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
-    c->d_t = c->alloc<int32_t>(std::max<size_t>(es.t_rows, 1) * v);
-    c->d_h = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
+    // The gathered vectors (xs, y, t, u2) carry two padding rows: a subset-major
+    // gather reads two rows at every neighbour block, also past a one-row block.
+    c->d_xs = c->alloc<int32_t>((c->base_cols + c->dense.columns + 2) * v);
+    c->d_y = c->alloc<int32_t>((es.y_rows + 2) * v);
+    c->d_t = c->alloc<int32_t>((es.t_rows + 2) * v);
+    if (!c->subset_path) c->d_h = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
     c->d_u = c->alloc<int32_t>(std::max<size_t>(es.target_rows, 1) * v);
-    c->d_u2 = c->alloc<int32_t>(std::max<size_t>(es.target_rows, 1) * v);
+    c->d_u2 = c->alloc<int32_t>((es.target_rows + 2) * v);
     c->gram_grid = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>((nc + kThreads - 1) / kThreads,
                                                                                 static_cast<size_t>(c->sms) * 2)));
     c->d_partials = c->alloc<int32_t>(static_cast<size_t>(c->gram_grid) * 20);
@@ -774,6 +732,11 @@ void CyclicCtx::forward(const int32_t* in, int32_t* u, bool precondition) {
     cyc_source_kernel<<<grid_for(base_cols + dense.columns), kThreads, 0, stream>>>(E, in, precondition ? d_dc : nullptr,
                                                                                     d_xs);
     BW_CHECK_LAUNCH();
+    ++launches;
+    if (subset_path) {
+        subset_forward(u);
+        return;
+    }
     if (small) {
         cyc_dm_forward_kernel<true><<<grid_for(es.t_rows), kThreads, 0, stream>>>(E, d_xs, d_t);
         cyc_elim_y_kernel<true><<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, d_xs, d_t, d_y);
@@ -784,13 +747,15 @@ void CyclicCtx::forward(const int32_t* in, int32_t* u, bool precondition) {
         cyc_d2_forward_kernel<false><<<grid_for(es.target_rows), kThreads, 0, stream>>>(E, d_y, d_xs, u);
     }
     BW_CHECK_LAUNCH();
-    launches += 4;
+    launches += 3;
 }
 
 void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
     const int32_t* dc = precondition ? d_dc : nullptr;
     const size_t tz = es.t_rows + es.z_cols;
-    if (small) {
+    if (subset_path) {
+        subset_backward(u2, dc, out);
+    } else if (small) {
         cyc_d2_transpose_kernel<true><<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, u2, d_h);
         cyc_adjoint_t_z_kernel<true><<<grid_for(tz), kThreads, 0, stream>>>(E, d_h, dc, d_t, out);
         cyc_dm_transpose_kernel<true><<<grid_for(es.x_cols), kThreads, 0, stream>>>(E, d_t, dc, out);
@@ -800,7 +765,7 @@ void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
         cyc_dm_transpose_kernel<false><<<grid_for(es.x_cols), kThreads, 0, stream>>>(E, d_t, dc, out);
     }
     BW_CHECK_LAUNCH();
-    launches += 3;
+    if (!subset_path) launches += 3;
     if (E.n_extra) {
         cyc_dense_t_kernel<<<dense_grid, kThreads, 0, stream>>>(E, u2, dc, out, d_dpart, d_dcounter);
         BW_CHECK_LAUNCH();

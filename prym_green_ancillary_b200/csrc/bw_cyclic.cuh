@@ -5,6 +5,7 @@
 #include "cyclic_host.hpp"
 #include "../../include/bw_engine.h"
 
+#include <cstdlib>
 #include <memory>
 #include <string>
 #include <vector>
@@ -39,6 +40,31 @@ struct ElimDev {
     long long drop0, drop1;       // dropped base columns, -1 when none (drop0 < drop1)
     int n_extra, dense_sign;      // 0 / 0 for the eliminated operator
     const int32_t* dense;         // n_r x n_extra balanced, row-major
+};
+
+// Device view of the subset-major tables (bw_cyclic_subset.cu): one thread
+// per subset computes every row of that subset's block, so the rows share
+// their incidence words and neighbour-block loads.  The small tables (signed
+// coefficients, R, B, character maps) are staged in shared memory from one
+// blob per direction with the layout below (int32 words):
+//   coef  [2 signs][n][K][2]  (K = max(n, g); forward keys beta, transpose keys a)
+//   R [g][n], B [g][kdim], a0 offsets [r+1], a0 indices [g], a1 offsets [r+1],
+//   a1 indices [n], kernel-weight offsets [r+1], indices [kdim], ych [r]
+//   (ych[c] = y character of an (m-1)-subset whose t character is c).
+struct SubsetDev {
+    Mod mod;
+    int n, g, kdim, r, K;
+    uint32_t n1, n2, n0;                   // (m-1)-, (m-2)- and m-subsets
+    uint32_t w_dmf, w_d2f, w_d2t, w_dmt;   // incidences per subset of each gather
+    const uint32_t *m1_t, *m1_y, *m1_z, *m2_u, *m_x;
+    const uint32_t *inc_dmf, *inc_d2f, *inc_d2t, *inc_dmt;
+    const int32_t *blob_f, *blob_t;
+    int blob_words;
+    int o_R, o_B, o_a0off, o_a0idx, o_a1off, o_a1idx, o_koff, o_kidx, o_ych;
+    uint64_t x_cols, base_cols;
+    long long drop0, drop1;
+    int n_extra, dense_sign;
+    const int32_t* dense;
 };
 
 // Preconditioners, initial block and row-mixing recipe of an existing WDM file
@@ -84,6 +110,9 @@ struct CyclicCtx {
     int32_t *d_b = nullptr, *d_d = nullptr, *d_xs = nullptr, *d_y = nullptr, *d_h = nullptr, *d_u = nullptr,
             *d_u2 = nullptr, *d_t = nullptr;
     bool small = false;          // int32 accumulation is exact for this sector
+    bool subset_path = false;    // the subset-major gathers run (bw_cyclic_subset.cu)
+    std::string subset_reason;   // why not, when they do not
+    SubsetDev S{};
     uint64_t max_terms = 0;      // most products summed into one output by any kernel
     uint32_t* d_canon = nullptr;
     unsigned gram_grid = 1, dense_grid = 1;
@@ -115,6 +144,10 @@ struct CyclicCtx {
     void to_balanced(const uint32_t* in, int32_t* out, size_t count);
     void to_canonical(const int32_t* in, uint32_t* out, size_t count);
     void forward(const int32_t* in, int32_t* u, bool precondition);
+    // subset-major path (bw_cyclic_subset.cu)
+    void setup_subset_path();
+    void subset_forward(int32_t* u);
+    void subset_backward(const int32_t* u2, const int32_t* dc, int32_t* out);
     void target_precondition(const int32_t* u, int32_t* u2);
     void backward(const int32_t* u2, int32_t* out, bool precondition);
     void apply_square(const int32_t* in, int32_t* out);

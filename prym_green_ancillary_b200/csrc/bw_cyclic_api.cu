@@ -197,6 +197,18 @@ void bw::validate_ctx(CyclicCtx& c, uint32_t columns) {
 
 extern "C" uint64_t bw_cyclic_launch_count(const bw_cyclic* ctx) { return ctx ? ctx->impl->launches : 0; }
 
+extern "C" int bw_cyclic_gather_path(const bw_cyclic* ctx, char* buf, size_t cap) {
+    return guarded([&] {
+        BW_REQUIRE(ctx && buf && cap > 0, "bw_cyclic_gather_path: null argument");
+        const CyclicCtx& c = *ctx->impl;
+        const std::string path = c.host_only ? std::string("none: host-only context")
+                                 : c.subset_path ? std::string("subset")
+                                                 : "generic: " + c.subset_reason;
+        BW_REQUIRE(path.size() < cap, "bw_cyclic_gather_path: buffer too small");
+        std::memcpy(buf, path.c_str(), path.size() + 1);
+    });
+}
+
 extern "C" int bw_file_read_text(const char* path, char* buf, size_t cap, size_t* len) {
     return guarded([&] {
         BW_REQUIRE(path && len, "bw_file_read_text: null argument");

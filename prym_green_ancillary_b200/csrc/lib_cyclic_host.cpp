@@ -829,6 +829,57 @@ EliminatedSector assemble_eliminated_sector(const Instance& inst, size_t sector)
     return es;
 }
 
+// Subset-major gather tables (the device side is bw_cyclic_subset.cu).
+std::string build_subset_tables(const Instance& inst, const EliminatedSector& es, SubsetTables& out) {
+    out = SubsetTables{};
+    const CharMap a0 = build_char_map(inst.weight_a0, inst.r);
+    const CharMap a1 = build_char_map(inst.weight_a1, inst.r);
+    const CharMap km = build_char_map(inst.kernel_weights, inst.r);
+    if (a0.max_block() > 2 || a1.max_block() > 2 || km.max_block() > 2) return "a character block has more than two rows";
+    if (inst.n > 32) return "more than 32 generators";
+    if (inst.r > 64) return "cyclic order above 64";
+    const uint64_t limit = 1ull << 26;
+    if (es.total_cols() >= limit || es.t_rows >= limit || es.y_rows >= limit || es.target_rows >= limit)
+        return "a vector has 2^26 rows or more";
+    const Incidence& dm = es.dm;
+    const Incidence& d2 = es.d2;
+    const size_t n1 = dm.row_subsets, n2 = d2.row_subsets, n0 = dm.column_subsets;
+    if (d2.column_subsets != n1) return "inconsistent subset counts";
+    out.m1_t.resize(n1);
+    out.m1_y.resize(n1);
+    out.m1_z.resize(n1);
+    out.m2_u.resize(n2);
+    out.m_x.resize(n0);
+    for (size_t s = 0; s < n1; ++s) {
+        const uint32_t ch = sub_mod(es.sector, dm.row_subset_weights[s], inst.r);
+        out.m1_t[s] = es.dm_layout.row_offsets[s] | (ch << 26);
+        out.m1_y[s] = es.d2_layout.col_offsets[s];
+        out.m1_z[s] = es.z_layout.offsets[s];
+    }
+    for (size_t s = 0; s < n2; ++s)
+        out.m2_u[s] = es.d2_layout.row_offsets[s] | (sub_mod(es.y_sector, d2.row_subset_weights[s], inst.r) << 26);
+    for (size_t s = 0; s < n0; ++s)
+        out.m_x[s] = es.dm_layout.col_offsets[s] | (sub_mod(es.sector, dm.column_subset_weights[s], inst.r) << 26);
+    // incidence words, transposed to [position][subset]
+    auto fill = [](std::vector<uint32_t>& dst, size_t subsets, size_t width, const std::vector<uint32_t>& nb,
+                   const std::vector<uint32_t>& idx, const std::vector<uint8_t>& neg,
+                   const std::vector<uint32_t>& offsets) {
+        dst.resize(subsets * width);
+        parallel_chunks(subsets, [&](size_t b, size_t e) {
+            for (size_t s = b; s < e; ++s)
+                for (size_t pos = 0; pos < width; ++pos) {
+                    const size_t q = s * width + pos;
+                    dst[pos * subsets + s] = offsets[nb[q]] | (idx[q] << 26) | (neg[q] ? 0x80000000u : 0u);
+                }
+        });
+    };
+    fill(out.inc_dmf, n1, dm.row_width, dm.row_col, dm.row_i, dm.row_neg, es.dm_layout.col_offsets);
+    fill(out.inc_d2f, n2, d2.row_width, d2.row_col, d2.row_i, d2.row_neg, es.d2_layout.col_offsets);
+    fill(out.inc_d2t, n1, d2.column_width, d2.col_row, d2.col_i, d2.col_neg, es.d2_layout.row_offsets);
+    fill(out.inc_dmt, n0, dm.column_width, dm.col_row, dm.col_i, dm.col_neg, es.dm_layout.row_offsets);
+    return "";
+}
+
 // ----- deformation inputs (cuda/cuprym_deformation.cu:253-473): text scanning
 namespace {
 

@@ -89,6 +89,7 @@ SIGNATURES = {
     "bw_cyclic_write_wdm": (_INT, [_VP, ctypes.c_char_p]),
     "bw_cyclic_validate": (_INT, [_VP, _U32]),
     "bw_cyclic_launch_count": (_U64, [_VP]),
+    "bw_cyclic_gather_path": (_INT, [_VP, ctypes.c_char_p, ctypes.c_size_t]),
     "bw_file_read_text": (_INT, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "bw_project_noalloc": (_INT, [_VP, _VP, _U64, _U32, _U32, _U32, _VP, _INT, _VP]),
     "bw_cyclic_recover": (_INT, [ctypes.c_char_p, ctypes.c_char_p, _U32, ctypes.c_char_p, ctypes.c_char_p,
@@ -428,3 +429,10 @@ class CyclicEngine:
     @property
     def launch_count(self):
         return int(load().bw_cyclic_launch_count(self._h))
+
+    @property
+    def gather_path(self):
+        """"subset" or "generic: <reason>" (bw_cyclic_gather_path)."""
+        buf = ctypes.create_string_buffer(256)
+        _check(load().bw_cyclic_gather_path(self._h, buf, len(buf)))
+        return buf.value.decode()

@@ -33,12 +33,23 @@ REF_DATA = ROOT / "oracle" / "_ref" / "data"
 RECIPE = ["--operator", "eliminated", "-v", "4", "--seed", "1", "--rowmix-rounds", "2", "--rowmix-seed", "10001"]
 
 
+@pytest.fixture(params=["subset", "generic"])
+def gather_path(request, monkeypatch):
+    """Runs a test on the subset-major gathers (the default) and on the generic row kernels."""
+    if request.param == "generic":
+        monkeypatch.setenv("BW_CYCLIC_GENERIC", "1")
+    else:
+        monkeypatch.delenv("BW_CYCLIC_GENERIC", raising=False)
+    return request.param
+
+
 @pytest.mark.parametrize("p", [661, 109])
 @pytest.mark.parametrize("sector", range(6))
-def test_forward_and_transpose_match_explicit_blocks(p, sector):
+def test_forward_and_transpose_match_explicit_blocks(p, sector, gather_path):
     F = G[f"p{p}/sector{sector}/F"].astype(np.int64)
     rng = np.random.default_rng(sector + p)
     with CyclicEngine(GOLDEN / f"g12_p{p}.json", sector) as eng:
+        assert eng.gather_path.split(":")[0] == gather_path
         x = rng.integers(0, p, (F.shape[1], 4), dtype=np.uint32)
         y = rng.integers(0, p, (F.shape[0], 4), dtype=np.uint32)
         np.testing.assert_array_equal(eng.apply(APPLY_FORWARD, x), (F @ x.astype(np.int64)) % p)
@@ -46,7 +57,7 @@ def test_forward_and_transpose_match_explicit_blocks(p, sector):
 
 
 @pytest.mark.parametrize("sector", [0, 1])
-def test_square_is_symmetric_and_self_validation_passes(sector):
+def test_square_is_symmetric_and_self_validation_passes(sector, gather_path):
     p = 661
     rng = np.random.default_rng(7)
     with CyclicEngine(GOLDEN / f"g12_p{p}.json", sector) as eng:
@@ -129,6 +140,24 @@ def test_paper_outputs_identical_to_reference_binary(genus, sector, tmp_path):
     if not inst.exists():
         pytest.skip("paper inputs not staged (oracle/build_ref.sh)")
     _compare_with_reference(inst, sector, tmp_path)
+
+
+def test_paper_square_same_on_both_gather_paths(monkeypatch):
+    """g20 sector 3: S applied by the subset-major gathers equals S applied by the row kernels."""
+    inst = REF_DATA / "g20.json"
+    if not inst.exists():
+        pytest.skip("paper inputs not staged (oracle/build_ref.sh)")
+    out = {}
+    for path in ("subset", "generic"):
+        if path == "generic":
+            monkeypatch.setenv("BW_CYCLIC_GENERIC", "1")
+        else:
+            monkeypatch.delenv("BW_CYCLIC_GENERIC", raising=False)
+        with CyclicEngine(inst, 3) as eng:
+            assert eng.gather_path.split(":")[0] == path
+            x = np.random.default_rng(5).integers(0, eng.info["prime"], (eng.info["cols"], 4), dtype=np.uint32)
+            out[path] = eng.apply(APPLY_SQUARE, x)
+    np.testing.assert_array_equal(out["subset"], out["generic"])
 
 
 def test_cli_refuses_existing_outputs(tmp_path):

@@ -57,9 +57,14 @@ def _explicit(F0, dense, op, drop, p):
     return np.concatenate([F0[:, keep], dense], axis=1) % p
 
 
+@pytest.mark.parametrize("generic", [False, True], ids=["subset", "generic"])
 @pytest.mark.parametrize("op", ["augmented", "replacement"])
 @pytest.mark.parametrize("p, sector", [(661, 0), (661, 1), (661, 4), (109, 0), (109, 2)])
-def test_operator_matches_explicit_matrix(op, p, sector, tmp_path):
+def test_operator_matches_explicit_matrix(op, p, sector, generic, tmp_path, monkeypatch):
+    if generic:
+        monkeypatch.setenv("BW_CYCLIC_GENERIC", "1")
+    else:
+        monkeypatch.delenv("BW_CYCLIC_GENERIC", raising=False)
     inst = GOLDEN / f"g12_p{p}.json"
     _, rows, base, dense, dense_path, drop, drop_path = _inputs(tmp_path, inst, sector, op, 10 * sector + p)
     F0 = G[f"p{p}/sector{sector}/F"].astype(np.int64)
@@ -67,6 +72,7 @@ def test_operator_matches_explicit_matrix(op, p, sector, tmp_path):
     F = _explicit(F0, dense.astype(np.int64), op, drop, p)
     rng = np.random.default_rng(sector + 7)
     with CyclicEngine(inst, sector, op=op, dense_file=dense_path, drop_columns=drop_path) as eng:
+        assert eng.gather_path.startswith("generic" if generic else "subset")
         assert eng.info["cols"] == F.shape[1]
         X = rng.integers(0, p, (F.shape[1], 4)).astype(np.uint32)
         U = rng.integers(0, p, (rows, 4)).astype(np.uint32)
