@@ -332,26 +332,16 @@ __global__ void __launch_bounds__(kThreads) cyc_gram_kernel(
 #pragma unroll
         for (int e = 0; e < 20; ++e) red[warp][e] = reduce_balanced(acc[e], mod);
     __syncthreads();
+    int32_t mine = 0, total = 0;
     if (threadIdx.x < 20) {
-        int32_t s = 0;
-        for (int w = 0; w < kThreads / 32; ++w) s += red[w][threadIdx.x];
-        partials[static_cast<size_t>(blockIdx.x) * 20 + threadIdx.x] = reduce_balanced(s, mod);
+        for (int w = 0; w < kThreads / 32; ++w) mine += red[w][threadIdx.x];
+        mine = reduce_balanced(mine, mod);
     }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
-    __syncthreads();
-    if (!am_last) return;
-    __threadfence();
+    if (!cyc::grid_sum(partials, counter, 20, mine, total, &am_last)) return;
     const unsigned long long pos = *reinterpret_cast<volatile unsigned long long*>(seq_index);
     if (threadIdx.x < 10 * count) {
-        int32_t s = 0;
-        for (unsigned b = 0; b < gridDim.x; ++b) {
-            s += reinterpret_cast<volatile int32_t*>(partials)[static_cast<size_t>(b) * 20 + threadIdx.x];
-            if ((b & 7) == 7) s = reduce_partial(s, mod);
-        }
         const int which = threadIdx.x / 10, e = threadIdx.x % 10;
-        seq[(pos + which) * 10 + e] = to_canonical(reduce_balanced(s, mod), mod);
+        seq[(pos + which) * 10 + e] = to_canonical(reduce_balanced(total, mod), mod);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -363,9 +353,9 @@ __global__ void __launch_bounds__(kThreads) cyc_gram_kernel(
 
 // Extra source rows of the deformation transpose:
 //   out[kept_cols + j][c] = dense_sign * dc[kept_cols + j] * sum_row dense[row][j] u2[row][c]
-// (dc == nullptr: unscaled).  Each CTA sums a stripe of rows; the last CTA to
-// finish combines the per-CTA sums and writes the n_extra rows (deterministic,
-// no atomics on data; the counter resets itself for the next launch).
+// (dc == nullptr: unscaled).  Each CTA sums a stripe of rows; the CTA sums
+// meet in an 8-entry accumulator (cyc::grid_sum) and the last CTA writes the
+// n_extra rows (deterministic; accumulator and counter reset themselves).
 __global__ void __launch_bounds__(kThreads) cyc_dense_t_kernel(ElimDev E, const int32_t* __restrict__ u2,
                                                                const int32_t* __restrict__ dc,
                                                                int32_t* __restrict__ out, int32_t* __restrict__ partials,
@@ -400,26 +390,16 @@ __global__ void __launch_bounds__(kThreads) cyc_dense_t_kernel(ElimDev E, const 
         if (lane == 0) red[warp][e] = reduce_balanced(v, E.mod);
     }
     __syncthreads();
+    int32_t mine = 0, total = 0;
     if (threadIdx.x < 8) {
-        int32_t sum = 0;
-        for (int w = 0; w < kThreads / 32; ++w) sum += red[w][threadIdx.x];
-        partials[static_cast<size_t>(blockIdx.x) * 8 + threadIdx.x] = reduce_balanced(sum, E.mod);
+        for (int w = 0; w < kThreads / 32; ++w) mine += red[w][threadIdx.x];
+        mine = reduce_balanced(mine, E.mod);
     }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
-    __syncthreads();
-    if (!am_last) return;
-    __threadfence();
+    if (!cyc::grid_sum(partials, counter, 8, mine, total, &am_last)) return;
     if (threadIdx.x < 4 * E.n_extra) {
-        int32_t sum = 0;
-        for (unsigned b = 0; b < gridDim.x; ++b) {
-            sum += reinterpret_cast<volatile int32_t*>(partials)[static_cast<size_t>(b) * 8 + threadIdx.x];
-            if ((b & 7) == 7) sum = reduce_partial(sum, E.mod);
-        }
         const int j = threadIdx.x / 4, c = threadIdx.x % 4;
         const long long orow = static_cast<long long>(E.kept_cols) + j;
-        int32_t v = E.dense_sign * reduce_balanced(sum, E.mod);
+        int32_t v = E.dense_sign * reduce_balanced(total, E.mod);
         if (dc) v = reduce_balanced(v * __ldg(dc + orow), E.mod);
         out[orow * 4 + c] = v;
     }
@@ -476,6 +456,13 @@ T* CyclicCtx::alloc(size_t count) {
     device_bytes += bytes;
     return static_cast<T*>(p);
 }
+
+// used by the subset-major path (bw_cyclic_subset.cu)
+template uint4* CyclicCtx::alloc<uint4>(size_t);
+template int16_t* CyclicCtx::upload<int16_t>(const std::vector<int16_t>&);
+template uint32_t* CyclicCtx::upload<uint32_t>(const std::vector<uint32_t>&);
+template int32_t* CyclicCtx::upload<int32_t>(const std::vector<int32_t>&);
+template int32_t* CyclicCtx::alloc<int32_t>(size_t);
 
 unsigned CyclicCtx::grid_for(size_t rows) const {
     const size_t blocks = (rows + kThreads - 1) / kThreads;
@@ -680,29 +667,33 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
         E.Bk = c->upload(balanced(inst.kernel_basis, c->mod));
     }
     c->d_dc = c->upload(balanced(c->col_precond, c->mod));
-    c->d_p_ptr = c->upload(c->precond.row_ptr);
-    c->d_p_col = c->upload(c->precond.col);
-    c->d_p_val = c->upload(balanced(c->precond.val, c->mod));
+    if (!c->subset_path) {
+        c->d_p_ptr = c->upload(c->precond.row_ptr);
+        c->d_p_col = c->upload(c->precond.col);
+        c->d_p_val = c->upload(balanced(c->precond.val, c->mod));
+    }
 
     const size_t nc = ncols, v = num_v;
     c->d_b = c->alloc<int32_t>(nc * v);
     c->d_d = c->alloc<int32_t>(nc * v);
-    // The gathered vectors (xs, y, t, u2) carry two padding rows: a subset-major
-    // gather reads two rows at every neighbour block, also past a one-row block.
-    c->d_xs = c->alloc<int32_t>((c->base_cols + c->dense.columns + 2) * v);
-    c->d_y = c->alloc<int32_t>((es.y_rows + 2) * v);
-    c->d_t = c->alloc<int32_t>((es.t_rows + 2) * v);
-    if (!c->subset_path) c->d_h = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
+    if (!c->subset_path) {
+        c->d_xs = c->alloc<int32_t>((c->base_cols + c->dense.columns) * v);
+        c->d_y = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
+        c->d_t = c->alloc<int32_t>(std::max<size_t>(es.t_rows, 1) * v);
+        c->d_h = c->alloc<int32_t>(std::max<size_t>(es.y_rows, 1) * v);
+    }
     c->d_u = c->alloc<int32_t>(std::max<size_t>(es.target_rows, 1) * v);
-    c->d_u2 = c->alloc<int32_t>((es.target_rows + 2) * v);
+    c->d_u2 = c->alloc<int32_t>(std::max<size_t>(es.target_rows, 1) * v);
     c->gram_grid = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>((nc + kThreads - 1) / kThreads,
-                                                                                static_cast<size_t>(c->sms) * 2)));
-    c->d_partials = c->alloc<int32_t>(static_cast<size_t>(c->gram_grid) * 20);
+                                                                                static_cast<size_t>(c->sms) * 8)));
+    c->d_partials = c->alloc<int32_t>(20);   // grid-sum accumulators (zero between launches)
+    BW_CUDA(cudaMemsetAsync(c->d_partials, 0, 20 * sizeof(int32_t), c->stream));
     c->d_counter = c->alloc<unsigned int>(1);
     if (deformation) {
         c->dense_grid = static_cast<unsigned>(std::max<size_t>(
             1, std::min<size_t>((es.target_rows + kThreads - 1) / kThreads, static_cast<size_t>(c->sms) * 2)));
-        c->d_dpart = c->alloc<int32_t>(static_cast<size_t>(c->dense_grid) * 8);
+        c->d_dpart = c->alloc<int32_t>(8);
+        BW_CUDA(cudaMemsetAsync(c->d_dpart, 0, 8 * sizeof(int32_t), c->stream));
         c->d_dcounter = c->alloc<unsigned int>(1);
         BW_CUDA(cudaMemsetAsync(c->d_dcounter, 0, sizeof(unsigned int), c->stream));
     }
@@ -729,14 +720,14 @@ void CyclicCtx::to_canonical(const int32_t* in, uint32_t* out, size_t count) {
 }
 
 void CyclicCtx::forward(const int32_t* in, int32_t* u, bool precondition) {
+    if (subset_path) {
+        subset_forward16(in, precondition ? d_dc : nullptr);
+        subset_unpack_u(d_u16, u);
+        return;
+    }
     cyc_source_kernel<<<grid_for(base_cols + dense.columns), kThreads, 0, stream>>>(E, in, precondition ? d_dc : nullptr,
                                                                                     d_xs);
     BW_CHECK_LAUNCH();
-    ++launches;
-    if (subset_path) {
-        subset_forward(u);
-        return;
-    }
     if (small) {
         cyc_dm_forward_kernel<true><<<grid_for(es.t_rows), kThreads, 0, stream>>>(E, d_xs, d_t);
         cyc_elim_y_kernel<true><<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, d_xs, d_t, d_y);
@@ -747,15 +738,18 @@ void CyclicCtx::forward(const int32_t* in, int32_t* u, bool precondition) {
         cyc_d2_forward_kernel<false><<<grid_for(es.target_rows), kThreads, 0, stream>>>(E, d_y, d_xs, u);
     }
     BW_CHECK_LAUNCH();
-    launches += 3;
+    launches += 4;
 }
 
 void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
     const int32_t* dc = precondition ? d_dc : nullptr;
-    const size_t tz = es.t_rows + es.z_cols;
     if (subset_path) {
-        subset_backward(u2, dc, out);
-    } else if (small) {
+        subset_pack_u(u2, d_u2_16);
+        subset_backward16(dc, out);
+        return;
+    }
+    const size_t tz = es.t_rows + es.z_cols;
+    if (small) {
         cyc_d2_transpose_kernel<true><<<grid_for(es.y_rows), kThreads, 0, stream>>>(E, u2, d_h);
         cyc_adjoint_t_z_kernel<true><<<grid_for(tz), kThreads, 0, stream>>>(E, d_h, dc, d_t, out);
         cyc_dm_transpose_kernel<true><<<grid_for(es.x_cols), kThreads, 0, stream>>>(E, d_t, dc, out);
@@ -765,7 +759,7 @@ void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
         cyc_dm_transpose_kernel<false><<<grid_for(es.x_cols), kThreads, 0, stream>>>(E, d_t, dc, out);
     }
     BW_CHECK_LAUNCH();
-    if (!subset_path) launches += 3;
+    launches += 3;
     if (E.n_extra) {
         cyc_dense_t_kernel<<<dense_grid, kThreads, 0, stream>>>(E, u2, dc, out, d_dpart, d_dcounter);
         BW_CHECK_LAUNCH();
@@ -774,6 +768,12 @@ void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
 }
 
 void CyclicCtx::target_precondition(const int32_t* u, int32_t* u2) {
+    if (subset_path) {
+        subset_pack_u(u, d_u16);
+        subset_precondition16();
+        subset_unpack_u(d_u2_16, u2);
+        return;
+    }
     if (small)
         cyc_spmv_kernel<true><<<grid_for(es.target_rows), kThreads, 0, stream>>>(
             d_p_ptr, d_p_col, d_p_val, u, u2, static_cast<long long>(es.target_rows), mod);
@@ -785,6 +785,12 @@ void CyclicCtx::target_precondition(const int32_t* u, int32_t* u2) {
 }
 
 void CyclicCtx::apply_square(const int32_t* in, int32_t* out) {
+    if (subset_path) {   // padded int16 internals end to end
+        subset_forward16(in, d_dc);
+        subset_precondition16();
+        subset_backward16(d_dc, out);
+        return;
+    }
     forward(in, d_u, true);
     target_precondition(d_u, d_u2);
     backward(d_u2, out, true);

@@ -42,26 +42,28 @@ struct ElimDev {
     const int32_t* dense;         // n_r x n_extra balanced, row-major
 };
 
-// Device view of the subset-major tables (bw_cyclic_subset.cu): one thread
-// per subset computes every row of that subset's block, so the rows share
-// their incidence words and neighbour-block loads.  The small tables (signed
-// coefficients, R, B, character maps) are staged in shared memory from one
-// blob per direction with the layout below (int32 words):
-//   coef  [2 signs][n][K][2]  (K = max(n, g); forward keys beta, transpose keys a)
+// Device view of the subset-major operator (bw_cyclic_subset.cu): one thread
+// per subset computes every row of that subset's block; internal vectors are
+// int16 with two row slots per subset.  The small tables (signed coefficients,
+// R, B, character maps) are staged in shared memory from one blob per
+// direction with the layout below (int32 words):
+//   coef [2 signs][n][r] x int2  (four packed int16: own rows x neighbour slots)
 //   R [g][n], B [g][kdim], a0 offsets [r+1], a0 indices [g], a1 offsets [r+1],
 //   a1 indices [n], kernel-weight offsets [r+1], indices [kdim], ych [r]
 //   (ych[c] = y character of an (m-1)-subset whose t character is c).
 struct SubsetDev {
     Mod mod;
-    int n, g, kdim, r, K;
+    int n, g, kdim, r;
     uint32_t n1, n2, n0;                   // (m-1)-, (m-2)- and m-subsets
     uint32_t w_dmf, w_d2f, w_d2t, w_dmt;   // incidences per subset of each gather
-    const uint32_t *m1_t, *m1_y, *m1_z, *m2_u, *m_x;
+    const uint32_t *m1, *m2, *m0;          // subset words: compact block row | character << 26
     const uint32_t *inc_dmf, *inc_d2f, *inc_d2t, *inc_dmt;
+    const uint32_t *p_ptr, *p_col;         // folded target preconditioner over padded u rows
+    const int16_t* p_val;
     const int32_t *blob_f, *blob_t;
     int blob_words;
     int o_R, o_B, o_a0off, o_a0idx, o_a1off, o_a1idx, o_koff, o_kidx, o_ych;
-    uint64_t x_cols, base_cols;
+    uint64_t x_cols, z_cols, kept_cols;
     long long drop0, drop1;
     int n_extra, dense_sign;
     const int32_t* dense;
@@ -112,7 +114,10 @@ struct CyclicCtx {
     bool small = false;          // int32 accumulation is exact for this sector
     bool subset_path = false;    // the subset-major gathers run (bw_cyclic_subset.cu)
     std::string subset_reason;   // why not, when they do not
+    bool stream_tables = false;  // its tables exceed half the L2: read them evict-first
     SubsetDev S{};
+    uint4 *d_xs16 = nullptr, *d_y16 = nullptr, *d_t16 = nullptr, *d_u16 = nullptr, *d_u2_16 = nullptr;
+    int32_t* d_zs = nullptr;     // compact z rows and extra columns of the scaled source
     uint64_t max_terms = 0;      // most products summed into one output by any kernel
     uint32_t* d_canon = nullptr;
     unsigned gram_grid = 1, dense_grid = 1;
@@ -144,10 +149,13 @@ struct CyclicCtx {
     void to_balanced(const uint32_t* in, int32_t* out, size_t count);
     void to_canonical(const int32_t* in, uint32_t* out, size_t count);
     void forward(const int32_t* in, int32_t* u, bool precondition);
-    // subset-major path (bw_cyclic_subset.cu)
+    // subset-major path (bw_cyclic_subset.cu): in -> d_u16, d_u16 -> d_u2_16, d_u2_16 -> out
     void setup_subset_path();
-    void subset_forward(int32_t* u);
-    void subset_backward(const int32_t* u2, const int32_t* dc, int32_t* out);
+    void subset_forward16(const int32_t* in, const int32_t* dc);
+    void subset_precondition16();
+    void subset_backward16(const int32_t* dc, int32_t* out);
+    void subset_pack_u(const int32_t* u32, uint4* u16);
+    void subset_unpack_u(const uint4* u16, int32_t* u32);
     void target_precondition(const int32_t* u, int32_t* u2);
     void backward(const int32_t* u2, int32_t* out, bool precondition);
     void apply_square(const int32_t* in, int32_t* out);

@@ -68,5 +68,25 @@ __device__ __forceinline__ long long op_col(long long drop0, long long drop1, lo
     return q - (q > drop0 ? 1 : 0) - (q > drop1 ? 1 : 0);
 }
 
+// Grid-wide sum of W balanced residues per CTA, without a partials array:
+// threads 0..W-1 of every CTA add their CTA's value into acc[0..W) (int32 at
+// L2; |total| <= gridDim.x * p/2 stays far below 2^31 for p < 2^15), and the
+// CTA that finishes last gets the totals back, each thread t < W taking
+// acc[t] and leaving 0 for the next launch.  Integer sums do not depend on
+// the order of the additions, so the result is deterministic.  Every thread
+// of the CTA calls it; returns true only in the last CTA.
+__device__ __forceinline__ bool grid_sum(int32_t* acc, unsigned int* counter, int W, int32_t mine, int32_t& total,
+                                         bool* am_last /* shared */) {
+    if (static_cast<int>(threadIdx.x) < W) atomicAdd(acc + threadIdx.x, mine);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) *am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!*am_last) return false;
+    __threadfence();
+    if (static_cast<int>(threadIdx.x) < W) total = atomicExch(acc + threadIdx.x, 0);
+    return true;
+}
+
 }  // namespace cyc
 }  // namespace bw

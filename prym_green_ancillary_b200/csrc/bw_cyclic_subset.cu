@@ -1,27 +1,34 @@
-// Subset-major paper-mode gathers: the four Koszul maps of the eliminated
-// operator with one thread per subset.
+// Subset-major paper-mode operator: the four Koszul gathers of the eliminated
+// operator with one thread per subset, on 16-bit vectors in padded blocks.
 //
 // Every character block of the shipped instances has at most two rows (A0
 // blocks two, A1 blocks one or two, kernel-weight blocks at most one), and
-// the rows of one subset's block read the same neighbour blocks with different
-// coefficients.  So one thread takes a subset, loads each incidence word and
-// each neighbour block once, and accumulates both rows.  The incidence word
-// holds the neighbour block's first row directly (no offset lookup), and the
-// signed coefficients of mu sit in a dense [sign][i][key][2] table in shared
-// memory, so an incidence costs one coalesced word, two 16-byte loads and
-// sixteen multiply-adds.
+// the rows of one subset's block read the same neighbour blocks with
+// different coefficients.  So:
+//   * the internal vectors (scaled source x, y, u, u2, t_adj) hold balanced
+//     residues as int16 and give every subset's block two row slots: a block
+//     is one aligned 16-byte load, found from the subset's rank alone;
+//   * one thread takes a subset, loads each incidence word (neighbour rank,
+//     generator, sign) and each neighbour block once, and accumulates both
+//     rows of its own block;
+//   * the signed coefficients of mu for (sign, generator, own character) are
+//     four packed int16 in shared memory: one 8-byte load per incidence.
+// An incidence thus costs one coalesced word, one 16-byte load, one 8-byte
+// shared load and sixteen multiply-adds.
 //
-// Two of the reference's kernel pairs are fused, with their intermediates
-// kept in registers:
+// Two of the reference's kernel pairs are fused, with their intermediates in
+// registers:
 //   * D_m forward (cuda/cyclic_cuda_helpers.h:145-204) with the elimination
 //     y = B z - R t (cyclic_elim_z_to_y_kernel, cyclic_elim_subtract_Rt_kernel,
 //     :718-791): t never reaches memory;
-//   * D_(m-1) transpose (:206-266) with t_adj = R^t h and z_adj = B^t h and the
+//   * D_(m-1) transpose (:206-266) with t_adj = R^t h, z_adj = B^t h and the
 //     z part of the adjoint assembly (cyclic_elim_RT_h_kernel,
 //     cyclic_elim_BT_h_kernel, cyclic_elim_assemble_adjoint_kernel, :793-895):
 //     h never reaches memory.
-// Results are the same canonical residues as the generic row kernels in
-// bw_cyclic.cu, which remain for instances outside this format.
+// The folded target preconditioner runs over the padded u rows with int16
+// values.  The operator's inputs and outputs (the block B, S B) stay compact
+// int32; results are the same canonical residues as the generic row kernels
+// of bw_cyclic.cu, which remain for instances outside this format.
 #include "bw_cyclic.cuh"
 #include "bw_cyclic_dev.cuh"
 
@@ -32,13 +39,26 @@ namespace bw {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr uint32_t kOffsetMask = (1u << 26) - 1;
+constexpr uint32_t kLow26 = (1u << 26) - 1;
 
 using cyc::Acc4;
 using cyc::ld4;
 using cyc::neg4;
 using cyc::scale4;
 using cyc::st4;
+
+// ----- 16-bit rows: 4 columns in 8 bytes, a block of two rows in 16
+__device__ __forceinline__ uint32_t pack2(int32_t a, int32_t b) {
+    return (static_cast<uint32_t>(a) & 0xFFFFu) | (static_cast<uint32_t>(b) << 16);
+}
+__device__ __forceinline__ int32_t lo16(uint32_t w) { return static_cast<int16_t>(w & 0xFFFFu); }
+__device__ __forceinline__ int32_t hi16(uint32_t w) { return static_cast<int32_t>(w) >> 16; }
+__device__ __forceinline__ uint2 pack_row(const int4& v) { return make_uint2(pack2(v.x, v.y), pack2(v.z, v.w)); }
+__device__ __forceinline__ int4 unpack_row(uint32_t a, uint32_t b) { return make_int4(lo16(a), hi16(a), lo16(b), hi16(b)); }
+__device__ __forceinline__ void st_block(uint4* v, uint32_t s, const int4& r0, const int4& r1) {
+    const uint2 a = pack_row(r0), b = pack_row(r1);
+    v[s] = make_uint4(a.x, a.y, b.x, b.y);
+}
 
 // Views of the staged shared-memory tables.
 struct Tables {
@@ -63,172 +83,240 @@ __device__ __forceinline__ Tables stage(const SubsetDev& D, const int32_t* __res
     return t;
 }
 
-// Both rows (keys k0, k1) of subset s against its `width` neighbour blocks:
-//   acc_r += sum_pos sum_{l < 2} coef[sign, i, k_r][l] * in[first row + l].
-// A neighbour block with fewer than two rows has zero coefficients beyond its
-// end; the row read there is a real row or one of the two padding rows every
-// gathered vector carries.
+// Streamed table words: evict-first when the sector's tables exceed the L2
+// (they would only push the gathered vector out), cached otherwise (small
+// sectors keep tables and vectors in L2 from one application to the next).
+template <bool STREAM, class T>
+__device__ __forceinline__ T ld_table(const T* p) {
+    if constexpr (STREAM)
+        return __ldcs(p);
+    else
+        return __ldg(p);
+}
+
+// acc_r += c_r0 * row0 + c_r1 * row1, the four coefficients packed in c
+// (.x: own row 0 against neighbour rows 0 and 1; .y: own row 1).
 template <bool SMALL>
-__device__ __forceinline__ void gather2(const uint32_t* __restrict__ inc, uint32_t nsub, uint32_t s, uint32_t width,
-                                        const int2* coef, int n, int K, int k0, int k1,
-                                        const int32_t* __restrict__ in, Acc4<SMALL>& acc0, Acc4<SMALL>& acc1) {
-    // Four incidences at a time: their words, then their eight rows, then the
-    // products, so that eight independent 16-byte loads are in flight.
+__device__ __forceinline__ void mac_block(const int2& c, const uint4& b, Acc4<SMALL>& acc0, Acc4<SMALL>& acc1) {
+    const int4 r0 = unpack_row(b.x, b.y), r1 = unpack_row(b.z, b.w);
+    const uint32_t c0 = static_cast<uint32_t>(c.x), c1 = static_cast<uint32_t>(c.y);
+    acc0.mac(lo16(c0), r0);
+    acc0.mac(hi16(c0), r1);
+    acc1.mac(lo16(c1), r0);
+    acc1.mac(hi16(c1), r1);
+}
+
+// Both rows of subset s against its `width` neighbour blocks.  The coefficient
+// table is [sign][generator][own character]; a neighbour block with one row
+// has zero coefficients for its second slot (which holds zeros).  Incidence
+// words are read once per application (ld_table).
+template <bool SMALL, bool STREAM>
+__device__ __forceinline__ void gather_block(const uint32_t* __restrict__ inc, uint32_t nsub, uint32_t s,
+                                             uint32_t width, const int2* coef, int n, int r, int ch,
+                                             const uint4* __restrict__ in, Acc4<SMALL>& acc0, Acc4<SMALL>& acc1) {
+    // Four incidences at a time: their words, then their blocks, then the
+    // products, so that four independent 16-byte loads are in flight.
     constexpr int U = 4;
     uint32_t pos = 0;
     for (; pos + U <= width; pos += U) {
         uint32_t e[U];
-        int4 v0[U], v1[U];
+        uint4 b[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) e[u] = __ldg(inc + static_cast<size_t>(pos + u) * nsub + s);
+        for (int u = 0; u < U; ++u) e[u] = ld_table<STREAM>(inc + static_cast<size_t>(pos + u) * nsub + s);
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const long long first = e[u] & kOffsetMask;
-            v0[u] = ld4(in, first);
-            v1[u] = ld4(in, first + 1);
-        }
+        for (int u = 0; u < U; ++u) b[u] = __ldg(in + (e[u] & kLow26));
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int ci = (static_cast<int>(e[u] >> 31) * n + static_cast<int>((e[u] >> 26) & 31u)) * K;
-            const int2 c0 = coef[ci + k0], c1 = coef[ci + k1];
-            acc0.mac(c0.x, v0[u]);
-            acc0.mac(c0.y, v1[u]);
-            acc1.mac(c1.x, v0[u]);
-            acc1.mac(c1.y, v1[u]);
-        }
+        for (int u = 0; u < U; ++u)
+            mac_block<SMALL>(coef[(static_cast<int>(e[u] >> 31) * n + static_cast<int>((e[u] >> 26) & 31u)) * r + ch],
+                             b[u], acc0, acc1);
     }
     for (; pos < width; ++pos) {
-        const uint32_t e = __ldg(inc + static_cast<size_t>(pos) * nsub + s);
-        const long long first = e & kOffsetMask;
-        const int4 v0 = ld4(in, first), v1 = ld4(in, first + 1);
-        const int ci = (static_cast<int>(e >> 31) * n + static_cast<int>((e >> 26) & 31u)) * K;
-        const int2 c0 = coef[ci + k0], c1 = coef[ci + k1];
-        acc0.mac(c0.x, v0);
-        acc0.mac(c0.y, v1);
-        acc1.mac(c1.x, v0);
-        acc1.mac(c1.y, v1);
+        const uint32_t e = ld_table<STREAM>(inc + static_cast<size_t>(pos) * nsub + s);
+        const uint4 b = __ldg(in + (e & kLow26));
+        mac_block<SMALL>(coef[(static_cast<int>(e >> 31) * n + static_cast<int>((e >> 26) & 31u)) * r + ch], b, acc0,
+                         acc1);
     }
 }
 
-#define BW_SUBSETS(var, count)                                                                    \
-    for (uint32_t var = blockIdx.x * blockDim.x + threadIdx.x; var < (count); var += gridDim.x * blockDim.x)
+#define BW_ITEMS(var, count)                                                                         \
+    for (long long var = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; var < (count); \
+         var += static_cast<long long>(gridDim.x) * blockDim.x)
 
-// (m-1)-subset S: its t rows t(S, beta) = (D_m xs)(S, beta), then its y rows
-//   y(S, a) = sum_kappa B[a,kappa] zs(S, kappa) - sum_beta R[a,beta] t(S, beta).
-template <bool SMALL>
-__global__ void __launch_bounds__(kThreads) sub_dm_forward_elim_kernel(SubsetDev D, const int32_t* __restrict__ xs,
-                                                                       int32_t* __restrict__ y) {
+// Scaled source: items [0, n0) are m-subsets, whose x block (compact rows
+// x_off, x_off + 1 of the operator column op_col, times dc) goes to the padded
+// xs; items n0 + j are the compact z rows and the extra dense columns (int32).
+__global__ void __launch_bounds__(kThreads) sub_source_kernel(SubsetDev D, const int32_t* __restrict__ in,
+                                                              const int32_t* __restrict__ dc, uint4* __restrict__ xs,
+                                                              int32_t* __restrict__ zs) {
     extern __shared__ int32_t sm[];
     const Tables T = stage(D, D.blob_f, sm);
-    BW_SUBSETS(s, D.n1) {
-        const uint32_t dt = __ldg(D.m1_t + s);
-        const int tch = static_cast<int>(dt >> 26);
-        const int ych = T.ych[tch];
-        const int ya = T.a0off[ych], ny = T.a0off[ych + 1] - ya;
-        if (ny == 0) continue;
-        const int tb = T.a1off[tch], nt = T.a1off[tch + 1] - tb;
-        int4 t0 = make_int4(0, 0, 0, 0), t1 = t0;
-        int beta0 = 0, beta1 = 0;
-        if (nt > 0) {
-            beta0 = T.a1idx[tb];
-            beta1 = nt > 1 ? T.a1idx[tb + 1] : beta0;
-            Acc4<SMALL> acc0, acc1;
-            gather2<SMALL>(D.inc_dmf, D.n1, s, D.w_dmf, T.coef, D.n, D.K, beta0, beta1, xs, acc0, acc1);
-            t0 = acc0.reduce(D.mod);
-            t1 = acc1.reduce(D.mod);
-        }
-        const int kb = T.koff[ych], nz = T.koff[ych + 1] - kb;
-        int4 z0 = make_int4(0, 0, 0, 0), z1 = z0;
-        if (nz > 0) {
-            const long long zr = static_cast<long long>(D.x_cols) + __ldg(D.m1_z + s);
-            z0 = ld4(xs, zr);
-            if (nz > 1) z1 = ld4(xs, zr + 1);
-        }
-        const long long yrow = __ldg(D.m1_y + s);
-        for (int q = 0; q < ny; ++q) {
-            const int a = T.a0idx[ya + q];
-            Acc4<SMALL> acc;
-            if (nz > 0) acc.mac(T.B[a * D.kdim + T.kidx[kb]], z0);
-            if (nz > 1) acc.mac(T.B[a * D.kdim + T.kidx[kb + 1]], z1);
-            if (nt > 0) acc.mac(-T.R[a * D.n + beta0], t0);
-            if (nt > 1) acc.mac(-T.R[a * D.n + beta1], t1);
-            st4(y, yrow + q, acc.reduce(D.mod));
-        }
-    }
-}
-
-// (m-2)-subset S2: its u rows u(S2, beta) = (D_(m-1) y)(S2, beta), plus
-// dense_sign * dense xs_extra for the deformation variants.
-template <bool SMALL>
-__global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, const int32_t* __restrict__ y,
-                                                                  const int32_t* __restrict__ xs,
-                                                                  int32_t* __restrict__ u) {
-    extern __shared__ int32_t sm[];
-    const Tables T = stage(D, D.blob_f, sm);
-    BW_SUBSETS(s, D.n2) {
-        const uint32_t du = __ldg(D.m2_u + s);
-        const int uch = static_cast<int>(du >> 26);
-        const int ub = T.a1off[uch], nu = T.a1off[uch + 1] - ub;
-        if (nu == 0) continue;
-        const int beta0 = T.a1idx[ub], beta1 = nu > 1 ? T.a1idx[ub + 1] : beta0;
-        Acc4<SMALL> acc0, acc1;
-        gather2<SMALL>(D.inc_d2f, D.n2, s, D.w_d2f, T.coef, D.n, D.K, beta0, beta1, y, acc0, acc1);
-        const long long urow = du & kOffsetMask;
-        for (int q = 0; q < nu; ++q) {
-            int4 v = q == 0 ? acc0.reduce(D.mod) : acc1.reduce(D.mod);
-            if (D.n_extra) {
-                for (int j = 0; j < D.n_extra; ++j) {
-                    const int32_t c = D.dense_sign * __ldg(D.dense + (urow + q) * D.n_extra + j);
-                    const int4 e = ld4(xs, static_cast<long long>(D.base_cols) + j);
-                    v.x += c * e.x;
-                    v.y += c * e.y;
-                    v.z += c * e.z;
-                    v.w += c * e.w;
-                }
-                v = make_int4(reduce_balanced(v.x, D.mod), reduce_balanced(v.y, D.mod), reduce_balanced(v.z, D.mod),
-                              reduce_balanced(v.w, D.mod));
+    const long long n0 = D.n0, total = n0 + static_cast<long long>(D.z_cols) + D.n_extra;
+    BW_ITEMS(item, total) {
+        if (item < n0) {
+            const uint32_t dx = __ldg(D.m0 + item);
+            const int xch = static_cast<int>(dx >> 26);
+            const int nx = T.a0off[xch + 1] - T.a0off[xch];
+            int4 r[2] = {make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0)};
+            for (int q = 0; q < nx; ++q) {
+                const long long c = cyc::op_col(D.drop0, D.drop1, static_cast<long long>(dx & kLow26) + q);
+                if (c < 0) continue;   // dropped base column (replacement): zero
+                const int4 v = ld4(in, c);
+                r[q] = dc ? scale4(v, __ldg(dc + c), D.mod) : v;
             }
-            st4(u, urow + q, v);
+            st_block(xs, static_cast<uint32_t>(item), r[0], r[1]);
+        } else {
+            const long long zq = item - n0;
+            const long long src = zq < static_cast<long long>(D.z_cols)
+                                      ? cyc::op_col(D.drop0, D.drop1, static_cast<long long>(D.x_cols) + zq)
+                                      : static_cast<long long>(D.kept_cols) + (zq - static_cast<long long>(D.z_cols));
+            int4 v = make_int4(0, 0, 0, 0);
+            if (src >= 0) {
+                v = ld4(in, src);
+                if (dc) v = scale4(v, __ldg(dc + src), D.mod);
+            }
+            st4(zs, zq, v);
         }
+    }
+}
+
+// (m-1)-subset S: its t rows t(S, beta) = (D_m xs)(S, beta), then its y block
+//   y(S, a) = sum_kappa B[a,kappa] zs(S, kappa) - sum_beta R[a,beta] t(S, beta).
+template <bool SMALL, bool STREAM>
+__global__ void __launch_bounds__(kThreads) sub_dm_forward_elim_kernel(SubsetDev D, const uint4* __restrict__ xs,
+                                                                       const int32_t* __restrict__ zs,
+                                                                       uint4* __restrict__ y) {
+    extern __shared__ int32_t sm[];
+    const Tables T = stage(D, D.blob_f, sm);
+    BW_ITEMS(item, D.n1) {
+        const uint32_t s = static_cast<uint32_t>(item);
+        const uint32_t d = __ldg(D.m1 + s);
+        const int tch = static_cast<int>(d >> 26), ych = T.ych[tch];
+        const int ya = T.a0off[ych], ny = T.a0off[ych + 1] - ya;
+        int4 out[2] = {make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0)};
+        if (ny > 0) {
+            const int tb = T.a1off[tch], nt = T.a1off[tch + 1] - tb;
+            int4 t0 = make_int4(0, 0, 0, 0), t1 = t0;
+            if (nt > 0) {
+                Acc4<SMALL> acc0, acc1;
+                gather_block<SMALL, STREAM>(D.inc_dmf, D.n1, s, D.w_dmf, T.coef, D.n, D.r, tch, xs, acc0, acc1);
+                t0 = acc0.reduce(D.mod);
+                t1 = acc1.reduce(D.mod);
+            }
+            const int beta0 = nt > 0 ? T.a1idx[tb] : 0, beta1 = nt > 1 ? T.a1idx[tb + 1] : beta0;
+            const int kb = T.koff[ych], nz = T.koff[ych + 1] - kb;
+            int4 z0 = make_int4(0, 0, 0, 0), z1 = z0;
+            if (nz > 0) {
+                const long long zr = d & kLow26;
+                z0 = ld4(zs, zr);
+                if (nz > 1) z1 = ld4(zs, zr + 1);
+            }
+            for (int q = 0; q < ny; ++q) {
+                const int a = T.a0idx[ya + q];
+                Acc4<SMALL> acc;
+                if (nz > 0) acc.mac(T.B[a * D.kdim + T.kidx[kb]], z0);
+                if (nz > 1) acc.mac(T.B[a * D.kdim + T.kidx[kb + 1]], z1);
+                if (nt > 0) acc.mac(-T.R[a * D.n + beta0], t0);
+                if (nt > 1) acc.mac(-T.R[a * D.n + beta1], t1);
+                out[q] = acc.reduce(D.mod);
+            }
+        }
+        st_block(y, s, out[0], out[1]);
+    }
+}
+
+// (m-2)-subset S2: its u block u(S2, beta) = (D_(m-1) y)(S2, beta), plus
+// dense_sign * dense zs_extra for the deformation variants (|terms| stay below
+// 2^31: a balanced residue plus two products of balanced residues).
+template <bool SMALL, bool STREAM>
+__global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, const uint4* __restrict__ y,
+                                                                  const int32_t* __restrict__ zs,
+                                                                  uint4* __restrict__ u) {
+    extern __shared__ int32_t sm[];
+    const Tables T = stage(D, D.blob_f, sm);
+    BW_ITEMS(item, D.n2) {
+        const uint32_t s = static_cast<uint32_t>(item);
+        const uint32_t d = __ldg(D.m2 + s);
+        const int uch = static_cast<int>(d >> 26);
+        const int nu = T.a1off[uch + 1] - T.a1off[uch];
+        int4 out[2] = {make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0)};
+        if (nu > 0) {
+            Acc4<SMALL> acc0, acc1;
+            gather_block<SMALL, STREAM>(D.inc_d2f, D.n2, s, D.w_d2f, T.coef, D.n, D.r, uch, y, acc0, acc1);
+            out[0] = acc0.reduce(D.mod);
+            if (nu > 1) out[1] = acc1.reduce(D.mod);
+            if (D.n_extra) {
+                const long long urow = d & kLow26;
+                for (int q = 0; q < nu; ++q) {
+                    int4 v = out[q];
+                    for (int j = 0; j < D.n_extra; ++j) {
+                        const int32_t c = D.dense_sign * __ldg(D.dense + (urow + q) * D.n_extra + j);
+                        const int4 e = ld4(zs, static_cast<long long>(D.z_cols) + j);
+                        v.x += c * e.x;
+                        v.y += c * e.y;
+                        v.z += c * e.z;
+                        v.w += c * e.w;
+                    }
+                    out[q] = make_int4(reduce_balanced(v.x, D.mod), reduce_balanced(v.y, D.mod),
+                                       reduce_balanced(v.z, D.mod), reduce_balanced(v.w, D.mod));
+                }
+            }
+        }
+        st_block(u, s, out[0], out[1]);
+    }
+}
+
+// u2 = P u over the padded u rows (P = T^t Dr T folded, int16 values; padding
+// rows are empty and come out zero).
+template <bool SMALL, bool STREAM>
+__global__ void __launch_bounds__(kThreads) sub_spmv_kernel(SubsetDev D, const uint2* __restrict__ u,
+                                                            uint2* __restrict__ u2) {
+    BW_ITEMS(row, 2 * static_cast<long long>(D.n2)) {
+        Acc4<SMALL> acc;
+        const uint32_t e1 = __ldg(D.p_ptr + row + 1);
+        for (uint32_t e = __ldg(D.p_ptr + row); e < e1; ++e) {
+            const uint2 v = __ldg(u + ld_table<STREAM>(D.p_col + e));
+            acc.mac(ld_table<STREAM>(D.p_val + e), unpack_row(v.x, v.y));
+        }
+        u2[row] = pack_row(acc.reduce(D.mod));
     }
 }
 
 // (m-1)-subset S: its h rows h(S, a) = (D_(m-1)^t u2)(S, a), then
-//   t_adj(S, beta) = sum_a R[a,beta] h(S, a)               (all t rows of S)
-//   out_z(S, kappa) = dc * sum_a B[a,kappa] h(S, a)        (z rows, through op_col)
-template <bool SMALL>
+//   t_adj(S, beta) = sum_a R[a,beta] h(S, a)               (padded t block)
+//   out_z(S, kappa) = dc * sum_a B[a,kappa] h(S, a)        (compact, through op_col)
+template <bool SMALL, bool STREAM>
 __global__ void __launch_bounds__(kThreads) sub_d2_transpose_adjoint_kernel(SubsetDev D,
-                                                                            const int32_t* __restrict__ u2,
+                                                                            const uint4* __restrict__ u2,
                                                                             const int32_t* __restrict__ dc,
-                                                                            int32_t* __restrict__ t_adj,
+                                                                            uint4* __restrict__ t_adj,
                                                                             int32_t* __restrict__ out) {
     extern __shared__ int32_t sm[];
     const Tables T = stage(D, D.blob_t, sm);
-    BW_SUBSETS(s, D.n1) {
-        const uint32_t dt = __ldg(D.m1_t + s);
-        const int tch = static_cast<int>(dt >> 26);
-        const int ych = T.ych[tch];
+    BW_ITEMS(item, D.n1) {
+        const uint32_t s = static_cast<uint32_t>(item);
+        const uint32_t d = __ldg(D.m1 + s);
+        const int tch = static_cast<int>(d >> 26), ych = T.ych[tch];
         const int ya = T.a0off[ych], ny = T.a0off[ych + 1] - ya;
         const int a0 = ny > 0 ? T.a0idx[ya] : 0, a1 = ny > 1 ? T.a0idx[ya + 1] : a0;
         int4 h0 = make_int4(0, 0, 0, 0), h1 = h0;
         if (ny > 0) {
             Acc4<SMALL> acc0, acc1;
-            gather2<SMALL>(D.inc_d2t, D.n1, s, D.w_d2t, T.coef, D.n, D.K, a0, a1, u2, acc0, acc1);
+            gather_block<SMALL, STREAM>(D.inc_d2t, D.n1, s, D.w_d2t, T.coef, D.n, D.r, ych, u2, acc0, acc1);
             h0 = acc0.reduce(D.mod);
             h1 = acc1.reduce(D.mod);
         }
         const int tb = T.a1off[tch], nt = T.a1off[tch + 1] - tb;
-        const long long trow = dt & kOffsetMask;
+        int4 tv[2] = {make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0)};
         for (int q = 0; q < nt; ++q) {
             const int beta = T.a1idx[tb + q];
             Acc4<SMALL> acc;
             if (ny > 0) acc.mac(T.R[a0 * D.n + beta], h0);
             if (ny > 1) acc.mac(T.R[a1 * D.n + beta], h1);
-            st4(t_adj, trow + q, acc.reduce(D.mod));
+            tv[q] = acc.reduce(D.mod);
         }
+        st_block(t_adj, s, tv[0], tv[1]);
         const int kb = T.koff[ych], nz = T.koff[ych + 1] - kb;
-        if (nz == 0) continue;
-        const long long zfirst = static_cast<long long>(D.x_cols) + __ldg(D.m1_z + s);
+        const long long zfirst = static_cast<long long>(D.x_cols) + (d & kLow26);
         for (int q = 0; q < nz; ++q) {
             const long long orow = cyc::op_col(D.drop0, D.drop1, zfirst + q);
             if (orow < 0) continue;   // dropped base column (replacement)
@@ -242,22 +330,22 @@ __global__ void __launch_bounds__(kThreads) sub_d2_transpose_adjoint_kernel(Subs
     }
 }
 
-// m-subset S': its x rows out_x(S', a) = -dc * (D_m^t t_adj)(S', a), through op_col.
-template <bool SMALL>
-__global__ void __launch_bounds__(kThreads) sub_dm_transpose_kernel(SubsetDev D, const int32_t* __restrict__ t_adj,
+// m-subset S': its x rows out_x(S', a) = -dc * (D_m^t t_adj)(S', a), compact through op_col.
+template <bool SMALL, bool STREAM>
+__global__ void __launch_bounds__(kThreads) sub_dm_transpose_kernel(SubsetDev D, const uint4* __restrict__ t_adj,
                                                                     const int32_t* __restrict__ dc,
                                                                     int32_t* __restrict__ out) {
     extern __shared__ int32_t sm[];
     const Tables T = stage(D, D.blob_t, sm);
-    BW_SUBSETS(s, D.n0) {
-        const uint32_t dx = __ldg(D.m_x + s);
-        const int xch = static_cast<int>(dx >> 26);
-        const int xa = T.a0off[xch], nx = T.a0off[xch + 1] - xa;
+    BW_ITEMS(item, D.n0) {
+        const uint32_t s = static_cast<uint32_t>(item);
+        const uint32_t d = __ldg(D.m0 + s);
+        const int xch = static_cast<int>(d >> 26);
+        const int nx = T.a0off[xch + 1] - T.a0off[xch];
         if (nx == 0) continue;
-        const int a0 = T.a0idx[xa], a1 = nx > 1 ? T.a0idx[xa + 1] : a0;
         Acc4<SMALL> acc0, acc1;
-        gather2<SMALL>(D.inc_dmt, D.n0, s, D.w_dmt, T.coef, D.n, D.K, a0, a1, t_adj, acc0, acc1);
-        const long long xrow = dx & kOffsetMask;
+        gather_block<SMALL, STREAM>(D.inc_dmt, D.n0, s, D.w_dmt, T.coef, D.n, D.r, xch, t_adj, acc0, acc1);
+        const long long xrow = d & kLow26;
         for (int q = 0; q < nx; ++q) {
             const long long orow = cyc::op_col(D.drop0, D.drop1, xrow + q);
             if (orow < 0) continue;   // dropped base column (replacement)
@@ -267,11 +355,109 @@ __global__ void __launch_bounds__(kThreads) sub_dm_transpose_kernel(SubsetDev D,
     }
 }
 
+// Extra source rows of the deformation transpose from the padded u2:
+//   out[kept_cols + j][c] = dense_sign * dc[kept_cols + j] * sum_row dense[row][j] u2[row][c]
+// Each CTA sums a stripe of padded rows; the CTA sums meet in an 8-entry
+// accumulator (cyc::grid_sum) and the last CTA writes the n_extra rows.
+__global__ void __launch_bounds__(kThreads) sub_dense_t_kernel(SubsetDev D, const uint2* __restrict__ u2,
+                                                               const int32_t* __restrict__ dc,
+                                                               int32_t* __restrict__ out,
+                                                               int32_t* __restrict__ partials,
+                                                               unsigned int* __restrict__ counter) {
+    extern __shared__ int32_t sm[];
+    const Tables T = stage(D, D.blob_f, sm);
+    int32_t acc[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) acc[e] = 0;
+    int cnt = 0;
+    BW_ITEMS(row, 2 * static_cast<long long>(D.n2)) {
+        const uint32_t d = __ldg(D.m2 + (row >> 1));
+        const int uch = static_cast<int>(d >> 26);
+        const int q = static_cast<int>(row & 1);
+        if (q >= T.a1off[uch + 1] - T.a1off[uch]) continue;   // padding slot
+        const long long crow = static_cast<long long>(d & kLow26) + q;
+        const uint2 w = __ldg(u2 + row);
+        const int4 v = unpack_row(w.x, w.y);
+        for (int j = 0; j < D.n_extra; ++j) {
+            const int32_t c = __ldg(D.dense + crow * D.n_extra + j);
+            acc[4 * j] += c * v.x;
+            acc[4 * j + 1] += c * v.y;
+            acc[4 * j + 2] += c * v.z;
+            acc[4 * j + 3] += c * v.w;
+        }
+        if (++cnt == 8) {   // 8 products of balanced residues stay below 2^31
+            cnt = 0;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) acc[e] = reduce_partial(acc[e], D.mod);
+        }
+    }
+    __shared__ int32_t red[kThreads / 32][8];
+    __shared__ bool am_last;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        int32_t v = reduce_balanced(acc[e], D.mod);
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) red[warp][e] = reduce_balanced(v, D.mod);
+    }
+    __syncthreads();
+    int32_t mine = 0, total = 0;
+    if (threadIdx.x < 8) {
+        for (int w = 0; w < kThreads / 32; ++w) mine += red[w][threadIdx.x];
+        mine = reduce_balanced(mine, D.mod);
+    }
+    if (!cyc::grid_sum(partials, counter, 8, mine, total, &am_last)) return;
+    if (threadIdx.x < 4 * D.n_extra) {
+        const int j = threadIdx.x / 4, c = threadIdx.x % 4;
+        const long long orow = static_cast<long long>(D.kept_cols) + j;
+        int32_t v = D.dense_sign * reduce_balanced(total, D.mod);
+        if (dc) v = reduce_balanced(v * __ldg(dc + orow), D.mod);
+        out[orow * 4 + c] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *counter = 0;
+        __threadfence();
+    }
+}
+
+// Compact int32 u rows <-> padded int16 u blocks (the non-hot entry points:
+// forward / target_precondition / backward on compact vectors).
+__global__ void __launch_bounds__(kThreads) sub_u_pack_kernel(SubsetDev D, const int32_t* __restrict__ u32,
+                                                              uint4* __restrict__ u16) {
+    extern __shared__ int32_t sm[];
+    const Tables T = stage(D, D.blob_f, sm);
+    BW_ITEMS(item, D.n2) {
+        const uint32_t d = __ldg(D.m2 + item);
+        const int uch = static_cast<int>(d >> 26);
+        const int nu = T.a1off[uch + 1] - T.a1off[uch];
+        const long long first = d & kLow26;
+        const int4 zero = make_int4(0, 0, 0, 0);
+        st_block(u16, static_cast<uint32_t>(item), nu > 0 ? ld4(u32, first) : zero,
+                 nu > 1 ? ld4(u32, first + 1) : zero);
+    }
+}
+__global__ void __launch_bounds__(kThreads) sub_u_unpack_kernel(SubsetDev D, const uint4* __restrict__ u16,
+                                                                int32_t* __restrict__ u32) {
+    extern __shared__ int32_t sm[];
+    const Tables T = stage(D, D.blob_f, sm);
+    BW_ITEMS(item, D.n2) {
+        const uint32_t d = __ldg(D.m2 + item);
+        const int uch = static_cast<int>(d >> 26);
+        const int nu = T.a1off[uch + 1] - T.a1off[uch];
+        const long long first = d & kLow26;
+        const uint4 b = __ldg(u16 + item);
+        if (nu > 0) st4(u32, first, unpack_row(b.x, b.y));
+        if (nu > 1) st4(u32, first + 1, unpack_row(b.z, b.w));
+    }
+}
+
 int32_t balanced_of(uint32_t v, const Mod& m) { return to_balanced(v % static_cast<uint32_t>(m.p), m); }
 
 }  // namespace
 
-// Builds the subset tables and the two shared-memory blobs; leaves
+// Builds the subset tables, the padded preconditioner and the two
+// shared-memory blobs, and allocates the padded int16 vectors; leaves
 // subset_path false (and says why in subset_reason) when the sector does not
 // fit the format or BW_CYCLIC_GENERIC asks for the generic row kernels.
 void CyclicCtx::setup_subset_path() {
@@ -283,22 +469,21 @@ void CyclicCtx::setup_subset_path() {
         }
     }
     cyclic::SubsetTables tab;
-    subset_reason = cyclic::build_subset_tables(inst, es, tab);
+    subset_reason = cyclic::build_subset_tables(inst, es, precond, tab);
     if (!subset_reason.empty()) return;
 
     const cyclic::CharMap a0 = cyclic::build_char_map(inst.weight_a0, inst.r);
     const cyclic::CharMap a1 = cyclic::build_char_map(inst.weight_a1, inst.r);
     const cyclic::CharMap km = cyclic::build_char_map(inst.kernel_weights, inst.r);
     const int n = static_cast<int>(inst.n), g = static_cast<int>(inst.genus), r = static_cast<int>(inst.r);
-    const int kdim = static_cast<int>(inst.kernel_dim()), K = std::max(n, g);
+    const int kdim = static_cast<int>(inst.kernel_dim());
     SubsetDev& D = S;
     D.mod = mod;
     D.n = n;
     D.g = g;
     D.kdim = kdim;
     D.r = r;
-    D.K = K;
-    int w = 4 * n * K;
+    int w = 4 * n * r;   // coefficients: [2 signs][n][r] x int2
     D.o_R = w;
     w += g * n;
     D.o_B = w;
@@ -337,82 +522,148 @@ void CyclicCtx::setup_subset_path() {
     for (int e = 0; e < kdim; ++e) common[D.o_kidx + e] = km.indices[e];
     for (int c = 0; c < r; ++c)
         common[D.o_ych + c] = static_cast<int32_t>((c + r - static_cast<int>(inst.w_weight % inst.r)) % r);
-    std::vector<int32_t> blob_f = common, blob_t = common;
-    auto coef_at = [&](std::vector<int32_t>& blob, int neg, int i, int key, int l, uint32_t mu) {
+    // Coefficient word (sign, generator i, own character ch), own rows k = 0, 1
+    // (the first two keys of ch's block), neighbour slots l = 0, 1:
+    //   int16 number 2 k + l = +-mu at (own key k, neighbour key l).
+    auto put = [&](std::vector<int32_t>& blob, int i, int ch, int k, int l, uint32_t mu) {
         const int32_t b = balanced_of(mu, mod);
-        blob[(((neg * n + i) * K + key) * 2) + l] = neg ? -b : b;
-    };
-    // forward: (i, beta) -> mu[i, beta, a] over the A0 block of A1(beta) - V(i)
-    for (int i = 0; i < n; ++i)
-        for (int beta = 0; beta < n; ++beta) {
-            const uint32_t q = (inst.weight_a1[beta] + inst.r - inst.weight_v[i] % inst.r) % inst.r;
-            for (uint32_t idx = a0.offsets[q]; idx < a0.offsets[q + 1]; ++idx)
-                for (int neg = 0; neg < 2; ++neg)
-                    coef_at(blob_f, neg, i, beta, static_cast<int>(idx - a0.offsets[q]),
-                            inst.mu_at(i, beta, a0.indices[idx]));
+        for (int neg = 0; neg < 2; ++neg) {
+            const int32_t v = neg ? -b : b;
+            uint32_t& word = reinterpret_cast<uint32_t&>(blob[2 * ((neg * n + i) * r + ch) + k]);
+            word |= (static_cast<uint32_t>(v) & 0xFFFFu) << (16 * l);
         }
-    // transpose: (j, a) -> mu[j, beta, a] over the A1 block of A0(a) + V(j)
-    for (int j = 0; j < n; ++j)
-        for (int a = 0; a < g; ++a) {
-            const uint32_t q = (inst.weight_a0[a] + inst.weight_v[j]) % inst.r;
-            for (uint32_t idx = a1.offsets[q]; idx < a1.offsets[q + 1]; ++idx)
-                for (int neg = 0; neg < 2; ++neg)
-                    coef_at(blob_t, neg, j, a, static_cast<int>(idx - a1.offsets[q]),
-                            inst.mu_at(j, a1.indices[idx], a));
+    };
+    std::vector<int32_t> blob_f = common, blob_t = common;
+    for (int i = 0; i < n; ++i)
+        for (int ch = 0; ch < r; ++ch) {
+            // forward: own rows beta in the A1 block of ch; neighbour rows a in
+            // the A0 block of A1(beta) - V(i) (the same block for both betas)
+            for (uint32_t kb = a1.offsets[ch]; kb < a1.offsets[ch + 1]; ++kb) {
+                const int beta = a1.indices[kb];
+                const uint32_t q = (inst.weight_a1[beta] + inst.r - inst.weight_v[i] % inst.r) % inst.r;
+                for (uint32_t lb = a0.offsets[q]; lb < a0.offsets[q + 1]; ++lb)
+                    put(blob_f, i, ch, static_cast<int>(kb - a1.offsets[ch]), static_cast<int>(lb - a0.offsets[q]),
+                        inst.mu_at(i, beta, a0.indices[lb]));
+            }
+            // transpose: own rows a in the A0 block of ch; neighbour rows beta
+            // in the A1 block of A0(a) + V(i)
+            for (uint32_t kb = a0.offsets[ch]; kb < a0.offsets[ch + 1]; ++kb) {
+                const int a = a0.indices[kb];
+                const uint32_t q = (inst.weight_a0[a] + inst.weight_v[i]) % inst.r;
+                for (uint32_t lb = a1.offsets[q]; lb < a1.offsets[q + 1]; ++lb)
+                    put(blob_t, i, ch, static_cast<int>(kb - a0.offsets[ch]), static_cast<int>(lb - a1.offsets[q]),
+                        inst.mu_at(i, a1.indices[lb], a));
+            }
         }
 
-    D.n1 = static_cast<uint32_t>(tab.m1_t.size());
-    D.n2 = static_cast<uint32_t>(tab.m2_u.size());
-    D.n0 = static_cast<uint32_t>(tab.m_x.size());
+    D.n1 = static_cast<uint32_t>(tab.m1.size());
+    D.n2 = static_cast<uint32_t>(tab.m2.size());
+    D.n0 = static_cast<uint32_t>(tab.m0.size());
     D.w_dmf = static_cast<uint32_t>(es.dm.row_width);
     D.w_d2f = static_cast<uint32_t>(es.d2.row_width);
     D.w_d2t = static_cast<uint32_t>(es.d2.column_width);
     D.w_dmt = static_cast<uint32_t>(es.dm.column_width);
-    D.m1_t = upload(tab.m1_t);
-    D.m1_y = upload(tab.m1_y);
-    D.m1_z = upload(tab.m1_z);
-    D.m2_u = upload(tab.m2_u);
-    D.m_x = upload(tab.m_x);
+    D.m1 = upload(tab.m1);
+    D.m2 = upload(tab.m2);
+    D.m0 = upload(tab.m0);
     D.inc_dmf = upload(tab.inc_dmf);
     D.inc_d2f = upload(tab.inc_d2f);
     D.inc_d2t = upload(tab.inc_d2t);
     D.inc_dmt = upload(tab.inc_dmt);
+    D.p_ptr = upload(tab.p_ptr);
+    D.p_col = upload(tab.p_col);
+    D.p_val = upload(tab.p_val);
     D.blob_f = upload(blob_f);
     D.blob_t = upload(blob_t);
     D.x_cols = es.x_cols;
-    D.base_cols = E.base_cols;
+    D.z_cols = es.z_cols;
+    D.kept_cols = E.kept_cols;
     D.drop0 = E.drop0;
     D.drop1 = E.drop1;
     D.n_extra = E.n_extra;
     D.dense_sign = E.dense_sign;
     D.dense = E.dense;
+    // Tables read once per application: evict-first when they exceed half the L2.
+    const size_t table_bytes = 4 * (tab.inc_dmf.size() + tab.inc_d2f.size() + tab.inc_d2t.size() +
+                                    tab.inc_dmt.size() + tab.p_ptr.size() + tab.p_col.size()) +
+                               2 * tab.p_val.size();
+    int l2 = 0;
+    BW_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
+    stream_tables = table_bytes > static_cast<size_t>(l2) / 2;
+    d_xs16 = alloc<uint4>(D.n0);
+    d_zs = alloc<int32_t>((es.z_cols + dense.columns) * num_v);
+    d_y16 = alloc<uint4>(D.n1);
+    d_t16 = alloc<uint4>(D.n1);
+    d_u16 = alloc<uint4>(D.n2);
+    d_u2_16 = alloc<uint4>(D.n2);
     subset_path = true;
 }
 
-void CyclicCtx::subset_forward(int32_t* u) {
+// Kernel template dispatch: SMALL (int32 sums exact) x STREAM (tables above L2).
+#define BW_SUBSET_DISPATCH(launch)      \
+    do {                                \
+        if (small && stream_tables) {   \
+            launch(true, true);         \
+        } else if (small) {             \
+            launch(true, false);        \
+        } else if (stream_tables) {     \
+            launch(false, true);        \
+        } else {                        \
+            launch(false, false);       \
+        }                               \
+    } while (0)
+
+void CyclicCtx::subset_forward16(const int32_t* in, const int32_t* dc) {
     const size_t smem = static_cast<size_t>(S.blob_words) * 4;
-    if (small) {
-        sub_dm_forward_elim_kernel<true><<<grid_for(S.n1), kThreads, smem, stream>>>(S, d_xs, d_y);
-        sub_d2_forward_kernel<true><<<grid_for(S.n2), kThreads, smem, stream>>>(S, d_y, d_xs, u);
-    } else {
-        sub_dm_forward_elim_kernel<false><<<grid_for(S.n1), kThreads, smem, stream>>>(S, d_xs, d_y);
-        sub_d2_forward_kernel<false><<<grid_for(S.n2), kThreads, smem, stream>>>(S, d_y, d_xs, u);
-    }
+    const size_t items = static_cast<size_t>(S.n0) + es.z_cols + dense.columns;
+    sub_source_kernel<<<grid_for(items), kThreads, smem, stream>>>(S, in, dc, d_xs16, d_zs);
+#define BW_LAUNCH(A, B)                                                                                      \
+    sub_dm_forward_elim_kernel<A, B><<<grid_for(S.n1), kThreads, smem, stream>>>(S, d_xs16, d_zs, d_y16); \
+    sub_d2_forward_kernel<A, B><<<grid_for(S.n2), kThreads, smem, stream>>>(S, d_y16, d_zs, d_u16)
+    BW_SUBSET_DISPATCH(BW_LAUNCH);
+#undef BW_LAUNCH
     BW_CHECK_LAUNCH();
-    launches += 2;
+    launches += 3;
 }
 
-void CyclicCtx::subset_backward(const int32_t* u2, const int32_t* dc, int32_t* out) {
+void CyclicCtx::subset_precondition16() {
+    const uint2* u = reinterpret_cast<const uint2*>(d_u16);
+    uint2* u2 = reinterpret_cast<uint2*>(d_u2_16);
+    const unsigned grid = grid_for(2 * static_cast<size_t>(S.n2));
+#define BW_LAUNCH(A, B) sub_spmv_kernel<A, B><<<grid, kThreads, 0, stream>>>(S, u, u2)
+    BW_SUBSET_DISPATCH(BW_LAUNCH);
+#undef BW_LAUNCH
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+void CyclicCtx::subset_backward16(const int32_t* dc, int32_t* out) {
     const size_t smem = static_cast<size_t>(S.blob_words) * 4;
-    if (small) {
-        sub_d2_transpose_adjoint_kernel<true><<<grid_for(S.n1), kThreads, smem, stream>>>(S, u2, dc, d_t, out);
-        sub_dm_transpose_kernel<true><<<grid_for(S.n0), kThreads, smem, stream>>>(S, d_t, dc, out);
-    } else {
-        sub_d2_transpose_adjoint_kernel<false><<<grid_for(S.n1), kThreads, smem, stream>>>(S, u2, dc, d_t, out);
-        sub_dm_transpose_kernel<false><<<grid_for(S.n0), kThreads, smem, stream>>>(S, d_t, dc, out);
-    }
+#define BW_LAUNCH(A, B)                                                                                         \
+    sub_d2_transpose_adjoint_kernel<A, B><<<grid_for(S.n1), kThreads, smem, stream>>>(S, d_u2_16, dc, d_t16, out); \
+    sub_dm_transpose_kernel<A, B><<<grid_for(S.n0), kThreads, smem, stream>>>(S, d_t16, dc, out)
+    BW_SUBSET_DISPATCH(BW_LAUNCH);
+#undef BW_LAUNCH
     BW_CHECK_LAUNCH();
     launches += 2;
+    if (S.n_extra) {
+        sub_dense_t_kernel<<<dense_grid, kThreads, smem, stream>>>(S, reinterpret_cast<const uint2*>(d_u2_16), dc,
+                                                                   out, d_dpart, d_dcounter);
+        BW_CHECK_LAUNCH();
+        ++launches;
+    }
+}
+
+void CyclicCtx::subset_pack_u(const int32_t* u32, uint4* u16) {
+    sub_u_pack_kernel<<<grid_for(S.n2), kThreads, static_cast<size_t>(S.blob_words) * 4, stream>>>(S, u32, u16);
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+void CyclicCtx::subset_unpack_u(const uint4* u16, int32_t* u32) {
+    sub_u_unpack_kernel<<<grid_for(S.n2), kThreads, static_cast<size_t>(S.blob_words) * 4, stream>>>(S, u16, u32);
+    BW_CHECK_LAUNCH();
+    ++launches;
 }
 
 }  // namespace bw

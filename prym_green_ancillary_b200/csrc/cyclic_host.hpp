@@ -139,24 +139,30 @@ struct EliminatedSector {
 EliminatedSector assemble_eliminated_sector(const Instance& inst, size_t sector);
 
 // ----- subset-major tables of the four Koszul gathers (device layout)
-// One entry per subset of each degree and one incidence word per (position,
-// subset), laid out [position][subset] so that consecutive subsets read
-// consecutive words.  An incidence word is the first row of the neighbour
-// block in the gathered vector | i << 26 | (sign negative) << 31; a subset
-// word is the first row of its own block | character << 26.
+// Internal vectors hold every subset's block in two row slots (2 s, 2 s + 1),
+// so a neighbour block is found from its subset rank alone.  One entry per
+// subset of each degree, and one incidence word per (position, subset) laid
+// out [position][subset] so that consecutive subsets read consecutive words.
+// An incidence word is the neighbour subset's rank | i << 26 | (sign
+// negative) << 31; a subset word is the first compact row of one of its
+// blocks | its character << 26.
 struct SubsetTables {
-    // (m-1)-subsets: t block (and character), y block, z block
-    std::vector<uint32_t> m1_t, m1_y, m1_z;
-    std::vector<uint32_t> m2_u;   // (m-2)-subsets: u block | character
-    std::vector<uint32_t> m_x;    // m-subsets: x block | character
-    // D_m (row subsets, neighbours T u i in x), D_(m-1) (neighbours in y),
-    // D_(m-1)^t (neighbours S \ j in u), D_m^t (neighbours in t)
+    std::vector<uint32_t> m1;   // (m-1)-subsets: z block (compact) | t character
+    std::vector<uint32_t> m2;   // (m-2)-subsets: u block (compact) | u character
+    std::vector<uint32_t> m0;   // m-subsets: x block (compact) | x character
+    // D_m (row subsets, neighbours T u i), D_(m-1) (neighbours T u i),
+    // D_(m-1)^t (neighbours S \ j), D_m^t (neighbours S \ j)
     std::vector<uint32_t> inc_dmf, inc_d2f, inc_d2t, inc_dmt;
+    // the folded target preconditioner over the padded u rows: every compact
+    // row u_off(s) + q becomes 2 s + q (empty padding rows); balanced values
+    std::vector<uint32_t> p_ptr, p_col;
+    std::vector<int16_t> p_val;
 };
 // Empty string: the tables are built.  Otherwise the reason this sector does
 // not fit the packed format (a character block above two rows, an index or
-// offset beyond its field), and `out` is left empty.
-std::string build_subset_tables(const Instance& inst, const EliminatedSector& es, SubsetTables& out);
+// rank beyond its field), and `out` is left empty.
+std::string build_subset_tables(const Instance& inst, const EliminatedSector& es, const Csr& precond,
+                                SubsetTables& out);
 
 // ----- deformation inputs (cuda/cuprym_deformation.cu:426-473)
 // Both files are read the way the reference reads them: a key is its first

@@ -830,7 +830,8 @@ EliminatedSector assemble_eliminated_sector(const Instance& inst, size_t sector)
 }
 
 // Subset-major gather tables (the device side is bw_cyclic_subset.cu).
-std::string build_subset_tables(const Instance& inst, const EliminatedSector& es, SubsetTables& out) {
+std::string build_subset_tables(const Instance& inst, const EliminatedSector& es, const Csr& precond,
+                                SubsetTables& out) {
     out = SubsetTables{};
     const CharMap a0 = build_char_map(inst.weight_a0, inst.r);
     const CharMap a1 = build_char_map(inst.weight_a1, inst.r);
@@ -838,45 +839,71 @@ std::string build_subset_tables(const Instance& inst, const EliminatedSector& es
     if (a0.max_block() > 2 || a1.max_block() > 2 || km.max_block() > 2) return "a character block has more than two rows";
     if (inst.n > 32) return "more than 32 generators";
     if (inst.r > 64) return "cyclic order above 64";
-    const uint64_t limit = 1ull << 26;
-    if (es.total_cols() >= limit || es.t_rows >= limit || es.y_rows >= limit || es.target_rows >= limit)
-        return "a vector has 2^26 rows or more";
+    if (inst.modulus >= (1u << 15)) return "prime above 2^15 (balanced residues must fit int16)";
     const Incidence& dm = es.dm;
     const Incidence& d2 = es.d2;
     const size_t n1 = dm.row_subsets, n2 = d2.row_subsets, n0 = dm.column_subsets;
+    const uint64_t limit = 1ull << 26;
+    if (n0 >= limit || n1 >= limit || n2 >= limit || es.total_cols() >= limit || es.target_rows >= limit)
+        return "2^26 subsets or rows or more";
     if (d2.column_subsets != n1) return "inconsistent subset counts";
-    out.m1_t.resize(n1);
-    out.m1_y.resize(n1);
-    out.m1_z.resize(n1);
-    out.m2_u.resize(n2);
-    out.m_x.resize(n0);
-    for (size_t s = 0; s < n1; ++s) {
-        const uint32_t ch = sub_mod(es.sector, dm.row_subset_weights[s], inst.r);
-        out.m1_t[s] = es.dm_layout.row_offsets[s] | (ch << 26);
-        out.m1_y[s] = es.d2_layout.col_offsets[s];
-        out.m1_z[s] = es.z_layout.offsets[s];
-    }
+    if (precond.row_ptr.size() != es.target_rows + 1) return "preconditioner size does not match the sector";
+    out.m1.resize(n1);
+    out.m2.resize(n2);
+    out.m0.resize(n0);
+    for (size_t s = 0; s < n1; ++s)
+        out.m1[s] = es.z_layout.offsets[s] | (sub_mod(es.sector, dm.row_subset_weights[s], inst.r) << 26);
     for (size_t s = 0; s < n2; ++s)
-        out.m2_u[s] = es.d2_layout.row_offsets[s] | (sub_mod(es.y_sector, d2.row_subset_weights[s], inst.r) << 26);
+        out.m2[s] = es.d2_layout.row_offsets[s] | (sub_mod(es.y_sector, d2.row_subset_weights[s], inst.r) << 26);
     for (size_t s = 0; s < n0; ++s)
-        out.m_x[s] = es.dm_layout.col_offsets[s] | (sub_mod(es.sector, dm.column_subset_weights[s], inst.r) << 26);
+        out.m0[s] = es.dm_layout.col_offsets[s] | (sub_mod(es.sector, dm.column_subset_weights[s], inst.r) << 26);
     // incidence words, transposed to [position][subset]
     auto fill = [](std::vector<uint32_t>& dst, size_t subsets, size_t width, const std::vector<uint32_t>& nb,
-                   const std::vector<uint32_t>& idx, const std::vector<uint8_t>& neg,
-                   const std::vector<uint32_t>& offsets) {
+                   const std::vector<uint32_t>& idx, const std::vector<uint8_t>& neg) {
         dst.resize(subsets * width);
         parallel_chunks(subsets, [&](size_t b, size_t e) {
             for (size_t s = b; s < e; ++s)
                 for (size_t pos = 0; pos < width; ++pos) {
                     const size_t q = s * width + pos;
-                    dst[pos * subsets + s] = offsets[nb[q]] | (idx[q] << 26) | (neg[q] ? 0x80000000u : 0u);
+                    dst[pos * subsets + s] = nb[q] | (idx[q] << 26) | (neg[q] ? 0x80000000u : 0u);
                 }
         });
     };
-    fill(out.inc_dmf, n1, dm.row_width, dm.row_col, dm.row_i, dm.row_neg, es.dm_layout.col_offsets);
-    fill(out.inc_d2f, n2, d2.row_width, d2.row_col, d2.row_i, d2.row_neg, es.d2_layout.col_offsets);
-    fill(out.inc_d2t, n1, d2.column_width, d2.col_row, d2.col_i, d2.col_neg, es.d2_layout.row_offsets);
-    fill(out.inc_dmt, n0, dm.column_width, dm.col_row, dm.col_i, dm.col_neg, es.dm_layout.row_offsets);
+    fill(out.inc_dmf, n1, dm.row_width, dm.row_col, dm.row_i, dm.row_neg);
+    fill(out.inc_d2f, n2, d2.row_width, d2.row_col, d2.row_i, d2.row_neg);
+    fill(out.inc_d2t, n1, d2.column_width, d2.col_row, d2.col_i, d2.col_neg);
+    fill(out.inc_dmt, n0, dm.column_width, dm.col_row, dm.col_i, dm.col_neg);
+    // padded preconditioner: compact row -> padded slot
+    std::vector<uint32_t> slot(es.target_rows);
+    for (size_t s = 0; s < n2; ++s)
+        for (uint32_t q = es.d2_layout.row_offsets[s]; q < es.d2_layout.row_offsets[s + 1]; ++q)
+            slot[q] = static_cast<uint32_t>(2 * s + (q - es.d2_layout.row_offsets[s]));
+    std::vector<uint32_t> compact_of(2 * n2, UINT32_MAX);
+    for (size_t q = 0; q < es.target_rows; ++q) compact_of[slot[q]] = static_cast<uint32_t>(q);
+    const int32_t p = static_cast<int32_t>(inst.modulus), half = (p - 1) / 2;
+    out.p_ptr.resize(2 * n2 + 1);
+    out.p_ptr[0] = 0;
+    for (size_t pr = 0; pr < 2 * n2; ++pr) {
+        const uint32_t q = compact_of[pr];
+        const size_t len = q == UINT32_MAX ? 0 : precond.row_ptr[q + 1] - precond.row_ptr[q];
+        if (out.p_ptr[pr] + len >= (1ull << 32)) return "preconditioner above 2^32 entries";
+        out.p_ptr[pr + 1] = static_cast<uint32_t>(out.p_ptr[pr] + len);
+    }
+    out.p_col.resize(out.p_ptr[2 * n2]);
+    out.p_val.resize(out.p_ptr[2 * n2]);
+    parallel_chunks(2 * n2, [&](size_t b, size_t e) {
+        for (size_t pr = b; pr < e; ++pr) {
+            const uint32_t q = compact_of[pr];
+            if (q == UINT32_MAX) continue;
+            uint32_t dst = out.p_ptr[pr];
+            for (uint32_t k = precond.row_ptr[q]; k < precond.row_ptr[q + 1]; ++k, ++dst) {
+                out.p_col[dst] = slot[precond.col[k]];
+                int32_t v = static_cast<int32_t>(precond.val[k] % inst.modulus);
+                if (v > half) v -= p;
+                out.p_val[dst] = static_cast<int16_t>(v);
+            }
+        }
+    });
     return "";
 }
 
