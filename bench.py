@@ -44,6 +44,11 @@ DESCRIPTIONS = {
                "dim R_(q+1) = dim R_q + 8, block widths 8/16/32, p=32003, own seeded maps/D/X/Y each",
 }
 METRIC = "block-Wiedemann steps/s, INT8-limb TC vs plain CUDA-core, bit-exact; %HBM peak"
+# The reference's published base-sector sequence loop (RESULTS.md, data/cases.json:
+# historical.base_gpu_time_median_seconds, RTX PRO 6000 Blackwell, v = 4), as
+# steps/s = 2 ceil((2 N / 4 + 50 - 1) / 4) / seconds.
+PUBLISHED_PAPER_STEPS_PER_S = {"g20": 13966.0, "g22": 9541.0, "g24": 3301.0, "g26": 841.6, "g28": 205.7,
+                               "g30": 38.1}
 # Paper mode (the eliminated cyclic operator of one sector of the shipped instances, block width 4):
 # name -> default timed steps (applications of S; two per round of 4 moments)
 PAPER = {"g20": 2000, "g22": 2000, "g24": 2000, "g26": 800, "g28": 200, "g30": 40}
@@ -396,7 +401,9 @@ def run_paper(args):
         line = {
             "metric": METRIC, "value": world * K / (ms / 1e3), "unit": "steps/s", "n_gpus": world, "steps": K,
             "warmup": 2 * rounds_w, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32 balanced residues (canonical u32 in the WDM)",
+            "vs_baseline": (world * K / (ms / 1e3)) / PUBLISHED_PAPER_STEPS_PER_S[args.workload],
+            "vs_baseline_note": "value / the reference's published median base-sector steps/s (RTX PRO 6000)",
+            "dtype": "int16/int32 balanced residues (canonical u32 in the WDM)",
             "data": f"shipped instance {args.workload}.json, seeded preconditioners and block (paper recipe)",
             "config": {"workload": args.workload, "sector": sector, "form": "paper (eliminated operator, v=4)",
                        "rows": rows, "cols": cols, "rounds_timed": rounds_k, "open_s": t_open,

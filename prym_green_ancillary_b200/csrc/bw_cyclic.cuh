@@ -47,7 +47,7 @@ struct ElimDev {
 // int16 with two row slots per subset.  The small tables (signed coefficients,
 // R, B, character maps) are staged in shared memory from one blob per
 // direction with the layout below (int32 words):
-//   coef [2 signs][n][r] x int2  (four packed int16: own rows x neighbour slots)
+//   coef [2 n codes][r] x int4  (own rows x neighbour slots; code = sign * n + generator)
 //   R [g][n], B [g][kdim], a0 offsets [r+1], a0 indices [g], a1 offsets [r+1],
 //   a1 indices [n], kernel-weight offsets [r+1], indices [kdim], ych [r]
 //   (ych[c] = y character of an (m-1)-subset whose t character is c).

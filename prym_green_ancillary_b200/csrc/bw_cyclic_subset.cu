@@ -12,8 +12,9 @@
 //     generator, sign) and each neighbour block once, and accumulates both
 //     rows of its own block;
 //   * the signed coefficients of mu for (sign, generator, own character) are
-//     four packed int16 in shared memory: one 8-byte load per incidence.
-// An incidence thus costs one coalesced word, one 16-byte load, one 8-byte
+//     four int32 in shared memory: one 16-byte load per incidence, indexed by
+//     the code the incidence word carries (sign * n + generator).
+// An incidence thus costs one coalesced word, one 16-byte load, one 16-byte
 // shared load and sixteen multiply-adds.
 //
 // Two of the reference's kernel pairs are fused, with their intermediates in
@@ -62,7 +63,7 @@ __device__ __forceinline__ void st_block(uint4* v, uint32_t s, const int4& r0, c
 
 // Views of the staged shared-memory tables.
 struct Tables {
-    const int2* coef;
+    const int4* coef;
     const int32_t *R, *B, *a0off, *a0idx, *a1off, *a1idx, *koff, *kidx, *ych;
 };
 
@@ -70,7 +71,7 @@ __device__ __forceinline__ Tables stage(const SubsetDev& D, const int32_t* __res
     for (int w = threadIdx.x; w < D.blob_words; w += blockDim.x) sm[w] = __ldg(blob + w);
     __syncthreads();
     Tables t;
-    t.coef = reinterpret_cast<const int2*>(sm);
+    t.coef = reinterpret_cast<const int4*>(sm);
     t.R = sm + D.o_R;
     t.B = sm + D.o_B;
     t.a0off = sm + D.o_a0off;
@@ -94,47 +95,60 @@ __device__ __forceinline__ T ld_table(const T* p) {
         return __ldg(p);
 }
 
-// acc_r += c_r0 * row0 + c_r1 * row1, the four coefficients packed in c
-// (.x: own row 0 against neighbour rows 0 and 1; .y: own row 1).
+// acc_k += c_k0 * row0 + c_k1 * row1 for the neighbour block b (two int16
+// rows) and c = (c_00, c_01, c_10, c_11).
 template <bool SMALL>
-__device__ __forceinline__ void mac_block(const int2& c, const uint4& b, Acc4<SMALL>& acc0, Acc4<SMALL>& acc1) {
+__device__ __forceinline__ void mac_block(const int4& c, const uint4& b, Acc4<SMALL>& acc0, Acc4<SMALL>& acc1) {
     const int4 r0 = unpack_row(b.x, b.y), r1 = unpack_row(b.z, b.w);
-    const uint32_t c0 = static_cast<uint32_t>(c.x), c1 = static_cast<uint32_t>(c.y);
-    acc0.mac(lo16(c0), r0);
-    acc0.mac(hi16(c0), r1);
-    acc1.mac(lo16(c1), r0);
-    acc1.mac(hi16(c1), r1);
+    acc0.mac(c.x, r0);
+    acc0.mac(c.y, r1);
+    acc1.mac(c.z, r0);
+    acc1.mac(c.w, r1);
 }
 
 // Both rows of subset s against its `width` neighbour blocks.  The coefficient
-// table is [sign][generator][own character]; a neighbour block with one row
-// has zero coefficients for its second slot (which holds zeros).  Incidence
-// words are read once per application (ld_table).
+// table is [code = sign * n + generator][own character]; a neighbour block with
+// one row has zero coefficients for its second slot (which holds zeros).
+// Incidence words are read once per application (ld_table).  `nin` is the
+// number of blocks of `in`, which carries one more, all-zero block at nin.
 template <bool SMALL, bool STREAM>
 __device__ __forceinline__ void gather_block(const uint32_t* __restrict__ inc, uint32_t nsub, uint32_t s,
-                                             uint32_t width, const int2* coef, int n, int r, int ch,
-                                             const uint4* __restrict__ in, Acc4<SMALL>& acc0, Acc4<SMALL>& acc1) {
-    // Four incidences at a time: their words, then their blocks, then the
-    // products, so that four independent 16-byte loads are in flight.
+                                             uint32_t width, const int4* coef, int r, int ch,
+                                             const uint4* __restrict__ in, uint32_t nin, Acc4<SMALL>& acc0,
+                                             Acc4<SMALL>& acc1) {
+    // Chunks of four incidences: a chunk's blocks are loaded together, and
+    // the next chunk's words while those blocks are in flight.  Only the
+    // words of a last, partial chunk are loaded under a mask; its empty slots
+    // hold the zero block (code 0), so the products run unmasked.
     constexpr int U = 4;
-    uint32_t pos = 0;
-    for (; pos + U <= width; pos += U) {
-        uint32_t e[U];
+    const uint32_t* p = inc + s;
+    const size_t step = nsub;
+    const uint32_t full = width / U, rem = width % U, chunks = full + (rem ? 1u : 0u);
+    auto words = [&](uint32_t k, uint32_t (&w)[U]) {
+        const uint32_t* q = p + static_cast<size_t>(k) * U * step;
+        if (k < full) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) w[u] = ld_table<STREAM>(q + u * step);
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) w[u] = static_cast<uint32_t>(u) < rem ? ld_table<STREAM>(q + u * step) : nin;
+        }
+    };
+    uint32_t e[U];
+    if (chunks == 0) return;
+    words(0, e);
+    for (uint32_t k = 0; k < chunks; ++k) {
         uint4 b[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) e[u] = ld_table<STREAM>(inc + static_cast<size_t>(pos + u) * nsub + s);
-#pragma unroll
         for (int u = 0; u < U; ++u) b[u] = __ldg(in + (e[u] & kLow26));
+        uint32_t next[U];
+        if (k + 1 < chunks) words(k + 1, next);
 #pragma unroll
-        for (int u = 0; u < U; ++u)
-            mac_block<SMALL>(coef[(static_cast<int>(e[u] >> 31) * n + static_cast<int>((e[u] >> 26) & 31u)) * r + ch],
-                             b[u], acc0, acc1);
-    }
-    for (; pos < width; ++pos) {
-        const uint32_t e = ld_table<STREAM>(inc + static_cast<size_t>(pos) * nsub + s);
-        const uint4 b = __ldg(in + (e & kLow26));
-        mac_block<SMALL>(coef[(static_cast<int>(e >> 31) * n + static_cast<int>((e >> 26) & 31u)) * r + ch], b, acc0,
-                         acc1);
+        for (int u = 0; u < U; ++u) mac_block<SMALL>(coef[static_cast<int>(e[u] >> 26) * r + ch], b[u], acc0, acc1);
+        if (k + 1 < chunks) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) e[u] = next[u];
+        }
     }
 }
 
@@ -198,7 +212,7 @@ __global__ void __launch_bounds__(kThreads) sub_dm_forward_elim_kernel(SubsetDev
             int4 t0 = make_int4(0, 0, 0, 0), t1 = t0;
             if (nt > 0) {
                 Acc4<SMALL> acc0, acc1;
-                gather_block<SMALL, STREAM>(D.inc_dmf, D.n1, s, D.w_dmf, T.coef, D.n, D.r, tch, xs, acc0, acc1);
+                gather_block<SMALL, STREAM>(D.inc_dmf, D.n1, s, D.w_dmf, T.coef, D.r, tch, xs, D.n0, acc0, acc1);
                 t0 = acc0.reduce(D.mod);
                 t1 = acc1.reduce(D.mod);
             }
@@ -241,12 +255,14 @@ __global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, c
         int4 out[2] = {make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0)};
         if (nu > 0) {
             Acc4<SMALL> acc0, acc1;
-            gather_block<SMALL, STREAM>(D.inc_d2f, D.n2, s, D.w_d2f, T.coef, D.n, D.r, uch, y, acc0, acc1);
+            gather_block<SMALL, STREAM>(D.inc_d2f, D.n2, s, D.w_d2f, T.coef, D.r, uch, y, D.n1, acc0, acc1);
             out[0] = acc0.reduce(D.mod);
             if (nu > 1) out[1] = acc1.reduce(D.mod);
             if (D.n_extra) {
                 const long long urow = d & kLow26;
-                for (int q = 0; q < nu; ++q) {
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    if (q >= nu) break;
                     int4 v = out[q];
                     for (int j = 0; j < D.n_extra; ++j) {
                         const int32_t c = D.dense_sign * __ldg(D.dense + (urow + q) * D.n_extra + j);
@@ -301,7 +317,7 @@ __global__ void __launch_bounds__(kThreads) sub_d2_transpose_adjoint_kernel(Subs
         int4 h0 = make_int4(0, 0, 0, 0), h1 = h0;
         if (ny > 0) {
             Acc4<SMALL> acc0, acc1;
-            gather_block<SMALL, STREAM>(D.inc_d2t, D.n1, s, D.w_d2t, T.coef, D.n, D.r, ych, u2, acc0, acc1);
+            gather_block<SMALL, STREAM>(D.inc_d2t, D.n1, s, D.w_d2t, T.coef, D.r, ych, u2, D.n2, acc0, acc1);
             h0 = acc0.reduce(D.mod);
             h1 = acc1.reduce(D.mod);
         }
@@ -344,7 +360,7 @@ __global__ void __launch_bounds__(kThreads) sub_dm_transpose_kernel(SubsetDev D,
         const int nx = T.a0off[xch + 1] - T.a0off[xch];
         if (nx == 0) continue;
         Acc4<SMALL> acc0, acc1;
-        gather_block<SMALL, STREAM>(D.inc_dmt, D.n0, s, D.w_dmt, T.coef, D.n, D.r, xch, t_adj, acc0, acc1);
+        gather_block<SMALL, STREAM>(D.inc_dmt, D.n0, s, D.w_dmt, T.coef, D.r, xch, t_adj, D.n1, acc0, acc1);
         const long long xrow = d & kLow26;
         for (int q = 0; q < nx; ++q) {
             const long long orow = cyc::op_col(D.drop0, D.drop1, xrow + q);
@@ -483,7 +499,7 @@ void CyclicCtx::setup_subset_path() {
     D.g = g;
     D.kdim = kdim;
     D.r = r;
-    int w = 4 * n * r;   // coefficients: [2 signs][n][r] x int2
+    int w = 8 * n * r;   // coefficients: [2 n codes][r] x int4
     D.o_R = w;
     w += g * n;
     D.o_B = w;
@@ -522,16 +538,12 @@ void CyclicCtx::setup_subset_path() {
     for (int e = 0; e < kdim; ++e) common[D.o_kidx + e] = km.indices[e];
     for (int c = 0; c < r; ++c)
         common[D.o_ych + c] = static_cast<int32_t>((c + r - static_cast<int>(inst.w_weight % inst.r)) % r);
-    // Coefficient word (sign, generator i, own character ch), own rows k = 0, 1
-    // (the first two keys of ch's block), neighbour slots l = 0, 1:
-    //   int16 number 2 k + l = +-mu at (own key k, neighbour key l).
+    // Coefficients of code (sign, generator i) and own character ch: own rows
+    // k = 0, 1 (the first two keys of ch's block), neighbour slots l = 0, 1,
+    // at int32 number 2 k + l of the entry.
     auto put = [&](std::vector<int32_t>& blob, int i, int ch, int k, int l, uint32_t mu) {
         const int32_t b = balanced_of(mu, mod);
-        for (int neg = 0; neg < 2; ++neg) {
-            const int32_t v = neg ? -b : b;
-            uint32_t& word = reinterpret_cast<uint32_t&>(blob[2 * ((neg * n + i) * r + ch) + k]);
-            word |= (static_cast<uint32_t>(v) & 0xFFFFu) << (16 * l);
-        }
+        for (int neg = 0; neg < 2; ++neg) blob[4 * ((neg * n + i) * r + ch) + 2 * k + l] = neg ? -b : b;
     };
     std::vector<int32_t> blob_f = common, blob_t = common;
     for (int i = 0; i < n; ++i)
@@ -590,12 +602,18 @@ void CyclicCtx::setup_subset_path() {
     int l2 = 0;
     BW_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
     stream_tables = table_bytes > static_cast<size_t>(l2) / 2;
-    d_xs16 = alloc<uint4>(D.n0);
+    // Gathered vectors carry one more block, all zero, for the empty slots of
+    // a partial chunk of incidences (their words point at it).
+    d_xs16 = alloc<uint4>(D.n0 + 1);
     d_zs = alloc<int32_t>((es.z_cols + dense.columns) * num_v);
-    d_y16 = alloc<uint4>(D.n1);
-    d_t16 = alloc<uint4>(D.n1);
+    d_y16 = alloc<uint4>(D.n1 + 1);
+    d_t16 = alloc<uint4>(D.n1 + 1);
     d_u16 = alloc<uint4>(D.n2);
-    d_u2_16 = alloc<uint4>(D.n2);
+    d_u2_16 = alloc<uint4>(D.n2 + 1);
+    BW_CUDA(cudaMemsetAsync(d_xs16, 0, (D.n0 + 1) * sizeof(uint4), stream));
+    BW_CUDA(cudaMemsetAsync(d_y16, 0, (D.n1 + 1) * sizeof(uint4), stream));
+    BW_CUDA(cudaMemsetAsync(d_t16, 0, (D.n1 + 1) * sizeof(uint4), stream));
+    BW_CUDA(cudaMemsetAsync(d_u2_16, 0, (D.n2 + 1) * sizeof(uint4), stream));
     subset_path = true;
 }
 

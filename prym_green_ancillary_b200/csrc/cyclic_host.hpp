@@ -143,8 +143,8 @@ EliminatedSector assemble_eliminated_sector(const Instance& inst, size_t sector)
 // so a neighbour block is found from its subset rank alone.  One entry per
 // subset of each degree, and one incidence word per (position, subset) laid
 // out [position][subset] so that consecutive subsets read consecutive words.
-// An incidence word is the neighbour subset's rank | i << 26 | (sign
-// negative) << 31; a subset word is the first compact row of one of its
+// An incidence word is the neighbour subset's rank | (i + n * (sign
+// negative)) << 26; a subset word is the first compact row of one of its
 // blocks | its character << 26.
 struct SubsetTables {
     std::vector<uint32_t> m1;   // (m-1)-subsets: z block (compact) | t character

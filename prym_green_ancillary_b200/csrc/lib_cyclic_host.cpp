@@ -858,14 +858,16 @@ std::string build_subset_tables(const Instance& inst, const EliminatedSector& es
     for (size_t s = 0; s < n0; ++s)
         out.m0[s] = es.dm_layout.col_offsets[s] | (sub_mod(es.sector, dm.column_subset_weights[s], inst.r) << 26);
     // incidence words, transposed to [position][subset]
-    auto fill = [](std::vector<uint32_t>& dst, size_t subsets, size_t width, const std::vector<uint32_t>& nb,
+    const uint32_t n = static_cast<uint32_t>(inst.n);
+    auto fill = [n](std::vector<uint32_t>& dst, size_t subsets, size_t width, const std::vector<uint32_t>& nb,
                    const std::vector<uint32_t>& idx, const std::vector<uint8_t>& neg) {
         dst.resize(subsets * width);
         parallel_chunks(subsets, [&](size_t b, size_t e) {
             for (size_t s = b; s < e; ++s)
                 for (size_t pos = 0; pos < width; ++pos) {
                     const size_t q = s * width + pos;
-                    dst[pos * subsets + s] = nb[q] | (idx[q] << 26) | (neg[q] ? 0x80000000u : 0u);
+                    // coefficient code: sign * n + generator (six bits, n <= 32)
+                    dst[pos * subsets + s] = nb[q] | ((idx[q] + (neg[q] ? n : 0u)) << 26);
                 }
         });
     };
