@@ -58,8 +58,9 @@ struct SubsetDev {
     uint32_t w_dmf, w_d2f, w_d2t, w_dmt;   // incidences per subset of each gather
     const uint32_t *m1, *m2, *m0;          // subset words: compact block row | character << 26
     const uint32_t *inc_dmf, *inc_d2f, *inc_d2t, *inc_dmt;
-    const uint32_t *p_ptr, *p_col;         // folded target preconditioner over padded u rows
-    const int16_t* p_val;
+    const uint32_t* e_col;                 // folded target preconditioner, ELL over the padded u rows
+    const int16_t* e_val;
+    uint32_t ell;                          // slots a row (a multiple of four)
     const int32_t *blob_f, *blob_t;
     int blob_words;
     int o_R, o_B, o_a0off, o_a0idx, o_a1off, o_a1idx, o_koff, o_kidx, o_ych;

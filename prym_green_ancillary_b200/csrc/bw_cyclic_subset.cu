@@ -26,8 +26,8 @@
 //     z part of the adjoint assembly (cyclic_elim_RT_h_kernel,
 //     cyclic_elim_BT_h_kernel, cyclic_elim_assemble_adjoint_kernel, :793-895):
 //     h never reaches memory.
-// The folded target preconditioner runs over the padded u rows with int16
-// values.  The operator's inputs and outputs (the block B, S B) stay compact
+// The folded target preconditioner runs over the padded u rows in ELL form
+// with int16 values.  The operator's inputs and outputs (the block B, S B) stay compact
 // int32; results are the same canonical residues as the generic row kernels
 // of bw_cyclic.cu, which remain for instances outside this format.
 #include "bw_cyclic.cuh"
@@ -281,17 +281,47 @@ __global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, c
     }
 }
 
-// u2 = P u over the padded u rows (P = T^t Dr T folded, int16 values; padding
-// rows are empty and come out zero).
+// u2 = P u over the padded u rows for the folded target preconditioner
+// P = T^t Dr T in ELL form ([slot][row], `ell` slots a row, coalesced across
+// threads; empty slots hold value 0).  Four slots at a time: their rows are
+// gathered together, and the next four slots' words are loaded meanwhile.
 template <bool SMALL, bool STREAM>
-__global__ void __launch_bounds__(kThreads) sub_spmv_kernel(SubsetDev D, const uint2* __restrict__ u,
-                                                            uint2* __restrict__ u2) {
-    BW_ITEMS(row, 2 * static_cast<long long>(D.n2)) {
+__global__ void __launch_bounds__(kThreads) sub_ell_kernel(SubsetDev D, const uint2* __restrict__ u,
+                                                           uint2* __restrict__ u2) {
+    const long long rows = 2 * static_cast<long long>(D.n2);
+    BW_ITEMS(row, rows) {
         Acc4<SMALL> acc;
-        const uint32_t e1 = __ldg(D.p_ptr + row + 1);
-        for (uint32_t e = __ldg(D.p_ptr + row); e < e1; ++e) {
-            const uint2 v = __ldg(u + ld_table<STREAM>(D.p_col + e));
-            acc.mac(ld_table<STREAM>(D.p_val + e), unpack_row(v.x, v.y));
+        const uint32_t* c = D.e_col + row;
+        const int16_t* v = D.e_val + row;
+        uint32_t cc[4];
+        int32_t vv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            cc[q] = ld_table<STREAM>(c + q * rows);
+            vv[q] = ld_table<STREAM>(v + q * rows);
+        }
+        for (uint32_t k = 0; k < D.ell; k += 4) {
+            uint2 x[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x[q] = __ldg(u + cc[q]);
+            uint32_t nc[4];
+            int32_t nv[4];
+            if (k + 4 < D.ell) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    nc[q] = ld_table<STREAM>(c + (k + 4 + q) * rows);
+                    nv[q] = ld_table<STREAM>(v + (k + 4 + q) * rows);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc.mac(vv[q], unpack_row(x[q].x, x[q].y));
+            if (k + 4 < D.ell) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    cc[q] = nc[q];
+                    vv[q] = nv[q];
+                }
+            }
         }
         u2[row] = pack_row(acc.reduce(D.mod));
     }
@@ -582,9 +612,9 @@ void CyclicCtx::setup_subset_path() {
     D.inc_d2f = upload(tab.inc_d2f);
     D.inc_d2t = upload(tab.inc_d2t);
     D.inc_dmt = upload(tab.inc_dmt);
-    D.p_ptr = upload(tab.p_ptr);
-    D.p_col = upload(tab.p_col);
-    D.p_val = upload(tab.p_val);
+    D.e_col = upload(tab.e_col);
+    D.e_val = upload(tab.e_val);
+    D.ell = static_cast<uint32_t>(tab.ell);
     D.blob_f = upload(blob_f);
     D.blob_t = upload(blob_t);
     D.x_cols = es.x_cols;
@@ -596,9 +626,8 @@ void CyclicCtx::setup_subset_path() {
     D.dense_sign = E.dense_sign;
     D.dense = E.dense;
     // Tables read once per application: evict-first when they exceed half the L2.
-    const size_t table_bytes = 4 * (tab.inc_dmf.size() + tab.inc_d2f.size() + tab.inc_d2t.size() +
-                                    tab.inc_dmt.size() + tab.p_ptr.size() + tab.p_col.size()) +
-                               2 * tab.p_val.size();
+    size_t table_bytes = 4 * (tab.inc_dmf.size() + tab.inc_d2f.size() + tab.inc_d2t.size() + tab.inc_dmt.size());
+    table_bytes += 4 * tab.e_col.size() + 2 * tab.e_val.size();
     int l2 = 0;
     BW_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
     stream_tables = table_bytes > static_cast<size_t>(l2) / 2;
@@ -648,7 +677,7 @@ void CyclicCtx::subset_precondition16() {
     const uint2* u = reinterpret_cast<const uint2*>(d_u16);
     uint2* u2 = reinterpret_cast<uint2*>(d_u2_16);
     const unsigned grid = grid_for(2 * static_cast<size_t>(S.n2));
-#define BW_LAUNCH(A, B) sub_spmv_kernel<A, B><<<grid, kThreads, 0, stream>>>(S, u, u2)
+#define BW_LAUNCH(A, B) sub_ell_kernel<A, B><<<grid, kThreads, 0, stream>>>(S, u, u2)
     BW_SUBSET_DISPATCH(BW_LAUNCH);
 #undef BW_LAUNCH
     BW_CHECK_LAUNCH();

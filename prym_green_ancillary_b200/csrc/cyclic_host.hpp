@@ -115,6 +115,7 @@ struct Csr {
 Csr composite_target_preconditioner(const RowMixPlan& plan, const std::vector<uint32_t>& row_precond,
                                     uint32_t prime);
 
+
 // ----- file names and sidecar (cuda/cuprym_cyclic.cu:1289-1400)
 std::string rowmix_label(size_t rounds, uint64_t seed);
 std::string sector_filename(const std::string& out_dir, const std::string& op, size_t sector, size_t num_v,
@@ -153,14 +154,18 @@ struct SubsetTables {
     // D_m (row subsets, neighbours T u i), D_(m-1) (neighbours T u i),
     // D_(m-1)^t (neighbours S \ j), D_m^t (neighbours S \ j)
     std::vector<uint32_t> inc_dmf, inc_d2f, inc_d2t, inc_dmt;
-    // the folded target preconditioner over the padded u rows: every compact
-    // row u_off(s) + q becomes 2 s + q (empty padding rows); balanced values
-    std::vector<uint32_t> p_ptr, p_col;
-    std::vector<int16_t> p_val;
+    // the folded target preconditioner over the padded u rows (compact row
+    // u_off(s) + q is 2 s + q) in ELL form: `ell` slots a row (a multiple of
+    // four), laid out [slot][row]; empty slots and padding rows hold column 0
+    // with value 0; balanced values
+    size_t ell = 0;
+    std::vector<uint32_t> e_col;
+    std::vector<int16_t> e_val;
 };
 // Empty string: the tables are built.  Otherwise the reason this sector does
 // not fit the packed format (a character block above two rows, an index or
-// rank beyond its field), and `out` is left empty.
+// rank beyond its field), and `out` is left empty.  `precond` is the folded
+// target preconditioner over the compact target rows.
 std::string build_subset_tables(const Instance& inst, const EliminatedSector& es, const Csr& precond,
                                 SubsetTables& out);
 

@@ -595,15 +595,30 @@ void validate_rowmix_transpose_identity(const RowMixPlan& plan, size_t cols, uin
 }
 
 // P = T^t Dr T with T = T_R ... T_1 (the rounds of generate_rowmix_plan).
-Csr composite_target_preconditioner(const RowMixPlan& plan, const std::vector<uint32_t>& dr, uint32_t prime) {
+namespace {
+// T = T_R ... T_1 of a row-mixing plan, row by row: a round pairs disjoint
+// rows, so every row has at most W = 2^R entries (columns sorted), and its
+// columns (the rows of T^t, rows sorted).
+struct RowMixT {
+    size_t n = 0, W = 1;
+    std::vector<uint32_t> tc, tv;   // row k: columns and values at k * W, tn[k] of them
+    std::vector<uint8_t> tn;
+    std::vector<uint32_t> cptr, crow, cval;   // column i: rows crow and values cval at cptr[i]..cptr[i+1]
+};
+
+RowMixT build_rowmix_t(const RowMixPlan& plan, uint32_t prime) {
+    RowMixT t;
     const size_t n = plan.target_rows;
-    if (dr.size() != n) throw std::runtime_error("row preconditioner length does not match the rowmix plan");
     if (plan.rounds > 6) throw std::runtime_error("at most 6 row-mixing rounds can be folded");
-    // T = T_R ... T_1 row by row: a round pairs disjoint rows, so every row has
-    // at most W = 2^R entries; rows are kept sorted by column.
-    const size_t W = size_t(1) << plan.rounds;
-    std::vector<uint32_t> tc(n * W), tv(n * W);
-    std::vector<uint8_t> tn(n, 1);
+    t.n = n;
+    t.W = size_t(1) << plan.rounds;
+    const size_t W = t.W;
+    auto& tc = t.tc;
+    auto& tv = t.tv;
+    auto& tn = t.tn;
+    tc.resize(n * W);
+    tv.resize(n * W);
+    tn.assign(n, 1);
     for (size_t i = 0; i < n; ++i) {
         tc[i * W] = static_cast<uint32_t>(i);
         tv[i * W] = 1;
@@ -665,6 +680,25 @@ Csr composite_target_preconditioner(const RowMixPlan& plan, const std::vector<ui
                 cval[fill[i]++] = tv[k * W + e];
             }
     }
+    t.cptr = std::move(cptr);
+    t.crow = std::move(crow);
+    t.cval = std::move(cval);
+    return t;
+}
+}  // namespace
+
+Csr composite_target_preconditioner(const RowMixPlan& plan, const std::vector<uint32_t>& dr, uint32_t prime) {
+    const size_t n = plan.target_rows;
+    if (dr.size() != n) throw std::runtime_error("row preconditioner length does not match the rowmix plan");
+    const RowMixT t = build_rowmix_t(plan, prime);
+    const size_t W = t.W;
+    const uint64_t p = prime;
+    const auto& tc = t.tc;
+    const auto& tv = t.tv;
+    const auto& tn = t.tn;
+    const auto& cptr = t.cptr;
+    const auto& crow = t.crow;
+    const auto& cval = t.cval;
     // P[i][j] = sum_k T[k][i] Dr[k] T[k][j]: row i merges the rows k of column i
     const size_t PW = W * W;
     std::vector<uint32_t> pc(n * PW), pv(n * PW);
@@ -883,26 +917,25 @@ std::string build_subset_tables(const Instance& inst, const EliminatedSector& es
     std::vector<uint32_t> compact_of(2 * n2, UINT32_MAX);
     for (size_t q = 0; q < es.target_rows; ++q) compact_of[slot[q]] = static_cast<uint32_t>(q);
     const int32_t p = static_cast<int32_t>(inst.modulus), half = (p - 1) / 2;
-    out.p_ptr.resize(2 * n2 + 1);
-    out.p_ptr[0] = 0;
-    for (size_t pr = 0; pr < 2 * n2; ++pr) {
-        const uint32_t q = compact_of[pr];
-        const size_t len = q == UINT32_MAX ? 0 : precond.row_ptr[q + 1] - precond.row_ptr[q];
-        if (out.p_ptr[pr] + len >= (1ull << 32)) return "preconditioner above 2^32 entries";
-        out.p_ptr[pr + 1] = static_cast<uint32_t>(out.p_ptr[pr] + len);
-    }
-    out.p_col.resize(out.p_ptr[2 * n2]);
-    out.p_val.resize(out.p_ptr[2 * n2]);
-    parallel_chunks(2 * n2, [&](size_t b, size_t e) {
+    size_t widest = 1;
+    for (size_t q = 0; q < es.target_rows; ++q)
+        widest = std::max<size_t>(widest, precond.row_ptr[q + 1] - precond.row_ptr[q]);
+    if (widest > 64) return "preconditioner above 64 entries a row";
+    out.ell = (widest + 3) / 4 * 4;
+    const size_t rows = 2 * n2;
+    if (rows * out.ell >= (1ull << 32)) return "preconditioner above 2^32 slots";
+    out.e_col.assign(rows * out.ell, 0u);
+    out.e_val.assign(rows * out.ell, int16_t{0});
+    parallel_chunks(rows, [&](size_t b, size_t e) {
         for (size_t pr = b; pr < e; ++pr) {
             const uint32_t q = compact_of[pr];
             if (q == UINT32_MAX) continue;
-            uint32_t dst = out.p_ptr[pr];
-            for (uint32_t k = precond.row_ptr[q]; k < precond.row_ptr[q + 1]; ++k, ++dst) {
-                out.p_col[dst] = slot[precond.col[k]];
-                int32_t v = static_cast<int32_t>(precond.val[k] % inst.modulus);
+            size_t k = 0;
+            for (uint32_t x = precond.row_ptr[q]; x < precond.row_ptr[q + 1]; ++x, ++k) {
+                out.e_col[k * rows + pr] = slot[precond.col[x]];
+                int32_t v = static_cast<int32_t>(precond.val[x] % inst.modulus);
                 if (v > half) v -= p;
-                out.p_val[dst] = static_cast<int16_t>(v);
+                out.e_val[k * rows + pr] = static_cast<int16_t>(v);
             }
         }
     });
