@@ -51,7 +51,7 @@ PUBLISHED_PAPER_STEPS_PER_S = {"g20": 13966.0, "g22": 9541.0, "g24": 3301.0, "g2
                                "g30": 38.1}
 # Paper mode (the eliminated cyclic operator of one sector of the shipped instances, block width 4):
 # name -> default timed steps (applications of S; two per round of 4 moments)
-PAPER = {"g20": 2000, "g22": 2000, "g24": 2000, "g26": 800, "g28": 200, "g30": 40}
+PAPER = {"g20": 20000, "g22": 20000, "g24": 8000, "g26": 2000, "g28": 600, "g30": 100}
 
 
 def parse():

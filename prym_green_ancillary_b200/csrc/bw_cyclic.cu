@@ -708,6 +708,7 @@ CyclicCtx* CyclicCtx::open(const std::string& instance_path, const std::string& 
 }
 
 void CyclicCtx::to_balanced(const uint32_t* in, int32_t* out, size_t count) {
+    if (out == xs_for) xs_for = nullptr;
     cyc_to_balanced_kernel<<<grid_for(count), kThreads, 0, stream>>>(in, out, static_cast<long long>(count), mod);
     BW_CHECK_LAUNCH();
     ++launches;
@@ -721,7 +722,8 @@ void CyclicCtx::to_canonical(const int32_t* in, uint32_t* out, size_t count) {
 
 void CyclicCtx::forward(const int32_t* in, int32_t* u, bool precondition) {
     if (subset_path) {
-        subset_forward16(in, precondition ? d_dc : nullptr);
+        subset_source16(in, precondition ? d_dc : nullptr);
+        subset_forward16();
         subset_unpack_u(d_u16, u);
         return;
     }
@@ -745,7 +747,7 @@ void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
     const int32_t* dc = precondition ? d_dc : nullptr;
     if (subset_path) {
         subset_pack_u(u2, d_u2_16);
-        subset_backward16(dc, out);
+        subset_backward16(dc, out, false);
         return;
     }
     const size_t tz = es.t_rows + es.z_cols;
@@ -786,9 +788,10 @@ void CyclicCtx::target_precondition(const int32_t* u, int32_t* u2) {
 
 void CyclicCtx::apply_square(const int32_t* in, int32_t* out) {
     if (subset_path) {   // padded int16 internals end to end
-        subset_forward16(in, d_dc);
+        if (xs_for != in) subset_source16(in, d_dc);   // else the previous backward wrote it
+        subset_forward16();
         subset_precondition16();
-        subset_backward16(d_dc, out);
+        subset_backward16(d_dc, out, true);
         return;
     }
     forward(in, d_u, true);
@@ -835,6 +838,9 @@ void CyclicCtx::generate(size_t nlen_target, float* device_ms) {
     BW_CUDA(cudaMemcpyAsync(tmp, initial_block.data(), nc * num_v * 4, cudaMemcpyHostToDevice, stream));
     to_balanced(tmp, d_b, nc * num_v);
     gram(d_b, d_b, nullptr, nullptr, 1);
+    // the first application's source, outside the round graph: every later
+    // source is written by the backward kernels of the application before
+    if (subset_path && rounds > 0) subset_source16(d_b, d_dc);
     if (rounds > 0) {
         if (!graphs[0]) {
             const uint64_t l0 = launches;

@@ -119,6 +119,11 @@ struct CyclicCtx {
     SubsetDev S{};
     uint4 *d_xs16 = nullptr, *d_y16 = nullptr, *d_t16 = nullptr, *d_u16 = nullptr, *d_u2_16 = nullptr;
     int32_t* d_zs = nullptr;     // compact z rows and extra columns of the scaled source
+    // The buffer X for which d_xs16 / d_zs hold d_dc (.) X (nullptr: none):
+    // apply_square's backward kernels write the next application's source
+    // from its output, so a sequence runs the source kernel only once.  Any
+    // other write to X clears it (to_balanced, the compact entry points).
+    const int32_t* xs_for = nullptr;
     uint64_t max_terms = 0;      // most products summed into one output by any kernel
     uint32_t* d_canon = nullptr;
     unsigned gram_grid = 1, dense_grid = 1;
@@ -152,9 +157,10 @@ struct CyclicCtx {
     void forward(const int32_t* in, int32_t* u, bool precondition);
     // subset-major path (bw_cyclic_subset.cu): in -> d_u16, d_u16 -> d_u2_16, d_u2_16 -> out
     void setup_subset_path();
-    void subset_forward16(const int32_t* in, const int32_t* dc);
+    void subset_source16(const int32_t* in, const int32_t* dc);   // d_xs16 / d_zs = dc (.) in
+    void subset_forward16();                                        // d_xs16 / d_zs -> d_u16
     void subset_precondition16();
-    void subset_backward16(const int32_t* dc, int32_t* out);
+    void subset_backward16(const int32_t* dc, int32_t* out, bool next_source);
     void subset_pack_u(const int32_t* u32, uint4* u16);
     void subset_unpack_u(const uint4* u16, int32_t* u32);
     void target_precondition(const int32_t* u, int32_t* u2);

@@ -330,12 +330,15 @@ __global__ void __launch_bounds__(kThreads) sub_ell_kernel(SubsetDev D, const ui
 // (m-1)-subset S: its h rows h(S, a) = (D_(m-1)^t u2)(S, a), then
 //   t_adj(S, beta) = sum_a R[a,beta] h(S, a)               (padded t block)
 //   out_z(S, kappa) = dc * sum_a B[a,kappa] h(S, a)        (compact, through op_col)
+// and, with next_zs, the next application's source row dc * out_z (zero for
+// a dropped column), so that apply_square needs no source kernel.
 template <bool SMALL, bool STREAM>
 __global__ void __launch_bounds__(kThreads) sub_d2_transpose_adjoint_kernel(SubsetDev D,
                                                                             const uint4* __restrict__ u2,
                                                                             const int32_t* __restrict__ dc,
                                                                             uint4* __restrict__ t_adj,
-                                                                            int32_t* __restrict__ out) {
+                                                                            int32_t* __restrict__ out,
+                                                                            int32_t* __restrict__ next_zs) {
     extern __shared__ int32_t sm[];
     const Tables T = stage(D, D.blob_t, sm);
     BW_ITEMS(item, D.n1) {
@@ -362,25 +365,33 @@ __global__ void __launch_bounds__(kThreads) sub_d2_transpose_adjoint_kernel(Subs
         }
         st_block(t_adj, s, tv[0], tv[1]);
         const int kb = T.koff[ych], nz = T.koff[ych + 1] - kb;
-        const long long zfirst = static_cast<long long>(D.x_cols) + (d & kLow26);
+        const long long zq0 = d & kLow26, zfirst = static_cast<long long>(D.x_cols) + zq0;
         for (int q = 0; q < nz; ++q) {
             const long long orow = cyc::op_col(D.drop0, D.drop1, zfirst + q);
-            if (orow < 0) continue;   // dropped base column (replacement)
+            if (orow < 0) {   // dropped base column (replacement)
+                if (next_zs) st4(next_zs, zq0 + q, make_int4(0, 0, 0, 0));
+                continue;
+            }
             const int kap = T.kidx[kb + q];
             Acc4<SMALL> acc;
             if (ny > 0) acc.mac(T.B[a0 * D.kdim + kap], h0);
             if (ny > 1) acc.mac(T.B[a1 * D.kdim + kap], h1);
             const int4 v = acc.reduce(D.mod);
-            st4(out, orow, dc ? scale4(v, __ldg(dc + orow), D.mod) : v);
+            const int4 o = dc ? scale4(v, __ldg(dc + orow), D.mod) : v;
+            st4(out, orow, o);
+            if (next_zs) st4(next_zs, zq0 + q, scale4(o, __ldg(dc + orow), D.mod));   // next source row
         }
     }
 }
 
-// m-subset S': its x rows out_x(S', a) = -dc * (D_m^t t_adj)(S', a), compact through op_col.
+// m-subset S': its x rows out_x(S', a) = -dc * (D_m^t t_adj)(S', a), compact
+// through op_col, and, with next_xs, the next application's padded source
+// block dc * out_x (as the source kernel would build it from out).
 template <bool SMALL, bool STREAM>
 __global__ void __launch_bounds__(kThreads) sub_dm_transpose_kernel(SubsetDev D, const uint4* __restrict__ t_adj,
                                                                     const int32_t* __restrict__ dc,
-                                                                    int32_t* __restrict__ out) {
+                                                                    int32_t* __restrict__ out,
+                                                                    uint4* __restrict__ next_xs) {
     extern __shared__ int32_t sm[];
     const Tables T = stage(D, D.blob_t, sm);
     BW_ITEMS(item, D.n0) {
@@ -392,24 +403,32 @@ __global__ void __launch_bounds__(kThreads) sub_dm_transpose_kernel(SubsetDev D,
         Acc4<SMALL> acc0, acc1;
         gather_block<SMALL, STREAM>(D.inc_dmt, D.n0, s, D.w_dmt, T.coef, D.r, xch, t_adj, D.n1, acc0, acc1);
         const long long xrow = d & kLow26;
-        for (int q = 0; q < nx; ++q) {
+        int4 nxt[2] = {make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0)};
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (q >= nx) break;
             const long long orow = cyc::op_col(D.drop0, D.drop1, xrow + q);
-            if (orow < 0) continue;   // dropped base column (replacement)
+            if (orow < 0) continue;   // dropped base column (replacement): its source slot stays zero
             const int4 v = neg4(q == 0 ? acc0.reduce(D.mod) : acc1.reduce(D.mod));
-            st4(out, orow, dc ? scale4(v, __ldg(dc + orow), D.mod) : v);
+            const int4 o = dc ? scale4(v, __ldg(dc + orow), D.mod) : v;
+            st4(out, orow, o);
+            if (next_xs) nxt[q] = scale4(o, __ldg(dc + orow), D.mod);
         }
+        if (next_xs) st_block(next_xs, s, nxt[0], nxt[1]);   // next application's source block
     }
 }
 
 // Extra source rows of the deformation transpose from the padded u2:
 //   out[kept_cols + j][c] = dense_sign * dc[kept_cols + j] * sum_row dense[row][j] u2[row][c]
 // Each CTA sums a stripe of padded rows; the CTA sums meet in an 8-entry
-// accumulator (cyc::grid_sum) and the last CTA writes the n_extra rows.
+// accumulator (cyc::grid_sum) and the last CTA writes the n_extra rows (and,
+// with next_zs, their next source rows).
 __global__ void __launch_bounds__(kThreads) sub_dense_t_kernel(SubsetDev D, const uint2* __restrict__ u2,
                                                                const int32_t* __restrict__ dc,
                                                                int32_t* __restrict__ out,
                                                                int32_t* __restrict__ partials,
-                                                               unsigned int* __restrict__ counter) {
+                                                               unsigned int* __restrict__ counter,
+                                                               int32_t* __restrict__ next_zs) {
     extern __shared__ int32_t sm[];
     const Tables T = stage(D, D.blob_f, sm);
     int32_t acc[8];
@@ -459,6 +478,8 @@ __global__ void __launch_bounds__(kThreads) sub_dense_t_kernel(SubsetDev D, cons
         int32_t v = D.dense_sign * reduce_balanced(total, D.mod);
         if (dc) v = reduce_balanced(v * __ldg(dc + orow), D.mod);
         out[orow * 4 + c] = v;
+        if (next_zs)   // next application's source row of extra column j
+            next_zs[(static_cast<long long>(D.z_cols) + j) * 4 + c] = reduce_balanced(v * __ldg(dc + orow), D.mod);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -660,17 +681,24 @@ void CyclicCtx::setup_subset_path() {
         }                               \
     } while (0)
 
-void CyclicCtx::subset_forward16(const int32_t* in, const int32_t* dc) {
+void CyclicCtx::subset_source16(const int32_t* in, const int32_t* dc) {
     const size_t smem = static_cast<size_t>(S.blob_words) * 4;
     const size_t items = static_cast<size_t>(S.n0) + es.z_cols + dense.columns;
     sub_source_kernel<<<grid_for(items), kThreads, smem, stream>>>(S, in, dc, d_xs16, d_zs);
+    BW_CHECK_LAUNCH();
+    ++launches;
+    xs_for = dc == d_dc ? in : nullptr;
+}
+
+void CyclicCtx::subset_forward16() {
+    const size_t smem = static_cast<size_t>(S.blob_words) * 4;
 #define BW_LAUNCH(A, B)                                                                                      \
     sub_dm_forward_elim_kernel<A, B><<<grid_for(S.n1), kThreads, smem, stream>>>(S, d_xs16, d_zs, d_y16); \
     sub_d2_forward_kernel<A, B><<<grid_for(S.n2), kThreads, smem, stream>>>(S, d_y16, d_zs, d_u16)
     BW_SUBSET_DISPATCH(BW_LAUNCH);
 #undef BW_LAUNCH
     BW_CHECK_LAUNCH();
-    launches += 3;
+    launches += 2;
 }
 
 void CyclicCtx::subset_precondition16() {
@@ -684,21 +712,30 @@ void CyclicCtx::subset_precondition16() {
     ++launches;
 }
 
-void CyclicCtx::subset_backward16(const int32_t* dc, int32_t* out) {
+void CyclicCtx::subset_backward16(const int32_t* dc, int32_t* out, bool next_source) {
     const size_t smem = static_cast<size_t>(S.blob_words) * 4;
-#define BW_LAUNCH(A, B)                                                                                         \
-    sub_d2_transpose_adjoint_kernel<A, B><<<grid_for(S.n1), kThreads, smem, stream>>>(S, d_u2_16, dc, d_t16, out); \
-    sub_dm_transpose_kernel<A, B><<<grid_for(S.n0), kThreads, smem, stream>>>(S, d_t16, dc, out)
+    // next_source (apply_square, dc = the column preconditioner): the kernels
+    // also write the next application's source from `out`
+    uint4* nxs = next_source ? d_xs16 : nullptr;
+    int32_t* nzs = next_source ? d_zs : nullptr;
+#define BW_LAUNCH(A, B)                                                                                           \
+    sub_d2_transpose_adjoint_kernel<A, B><<<grid_for(S.n1), kThreads, smem, stream>>>(S, d_u2_16, dc, d_t16, out, \
+                                                                                     nzs);                        \
+    sub_dm_transpose_kernel<A, B><<<grid_for(S.n0), kThreads, smem, stream>>>(S, d_t16, dc, out, nxs)
     BW_SUBSET_DISPATCH(BW_LAUNCH);
 #undef BW_LAUNCH
     BW_CHECK_LAUNCH();
     launches += 2;
     if (S.n_extra) {
         sub_dense_t_kernel<<<dense_grid, kThreads, smem, stream>>>(S, reinterpret_cast<const uint2*>(d_u2_16), dc,
-                                                                   out, d_dpart, d_dcounter);
+                                                                   out, d_dpart, d_dcounter, nzs);
         BW_CHECK_LAUNCH();
         ++launches;
     }
+    if (next_source)
+        xs_for = out;
+    else if (xs_for == out)
+        xs_for = nullptr;
 }
 
 void CyclicCtx::subset_pack_u(const int32_t* u32, uint4* u16) {
