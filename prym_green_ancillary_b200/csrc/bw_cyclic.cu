@@ -724,7 +724,7 @@ void CyclicCtx::forward(const int32_t* in, int32_t* u, bool precondition) {
     if (subset_path) {
         subset_source16(in, precondition ? d_dc : nullptr);
         subset_forward16();
-        subset_unpack_u(d_u16, u);
+        subset_u_from_walk(u);
         return;
     }
     cyc_source_kernel<<<grid_for(base_cols + dense.columns), kThreads, 0, stream>>>(E, in, precondition ? d_dc : nullptr,
@@ -771,7 +771,7 @@ void CyclicCtx::backward(const int32_t* u2, int32_t* out, bool precondition) {
 
 void CyclicCtx::target_precondition(const int32_t* u, int32_t* u2) {
     if (subset_path) {
-        subset_pack_u(u, d_u16);
+        subset_u_to_walk(u);
         subset_precondition16();
         subset_unpack_u(d_u2_16, u2);
         return;

@@ -58,7 +58,8 @@ struct SubsetDev {
     uint32_t w_dmf, w_d2f, w_d2t, w_dmt;   // incidences per subset of each gather
     const uint32_t *m1, *m2, *m0;          // subset words: compact block row | character << 26
     const uint32_t *inc_dmf, *inc_d2f, *inc_d2t, *inc_dmt;
-    const uint32_t* e_col;                 // folded target preconditioner, ELL over the padded u rows
+    const uint32_t* u_pos;                 // compact u row -> its position in u (row-mixing locality order)
+    const uint32_t* e_col;                 // folded target preconditioner, ELL (rows: padded u2 slots; columns: u positions)
     const int16_t* e_val;
     uint32_t ell;                          // slots a row (a multiple of four)
     const int32_t *blob_f, *blob_t;
@@ -161,8 +162,10 @@ struct CyclicCtx {
     void subset_forward16();                                        // d_xs16 / d_zs -> d_u16
     void subset_precondition16();
     void subset_backward16(const int32_t* dc, int32_t* out, bool next_source);
-    void subset_pack_u(const int32_t* u32, uint4* u16);
+    void subset_pack_u(const int32_t* u32, uint4* u16);       // compact -> padded (u2)
     void subset_unpack_u(const uint4* u16, int32_t* u32);
+    void subset_u_to_walk(const int32_t* u32);                 // compact -> d_u16 in locality order
+    void subset_u_from_walk(int32_t* u32);
     void target_precondition(const int32_t* u, int32_t* u2);
     void backward(const int32_t* u2, int32_t* out, bool precondition);
     void apply_square(const int32_t* in, int32_t* out);

@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kThreads) sub_dm_forward_elim_kernel(SubsetDev
 template <bool SMALL, bool STREAM>
 __global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, const uint4* __restrict__ y,
                                                                   const int32_t* __restrict__ zs,
-                                                                  uint4* __restrict__ u) {
+                                                                  uint2* __restrict__ u) {
     extern __shared__ int32_t sm[];
     const Tables T = stage(D, D.blob_f, sm);
     BW_ITEMS(item, D.n2) {
@@ -252,6 +252,7 @@ __global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, c
         const uint32_t d = __ldg(D.m2 + s);
         const int uch = static_cast<int>(d >> 26);
         const int nu = T.a1off[uch + 1] - T.a1off[uch];
+        const long long urow = d & kLow26;
         int4 out[2] = {make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0)};
         if (nu > 0) {
             Acc4<SMALL> acc0, acc1;
@@ -259,7 +260,6 @@ __global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, c
             out[0] = acc0.reduce(D.mod);
             if (nu > 1) out[1] = acc1.reduce(D.mod);
             if (D.n_extra) {
-                const long long urow = d & kLow26;
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     if (q >= nu) break;
@@ -277,7 +277,10 @@ __global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, c
                 }
             }
         }
-        st_block(u, s, out[0], out[1]);
+        // rows to their positions in the row-mixing locality order
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (q < nu) u[__ldg(D.u_pos + urow + q)] = pack_row(out[q]);
     }
 }
 
@@ -519,6 +522,19 @@ __global__ void __launch_bounds__(kThreads) sub_u_unpack_kernel(SubsetDev D, con
     }
 }
 
+// Compact int32 u rows <-> u in the row-mixing locality order (int16 rows).
+__global__ void __launch_bounds__(kThreads) sub_u_to_walk_kernel(SubsetDev D, const int32_t* __restrict__ u32,
+                                                                 uint2* __restrict__ u, long long rows) {
+    BW_ITEMS(q, rows) u[__ldg(D.u_pos + q)] = pack_row(ld4(u32, q));
+}
+__global__ void __launch_bounds__(kThreads) sub_u_from_walk_kernel(SubsetDev D, const uint2* __restrict__ u,
+                                                                   int32_t* __restrict__ u32, long long rows) {
+    BW_ITEMS(q, rows) {
+        const uint2 w = __ldg(u + __ldg(D.u_pos + q));
+        st4(u32, q, unpack_row(w.x, w.y));
+    }
+}
+
 int32_t balanced_of(uint32_t v, const Mod& m) { return to_balanced(v % static_cast<uint32_t>(m.p), m); }
 
 }  // namespace
@@ -536,7 +552,10 @@ void CyclicCtx::setup_subset_path() {
         }
     }
     cyclic::SubsetTables tab;
-    subset_reason = cyclic::build_subset_tables(inst, es, precond, tab);
+    // u is kept in an order with row-mixing partners adjacent, so the folded
+    // preconditioner's sixteen columns of a row fall within a few sectors
+    const std::vector<uint32_t> u_pos = cyclic::rowmix_locality_order(plan);
+    subset_reason = cyclic::build_subset_tables(inst, es, precond, u_pos, tab);
     if (!subset_reason.empty()) return;
 
     const cyclic::CharMap a0 = cyclic::build_char_map(inst.weight_a0, inst.r);
@@ -633,6 +652,7 @@ void CyclicCtx::setup_subset_path() {
     D.inc_d2f = upload(tab.inc_d2f);
     D.inc_d2t = upload(tab.inc_d2t);
     D.inc_dmt = upload(tab.inc_dmt);
+    D.u_pos = upload(u_pos);
     D.e_col = upload(tab.e_col);
     D.e_val = upload(tab.e_val);
     D.ell = static_cast<uint32_t>(tab.ell);
@@ -658,7 +678,7 @@ void CyclicCtx::setup_subset_path() {
     d_zs = alloc<int32_t>((es.z_cols + dense.columns) * num_v);
     d_y16 = alloc<uint4>(D.n1 + 1);
     d_t16 = alloc<uint4>(D.n1 + 1);
-    d_u16 = alloc<uint4>(D.n2);
+    d_u16 = alloc<uint4>((es.target_rows + 1) / 2 + 1);   // u rows (int16) in the locality order
     d_u2_16 = alloc<uint4>(D.n2 + 1);
     BW_CUDA(cudaMemsetAsync(d_xs16, 0, (D.n0 + 1) * sizeof(uint4), stream));
     BW_CUDA(cudaMemsetAsync(d_y16, 0, (D.n1 + 1) * sizeof(uint4), stream));
@@ -694,7 +714,8 @@ void CyclicCtx::subset_forward16() {
     const size_t smem = static_cast<size_t>(S.blob_words) * 4;
 #define BW_LAUNCH(A, B)                                                                                      \
     sub_dm_forward_elim_kernel<A, B><<<grid_for(S.n1), kThreads, smem, stream>>>(S, d_xs16, d_zs, d_y16); \
-    sub_d2_forward_kernel<A, B><<<grid_for(S.n2), kThreads, smem, stream>>>(S, d_y16, d_zs, d_u16)
+    sub_d2_forward_kernel<A, B><<<grid_for(S.n2), kThreads, smem, stream>>>(S, d_y16, d_zs,               \
+                                                                             reinterpret_cast<uint2*>(d_u16))
     BW_SUBSET_DISPATCH(BW_LAUNCH);
 #undef BW_LAUNCH
     BW_CHECK_LAUNCH();
@@ -736,6 +757,22 @@ void CyclicCtx::subset_backward16(const int32_t* dc, int32_t* out, bool next_sou
         xs_for = out;
     else if (xs_for == out)
         xs_for = nullptr;
+}
+
+void CyclicCtx::subset_u_to_walk(const int32_t* u32) {
+    const long long rows = static_cast<long long>(es.target_rows);
+    sub_u_to_walk_kernel<<<grid_for(es.target_rows), kThreads, 0, stream>>>(S, u32, reinterpret_cast<uint2*>(d_u16),
+                                                                            rows);
+    BW_CHECK_LAUNCH();
+    ++launches;
+}
+
+void CyclicCtx::subset_u_from_walk(int32_t* u32) {
+    const long long rows = static_cast<long long>(es.target_rows);
+    sub_u_from_walk_kernel<<<grid_for(es.target_rows), kThreads, 0, stream>>>(
+        S, reinterpret_cast<const uint2*>(d_u16), u32, rows);
+    BW_CHECK_LAUNCH();
+    ++launches;
 }
 
 void CyclicCtx::subset_pack_u(const int32_t* u32, uint4* u16) {

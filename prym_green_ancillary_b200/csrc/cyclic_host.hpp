@@ -154,10 +154,11 @@ struct SubsetTables {
     // D_m (row subsets, neighbours T u i), D_(m-1) (neighbours T u i),
     // D_(m-1)^t (neighbours S \ j), D_m^t (neighbours S \ j)
     std::vector<uint32_t> inc_dmf, inc_d2f, inc_d2t, inc_dmt;
-    // the folded target preconditioner over the padded u rows (compact row
-    // u_off(s) + q is 2 s + q) in ELL form: `ell` slots a row (a multiple of
-    // four), laid out [slot][row]; empty slots and padding rows hold column 0
-    // with value 0; balanced values
+    // the folded target preconditioner in ELL form: rows are the padded u
+    // slots (compact row u_off(s) + q is 2 s + q; they write u2), columns are
+    // positions of u in the row-mixing locality order; `ell` slots a row (a
+    // multiple of four), laid out [slot][row]; empty slots and padding rows
+    // hold column 0 with value 0; balanced values
     size_t ell = 0;
     std::vector<uint32_t> e_col;
     std::vector<int16_t> e_val;
@@ -165,9 +166,12 @@ struct SubsetTables {
 // Empty string: the tables are built.  Otherwise the reason this sector does
 // not fit the packed format (a character block above two rows, an index or
 // rank beyond its field), and `out` is left empty.  `precond` is the folded
-// target preconditioner over the compact target rows.
+// target preconditioner over the compact target rows; its columns index u in
+// the order u_pos (compact row -> position).
 std::string build_subset_tables(const Instance& inst, const EliminatedSector& es, const Csr& precond,
-                                SubsetTables& out);
+                                const std::vector<uint32_t>& u_pos, SubsetTables& out);
+// Row order with row-mixing partners adjacent (pos[row]); see lib_cyclic_host.cpp.
+std::vector<uint32_t> rowmix_locality_order(const RowMixPlan& plan);
 
 // ----- deformation inputs (cuda/cuprym_deformation.cu:426-473)
 // Both files are read the way the reference reads them: a key is its first

@@ -863,9 +863,49 @@ EliminatedSector assemble_eliminated_sector(const Instance& inst, size_t sector)
     return es;
 }
 
+// A row order in which row-mixing partners sit next to each other.  Every
+// round pairs disjoint rows, so each row has at most one partner a round; with
+// two rounds the partner graph is a set of paths and cycles that alternate
+// between the rounds.  Walking each path (from an end) and then each cycle
+// puts both partners of a row beside it, so a row of T^t Dr T (its rows
+// within two partner steps on either side) lies within seven consecutive
+// positions.  Returns pos[row].
+std::vector<uint32_t> rowmix_locality_order(const RowMixPlan& plan) {
+    const size_t n = plan.target_rows, R = plan.rounds;
+    std::vector<uint32_t> partner(n * std::max<size_t>(R, 1), UINT32_MAX);
+    for (size_t r = 0; r < R; ++r)
+        for (const auto& pr : plan.round_pairs[r]) {
+            partner[pr.first * R + r] = pr.second;
+            partner[pr.second * R + r] = pr.first;
+        }
+    std::vector<uint32_t> pos(n, UINT32_MAX);
+    uint32_t next = 0;
+    auto walk = [&](size_t v) {
+        size_t cur = v;
+        while (cur != SIZE_MAX) {
+            pos[cur] = next++;
+            size_t nb = SIZE_MAX;
+            for (size_t r = 0; r < R && nb == SIZE_MAX; ++r) {
+                const uint32_t w = partner[cur * R + r];
+                if (w != UINT32_MAX && pos[w] == UINT32_MAX) nb = w;
+            }
+            cur = nb;
+        }
+    };
+    for (size_t v = 0; v < n; ++v) {   // path ends (fewer than R partners) first
+        if (pos[v] != UINT32_MAX) continue;
+        size_t degree = 0;
+        for (size_t r = 0; r < R; ++r) degree += partner[v * R + r] != UINT32_MAX;
+        if (degree < R) walk(v);
+    }
+    for (size_t v = 0; v < n; ++v)   // then the cycles
+        if (pos[v] == UINT32_MAX) walk(v);
+    return pos;
+}
+
 // Subset-major gather tables (the device side is bw_cyclic_subset.cu).
 std::string build_subset_tables(const Instance& inst, const EliminatedSector& es, const Csr& precond,
-                                SubsetTables& out) {
+                                const std::vector<uint32_t>& u_pos, SubsetTables& out) {
     out = SubsetTables{};
     const CharMap a0 = build_char_map(inst.weight_a0, inst.r);
     const CharMap a1 = build_char_map(inst.weight_a1, inst.r);
@@ -882,6 +922,7 @@ std::string build_subset_tables(const Instance& inst, const EliminatedSector& es
         return "2^26 subsets or rows or more";
     if (d2.column_subsets != n1) return "inconsistent subset counts";
     if (precond.row_ptr.size() != es.target_rows + 1) return "preconditioner size does not match the sector";
+    if (u_pos.size() != es.target_rows) return "u order size does not match the sector";
     out.m1.resize(n1);
     out.m2.resize(n2);
     out.m0.resize(n0);
@@ -932,7 +973,7 @@ std::string build_subset_tables(const Instance& inst, const EliminatedSector& es
             if (q == UINT32_MAX) continue;
             size_t k = 0;
             for (uint32_t x = precond.row_ptr[q]; x < precond.row_ptr[q + 1]; ++x, ++k) {
-                out.e_col[k * rows + pr] = slot[precond.col[x]];
+                out.e_col[k * rows + pr] = u_pos[precond.col[x]];
                 int32_t v = static_cast<int32_t>(precond.val[x] % inst.modulus);
                 if (v > half) v -= p;
                 out.e_val[k * rows + pr] = static_cast<int16_t>(v);
