@@ -26,10 +26,13 @@
 //     z part of the adjoint assembly (cyclic_elim_RT_h_kernel,
 //     cyclic_elim_BT_h_kernel, cyclic_elim_assemble_adjoint_kernel, :793-895):
 //     h never reaches memory.
-// The folded target preconditioner runs over the padded u rows in ELL form
-// with int16 values.  The operator's inputs and outputs (the block B, S B) stay compact
-// int32; results are the same canonical residues as the generic row kernels
-// of bw_cyclic.cu, which remain for instances outside this format.
+// The folded target preconditioner runs in ELL form with int16 values; it
+// reads u kept in an order with row-mixing partners adjacent (so a row's
+// sixteen columns lie within nine consecutive rows) and writes u2 in the
+// padded subset layout.  The operator's inputs and outputs (the block B,
+// S B) stay compact int32; results are the same canonical residues as the
+// generic row kernels of bw_cyclic.cu, which remain for instances outside
+// this format.
 #include "bw_cyclic.cuh"
 #include "bw_cyclic_dev.cuh"
 
@@ -238,9 +241,10 @@ __global__ void __launch_bounds__(kThreads) sub_dm_forward_elim_kernel(SubsetDev
     }
 }
 
-// (m-2)-subset S2: its u block u(S2, beta) = (D_(m-1) y)(S2, beta), plus
+// (m-2)-subset S2: its u rows u(S2, beta) = (D_(m-1) y)(S2, beta), plus
 // dense_sign * dense zs_extra for the deformation variants (|terms| stay below
-// 2^31: a balanced residue plus two products of balanced residues).
+// 2^31: a balanced residue plus two products of balanced residues), each
+// written to its position u_pos in the row-mixing locality order.
 template <bool SMALL, bool STREAM>
 __global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, const uint4* __restrict__ y,
                                                                   const int32_t* __restrict__ zs,
@@ -284,9 +288,10 @@ __global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, c
     }
 }
 
-// u2 = P u over the padded u rows for the folded target preconditioner
-// P = T^t Dr T in ELL form ([slot][row], `ell` slots a row, coalesced across
-// threads; empty slots hold value 0).  Four slots at a time: their rows are
+// u2 = P u for the folded target preconditioner P = T^t Dr T in ELL form
+// ([slot][row] over the padded u2 slots, `ell` slots a row, coalesced across
+// threads; columns are positions of u in the locality order; empty slots hold
+// value 0).  Four slots at a time: their rows are
 // gathered together, and the next four slots' words are loaded meanwhile.
 template <bool SMALL, bool STREAM>
 __global__ void __launch_bounds__(kThreads) sub_ell_kernel(SubsetDev D, const uint2* __restrict__ u,
@@ -491,8 +496,8 @@ __global__ void __launch_bounds__(kThreads) sub_dense_t_kernel(SubsetDev D, cons
     }
 }
 
-// Compact int32 u rows <-> padded int16 u blocks (the non-hot entry points:
-// forward / target_precondition / backward on compact vectors).
+// Compact int32 rows <-> padded int16 blocks of the (m-2)-subsets: u2 in the
+// non-hot entry points (backward / target_precondition on compact vectors).
 __global__ void __launch_bounds__(kThreads) sub_u_pack_kernel(SubsetDev D, const int32_t* __restrict__ u32,
                                                               uint4* __restrict__ u16) {
     extern __shared__ int32_t sm[];
