@@ -237,12 +237,15 @@ BW_API int bw_cyclic_validate(bw_cyclic* ctx, uint32_t columns);
 
 BW_API uint64_t bw_cyclic_launch_count(const bw_cyclic* ctx);
 
-/* Which gather kernels the context runs: "subset" (one thread per subset,
- * every character block at most two rows: all shipped instances) or
- * "generic: <reason>" (one thread per row).  Setting BW_CYCLIC_GENERIC=1 in
- * the environment before bw_cyclic_open selects the generic kernels.  Both
- * give the same residues.  No reference counterpart (the reference has the
- * row kernels only, cuda/cyclic_cuda_helpers.h:145-266). */
+/* Which gather kernels the context runs: "subset: tables cached" or
+ * "subset: tables evict-first" (one thread per subset, every character block
+ * at most two rows: all shipped instances; the incidence tables are read
+ * evict-first when they exceed half the L2) or "generic: <reason>" (one
+ * thread per row).  Setting BW_CYCLIC_GENERIC=1 in the environment before
+ * bw_cyclic_open selects the generic kernels; BW_CYCLIC_STREAM_TABLES=1 (=0)
+ * forces the evict-first (cached) table reads at any size.  All give the same
+ * residues.  No reference counterpart (the reference has the row kernels
+ * only, cuda/cyclic_cuda_helpers.h:145-266). */
 BW_API int bw_cyclic_gather_path(const bw_cyclic* ctx, char* buf, size_t cap);
 
 /* Kernel-vector recovery (replaces cuda/cuprym_cyclic_kernel_vectors.cu,

@@ -202,7 +202,8 @@ extern "C" int bw_cyclic_gather_path(const bw_cyclic* ctx, char* buf, size_t cap
         BW_REQUIRE(ctx && buf && cap > 0, "bw_cyclic_gather_path: null argument");
         const CyclicCtx& c = *ctx->impl;
         const std::string path = c.host_only ? std::string("none: host-only context")
-                                 : c.subset_path ? std::string("subset")
+                                 : c.subset_path ? std::string(c.stream_tables ? "subset: tables evict-first"
+                                                                               : "subset: tables cached")
                                                  : "generic: " + c.subset_reason;
         BW_REQUIRE(path.size() < cap, "bw_cyclic_gather_path: buffer too small");
         std::memcpy(buf, path.c_str(), path.size() + 1);

@@ -677,6 +677,11 @@ void CyclicCtx::setup_subset_path() {
     int l2 = 0;
     BW_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
     stream_tables = table_bytes > static_cast<size_t>(l2) / 2;
+    // BW_CYCLIC_STREAM_TABLES=1 / =0 forces the evict-first (or the cached)
+    // table reads at any size, so that small sectors run either instantiation.
+    if (const char* env = std::getenv("BW_CYCLIC_STREAM_TABLES")) {
+        if (*env) stream_tables = std::string(env) != "0";
+    }
     // Gathered vectors carry one more block, all zero, for the empty slots of
     // a partial chunk of incidences (their words point at it).
     d_xs16 = alloc<uint4>(D.n0 + 1);

@@ -432,7 +432,8 @@ class CyclicEngine:
 
     @property
     def gather_path(self):
-        """"subset" or "generic: <reason>" (bw_cyclic_gather_path)."""
+        """"subset: tables cached", "subset: tables evict-first" or "generic: <reason>"
+        (bw_cyclic_gather_path)."""
         buf = ctypes.create_string_buffer(256)
         _check(load().bw_cyclic_gather_path(self._h, buf, len(buf)))
         return buf.value.decode()

@@ -32,7 +32,7 @@ def test_reference_arm_line_follows_the_contract(workload):
     assert d["metric"] == bench.METRIC and d["unit"] == "steps/s" and d["higher_is_better"] is True
     assert d["steps"] == 3 and d["warmup"] == 3 and d["n_gpus"] == 1
     assert d["value"] > 0 and d["ms_per_step"] > 0
-    assert d["config"]["workload"] == workload
+    assert d["config"] == bench.workload_config(workload)   # the engine arm prints the same object
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert cb["unit"] == "steps/s" and cb["sample"]

@@ -134,12 +134,61 @@ def test_g12_outputs_identical_to_reference_binary(sector, tmp_path):
     assert int(header[2]) == 661 and int(header[4]) == 4
 
 
-@pytest.mark.parametrize("genus, sector", [(20, 0), (20, 1), (22, 0)])
+# Every base sector of the two campaign genera of the end-to-end drop-in run
+# (scripts/reproduce.py:246-276 runs them all; data/g20.json has 10 sectors,
+# data/g22.json 11), and sector 0 of genus 24.
+PAPER_SECTORS = [(20, s) for s in range(10)] + [(22, s) for s in range(11)] + [(24, 0)]
+
+
+@pytest.mark.parametrize("genus, sector", PAPER_SECTORS)
 def test_paper_outputs_identical_to_reference_binary(genus, sector, tmp_path):
     inst = REF_DATA / f"g{genus}.json"
     if not inst.exists():
         pytest.skip("paper inputs not staged (oracle/build_ref.sh)")
     _compare_with_reference(inst, sector, tmp_path)
+
+
+@pytest.mark.parametrize("instance, sector", [("g12", 0), ("g12", 3), ("g20", 0), ("g20", 1), ("g22", 0)])
+def test_evict_first_tables_identical_to_reference_binary(instance, sector, tmp_path, monkeypatch):
+    """The evict-first instantiation of the subset kernels (chosen by size from
+    genus 26 up) forced at sizes the reference binary runs in seconds."""
+    monkeypatch.setenv("BW_CYCLIC_STREAM_TABLES", "1")
+    monkeypatch.delenv("BW_CYCLIC_GENERIC", raising=False)
+    inst = GOLDEN / "g12_p661.json" if instance == "g12" else REF_DATA / f"{instance}.json"
+    if not inst.exists():
+        pytest.skip("paper inputs not staged (oracle/build_ref.sh)")
+    with CyclicEngine(inst, sector) as eng:
+        assert eng.gather_path == "subset: tables evict-first"
+    _compare_with_reference(inst, sector, tmp_path)
+
+
+@pytest.mark.parametrize("genus", [26, 28])
+def test_large_sector_square_same_on_all_gather_paths(genus, monkeypatch):
+    """Sector 0 of genus 26 and 28 (sizes where the tables are read evict-first
+    by default): three applications of S on the subset-major gathers, with the
+    evict-first and with the cached table reads, equal those of the generic row
+    kernels (which the g12/g20 tests check against explicit blocks and the
+    reference binary)."""
+    inst = REF_DATA / f"g{genus}.json"
+    if not inst.exists():
+        pytest.skip("paper inputs not staged (oracle/build_ref.sh)")
+    runs = {"evict-first": ("0", "1"), "cached": ("0", "0"), "generic": ("1", "")}
+    out = {}
+    for name, (generic, stream) in runs.items():
+        monkeypatch.setenv("BW_CYCLIC_GENERIC", generic)
+        monkeypatch.setenv("BW_CYCLIC_STREAM_TABLES", stream)
+        with CyclicEngine(inst, 0) as eng:
+            path = eng.gather_path
+            assert path.startswith("generic") if name == "generic" else path == f"subset: tables {name}"
+            x = np.random.default_rng(genus).integers(0, eng.info["prime"], (eng.info["cols"], 4), dtype=np.uint32)
+            outs = []
+            for _ in range(3):
+                x = eng.apply(APPLY_SQUARE, x)
+                outs.append(x)
+            out[name] = outs
+    for name in ("evict-first", "cached"):
+        for k in range(3):
+            np.testing.assert_array_equal(out[name][k], out["generic"][k], err_msg=f"{name}, application {k + 1}")
 
 
 def test_paper_square_same_on_both_gather_paths(monkeypatch):
