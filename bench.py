@@ -265,9 +265,83 @@ def run_reference(args):
     return 0
 
 
+REF_BIN_DIR = ROOT / "oracle" / "_ref" / "bin"
+# Paper workloads on which the reference's CUDA build runs its whole sequence
+# loop within a minute on a B200 (longer ones are left out of the default run).
+REF_BINARY_PAPER = {"g20", "g22", "g24"}
+
+
+def paper_instance(name):
+    path = ROOT / "prym_green_ancillary_b200" / "_data" / f"{name}.json"
+    if not path.exists():
+        raise SystemExit(f"{path} missing: build() stages the shipped instances from a reference checkout")
+    return path
+
+
+def cpu_paper(name, sector, budget_s):
+    """The reference's own CPU square operator (cpu_apply_eliminated_square,
+    built from its source by oracle/build_ref.sh) applied repeatedly to the
+    seeded initial block of the sector: at least once, then for budget_s.
+    Returns (applications/s, info dict) or None when the harness is absent."""
+    exe = REF_BIN_DIR / "ref_cpu_square"
+    if not exe.exists():
+        return None
+    res = subprocess.run([str(exe), str(paper_instance(name)), str(sector), str(budget_s)], capture_output=True,
+                         text=True, timeout=1800)
+    if res.returncode != 0:
+        raise SystemExit(f"ref_cpu_square failed: {res.stderr[-500:]}")
+    d = json.loads(res.stdout.strip().splitlines()[-1])
+    return d["applications"] / d["seconds"], d
+
+
+def reference_binary_paper(name, sector):
+    """The reference's CUDA build (oracle/_ref/bin/cuprym_cyclic, the paper
+    recipe) on this GPU: steps/s of its whole sequence loop, from its own
+    "BCW sequence runtime" line and round count (cuda/cuprym_cyclic.cu:2425-2457)."""
+    import re
+    exe = REF_BIN_DIR / "cuprym_cyclic"
+    if not exe.exists():
+        return None
+    with tempfile.TemporaryDirectory() as out:
+        cmd = [str(exe), str(paper_instance(name)), "--operator", "eliminated", "--sector", str(sector), "--out", out,
+               "-v", "4", "--seed", "1", "--rowmix-rounds", "2", "--rowmix-seed", "10001",
+               "--device", os.environ.get("LOCAL_RANK", "0")]
+        t0 = time.perf_counter()
+        res = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+        wall = time.perf_counter() - t0
+    if res.returncode != 0:
+        return {"error": res.stderr[-300:]}
+    rounds = int(re.search(r"Computing (\d+) eliminated BCW rounds", res.stdout).group(1))
+    ms = float(re.search(r"BCW sequence runtime: (\d+) ms", res.stdout).group(1))
+    return {"value": 2 * rounds / (ms / 1e3), "unit": "steps/s", "steps": 2 * rounds, "loop_ms": ms,
+            "process_wall_s": wall,
+            "what": "the reference's own CUDA build (oracle/build_ref.sh, sm_100a), paper recipe, whole sequence "
+                    "loop on this GPU, timed by its own clock around the loop (host wall clock, synchronized)"}
+
+
 def run_reference_paper(args):
-    """Reference arm of a paper workload: not yet available on this path."""
-    line = {"impl": "reference", "unavailable": "paper workloads: reference CPU timing not wired"}
+    """Reference arm of a paper workload: the reference's own CPU square
+    operator on the host (the value), and its CUDA build on this GPU (ref_binary)."""
+    got = cpu_paper(args.workload, args.sector, 10.0)
+    if got is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/bin/ref_cpu_square not built "
+                                                              "(needs the reference checkout at build time)"}))
+        return 0
+    value, d = got
+    sample = (f"{d['applications']} applications of S (cpu_apply_eliminated_square, single-threaded as the "
+              f"reference wrote it) to the seeded initial block in {d['seconds']:.2f} s; Gram moments not included")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": d["applications"], "warmup": 0, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16 storage, u32/u64 accumulate",
+        "data": f"shipped instance {args.workload}.json, seeded preconditioners and block (paper recipe)",
+        "config": {"workload": args.workload, "sector": args.sector, "rows": d["rows"], "cols": d["cols"]},
+        "parallelism": "cpu",
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    if args.workload in REF_BINARY_PAPER:
+        line["ref_binary"] = reference_binary_paper(args.workload, args.sector)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -427,9 +501,7 @@ def run_paper(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    path = ROOT / "prym_green_ancillary_b200" / "_data" / f"{args.workload}.json"
-    if not path.exists():
-        raise SystemExit(f"{path} missing: build() stages the shipped instances from a reference checkout")
+    path = paper_instance(args.workload)
     from prym_green_ancillary_b200.sharding import max_over_ranks
     sector = args.sector + rank   # every rank its own sector (no collective on the data path)
     t_open = time.perf_counter()
@@ -456,6 +528,15 @@ def run_paper(args):
         dist.destroy_process_group()
     rows, cols = info["rows"], info["cols"]
     step_bytes = 2 * (rows + cols) * 4 * 4
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        got = cpu_paper(args.workload, sector, 5.0)
+        if got is not None:
+            v, d = got
+            cpu = {"value": v, "unit": "steps/s", "cores": 1, "kind": "reference",
+                   "sample": f"{d['applications']} applications of S by the reference's own CPU code "
+                             f"(cpu_apply_eliminated_square, single-threaded as written) in {d['seconds']:.2f} s; "
+                             f"Gram moments not included"}
     peak, peak_kind = measured_peaks()
     achieved = step_bytes / (ms / K / 1e3) / 1e9
     if rank == 0:
@@ -477,7 +558,7 @@ def run_paper(args):
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None,
                          "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
-            "cpu_baseline": None,
+            "cpu_baseline": cpu,
             "e2e": {"value": world * K / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": cols * 4 * 4 / K,
                     "d2h_bytes_per_step": (seq.nbytes + cur.nbytes) / K,
                     "note": "bw_cyclic_generate + bw_cyclic_download (initial block in, moments and block out)"},

@@ -2,9 +2,13 @@
  * C ABI of the B200 block-Wiedemann sequence engine over GF(p).
  *
  * Plain C types only (pointers, sizes, integers).  Every function returns 0 on
- * success and a nonzero status otherwise (1 = invalid argument or host error,
- * 2 = CUDA error, 3 = failed precondition); bw_last_error() then returns the
- * message (thread-local, valid until the next failing call on that thread).
+ * success and a nonzero status otherwise: 1 = invalid argument (a null
+ * pointer, or a size or value outside an entry point's documented range) or
+ * host error (files, parsing); 2 = CUDA error, including a tensor-core kernel
+ * that gave up a bounded wait; 3 = failed precondition (a shape the engine
+ * does not support, a call out of order such as a step without a session);
+ * bw_last_error() then returns the message (thread-local, valid until the
+ * next failing call on that thread).
  * No exception crosses this boundary.  Pointers documented as "device" are
  * CUDA device pointers of the context's device; "stream" is a cudaStream_t.
  * A NULL stream orders the call like the legacy default stream (the work runs
@@ -275,11 +279,11 @@ BW_API int bw_cyclic_recover(const char* instance_path, const char* op, uint32_t
  * a framework whose allocator owns all device memory, or code that must not
  * trigger the device-wide synchronisation of cudaMalloc / cudaFree.
  * Limits: m, n in {4, 8, 16, 32}; odd prime below 2^15; rows below 2^40;
- * larger sizes are rejected with status 1.  The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress) and should come before
- * any stream capture.  All calls share the array: calls that overlap on the
- * GPU race and give wrong results; each call clears the arrival counter it
- * needs at zero. */
+ * other sizes are rejected with status 1.  The first call on a device (and
+ * the first after cudaDeviceReset replaced its context) looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race and
+ * give wrong results; each call clears the arrival counter it needs at zero. */
 BW_API int bw_project_noalloc(const uint32_t* d_x, const uint32_t* d_w, uint64_t rows, uint32_t m, uint32_t n,
                               uint32_t prime, uint32_t* d_out, int device, void* stream);
 

@@ -38,6 +38,13 @@ int max_dynamic_smem(int device);
         if (!(cond)) throw ::bw::Error(msg, 3);                                    \
     } while (0)
 
+// An argument the caller passed outside what the entry point accepts (a null
+// pointer, a size or value beyond its documented range): status 1.
+#define BW_ARG(cond, msg)                                                          \
+    do {                                                                           \
+        if (!(cond)) throw ::bw::Error(msg, 1);                                    \
+    } while (0)
+
 // Kernels that use dynamic shared memory get the largest limit the device
 // allows them (the opt-in maximum less their static shared memory): the
 // per-function limit is process-wide, so setting one context's own size could

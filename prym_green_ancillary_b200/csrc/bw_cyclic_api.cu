@@ -16,7 +16,7 @@ extern "C" int bw_cyclic_open(const char* instance_path, const char* op, uint32_
                               uint64_t seed, uint32_t rowmix_rounds, uint64_t rowmix_seed, const char* dense_path,
                               const char* drop_path, int device, bw_cyclic** out) {
     return guarded([&] {
-        BW_REQUIRE(instance_path && op && out, "bw_cyclic_open: null argument");
+        BW_ARG(instance_path && op && out, "bw_cyclic_open: null argument");
         *out = nullptr;
         DeformInputs deform{dense_path ? dense_path : "", drop_path ? drop_path : ""};
         CyclicCtx* c = CyclicCtx::open(instance_path, op, sector, num_v, seed, rowmix_rounds, rowmix_seed, device,
@@ -27,7 +27,7 @@ extern "C" int bw_cyclic_open(const char* instance_path, const char* op, uint32_
 
 extern "C" int bw_cyclic_info_get(const bw_cyclic* ctx, bw_cyclic_info* out) {
     return guarded([&] {
-        BW_REQUIRE(ctx && out, "bw_cyclic_info_get: null argument");
+        BW_ARG(ctx && out, "bw_cyclic_info_get: null argument");
         const CyclicCtx& c = *ctx->impl;
         std::memset(out, 0, sizeof(*out));
         out->rows = c.es.target_rows;
@@ -60,7 +60,7 @@ extern "C" void bw_cyclic_close(bw_cyclic* ctx) {
 
 extern "C" int bw_cyclic_apply_host(bw_cyclic* ctx, int what, const uint32_t* in, uint32_t* out) {
     return guarded([&] {
-        BW_REQUIRE(ctx && in && out, "bw_cyclic_apply_host: null argument");
+        BW_ARG(ctx && in && out, "bw_cyclic_apply_host: null argument");
         ctx->impl->require_device();
         BW_CUDA(cudaSetDevice(ctx->impl->device));
         ctx->impl->apply_host(what, in, out);
@@ -78,7 +78,7 @@ extern "C" int bw_cyclic_generate(bw_cyclic* ctx, uint64_t nlen) {
 
 extern "C" int bw_cyclic_generate_timed(bw_cyclic* ctx, uint64_t nlen, float* device_ms) {
     return guarded([&] {
-        BW_REQUIRE(ctx && device_ms, "bw_cyclic_generate_timed: null argument");
+        BW_ARG(ctx && device_ms, "bw_cyclic_generate_timed: null argument");
         ctx->impl->require_device();
         BW_CUDA(cudaSetDevice(ctx->impl->device));
         ctx->impl->generate(nlen, device_ms);
@@ -104,7 +104,7 @@ extern "C" int bw_cyclic_download(bw_cyclic* ctx, uint32_t* packed_seq, uint64_t
 
 extern "C" int bw_cyclic_output_path(const bw_cyclic* ctx, const char* out_dir, char* buf, size_t cap) {
     return guarded([&] {
-        BW_REQUIRE(ctx && buf, "bw_cyclic_output_path: null argument");
+        BW_ARG(ctx && buf, "bw_cyclic_output_path: null argument");
         const CyclicCtx& c = *ctx->impl;
         const std::string path = cyclic::sector_filename(out_dir ? out_dir : ".", c.op, c.es.sector, c.num_v,
                                                          c.plan.rounds, c.plan.seed);
@@ -122,7 +122,7 @@ extern "C" int bw_cyclic_check_outputs_absent(const char* wdm_path) {
 
 extern "C" int bw_cyclic_write_sidecar(const bw_cyclic* ctx, const char* wdm_path) {
     return guarded([&] {
-        BW_REQUIRE(ctx && wdm_path, "bw_cyclic_write_sidecar: null argument");
+        BW_ARG(ctx && wdm_path, "bw_cyclic_write_sidecar: null argument");
         const CyclicCtx& c = *ctx->impl;
         cyclic::write_rowmix_sidecar(wdm_path, c.op, c.es.sector, c.es.target_rows, c.op_cols, c.num_v, c.p,
                                      c.seed, c.plan, c.row_precond, c.col_precond, c.initial_block);
@@ -132,7 +132,7 @@ extern "C" int bw_cyclic_write_sidecar(const bw_cyclic* ctx, const char* wdm_pat
 // save_all_data (cuda/cuprym_cyclic.cu:965-1007).
 extern "C" int bw_cyclic_write_wdm(bw_cyclic* ctx, const char* wdm_path) {
     return guarded([&] {
-        BW_REQUIRE(ctx && wdm_path, "bw_cyclic_write_wdm: null argument");
+        BW_ARG(ctx && wdm_path, "bw_cyclic_write_wdm: null argument");
         CyclicCtx& c = *ctx->impl;
         c.require_device();
         BW_REQUIRE(c.seq_len > 0, "bw_cyclic_write_wdm: no sequence generated");
@@ -199,7 +199,7 @@ extern "C" uint64_t bw_cyclic_launch_count(const bw_cyclic* ctx) { return ctx ? 
 
 extern "C" int bw_cyclic_gather_path(const bw_cyclic* ctx, char* buf, size_t cap) {
     return guarded([&] {
-        BW_REQUIRE(ctx && buf && cap > 0, "bw_cyclic_gather_path: null argument");
+        BW_ARG(ctx && buf && cap > 0, "bw_cyclic_gather_path: null argument");
         const CyclicCtx& c = *ctx->impl;
         const std::string path = c.host_only ? std::string("none: host-only context")
                                  : c.subset_path ? std::string(c.stream_tables ? "subset: tables evict-first"
@@ -212,7 +212,7 @@ extern "C" int bw_cyclic_gather_path(const bw_cyclic* ctx, char* buf, size_t cap
 
 extern "C" int bw_file_read_text(const char* path, char* buf, size_t cap, size_t* len) {
     return guarded([&] {
-        BW_REQUIRE(path && len, "bw_file_read_text: null argument");
+        BW_ARG(path && len, "bw_file_read_text: null argument");
         const std::string text = wdm::read_file(path);
         *len = text.size();
         if (buf) {

@@ -273,7 +273,7 @@ extern "C" int bw_cyclic_recover(const char* instance_path, const char* op, uint
                                  const char* drop_path, int64_t cli_rounds, uint64_t cli_seed, int rounds_supplied,
                                  int seed_supplied, int validate, int device) {
     return guarded([&] {
-        BW_REQUIRE(instance_path && op && wdm_path, "bw_cyclic_recover: null argument");
+        BW_ARG(instance_path && op && wdm_path, "bw_cyclic_recover: null argument");
         const std::string wdm(wdm_path);
         const std::string gens = generators_path && *generators_path ? generators_path
                                                                      : recovery::default_generators_filename(wdm);

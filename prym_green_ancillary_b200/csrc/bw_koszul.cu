@@ -517,7 +517,7 @@ void KoszulCtx::release(void* p) {
 
 void KoszulCtx::seq_start(const uint32_t* x, const uint32_t* y0, uint32_t* seq, uint64_t capacity,
                           cudaStream_t st) {
-    BW_REQUIRE(x != nullptr && y0 != nullptr && seq != nullptr, "seq_start: null buffer");
+    BW_ARG(x != nullptr && y0 != nullptr && seq != nullptr, "seq_start: null buffer");
     BW_REQUIRE(capacity >= 1, "seq_start: sequence capacity must be at least 1");
     d_seq = seq;
     seq_capacity = capacity;
@@ -625,7 +625,7 @@ struct StreamScope {
 
 extern "C" int bw_koszul_create(const bw_koszul_desc* desc, int device, bw_koszul** out) {
     return guarded([&] {
-        BW_REQUIRE(desc != nullptr && out != nullptr, "bw_koszul_create: null argument");
+        BW_ARG(desc != nullptr && out != nullptr, "bw_koszul_create: null argument");
         *out = nullptr;
         KoszulCtx* impl = KoszulCtx::create(*desc, device);
         *out = new bw_koszul{impl};
@@ -634,7 +634,7 @@ extern "C" int bw_koszul_create(const bw_koszul_desc* desc, int device, bw_koszu
 
 extern "C" int bw_koszul_info_get(const bw_koszul* ctx, bw_koszul_info* out) {
     return guarded([&] {
-        BW_REQUIRE(ctx != nullptr && out != nullptr, "bw_koszul_info_get: null argument");
+        BW_ARG(ctx != nullptr && out != nullptr, "bw_koszul_info_get: null argument");
         const KoszulCtx& c = *ctx->impl;
         out->n_src = c.n_src;
         out->n_tgt = c.n_tgt;
@@ -653,7 +653,7 @@ extern "C" void bw_koszul_destroy(bw_koszul* ctx) {
 
 extern "C" int bw_koszul_forward(bw_koszul* ctx, const uint32_t* d_y, uint32_t* d_z, void* stream) {
     return guarded([&] {
-        BW_REQUIRE(ctx && d_y && d_z, "bw_koszul_forward: null argument");
+        BW_ARG(ctx && d_y && d_z, "bw_koszul_forward: null argument");
         KoszulCtx& c = *ctx->impl;
         BW_REQUIRE(!c.in_session, "bw_koszul_forward: a sequence session is open");
         BW_CUDA(cudaSetDevice(c.device));
@@ -676,7 +676,7 @@ extern "C" int bw_koszul_forward(bw_koszul* ctx, const uint32_t* d_y, uint32_t* 
 extern "C" int bw_koszul_transpose(bw_koszul* ctx, const uint32_t* d_z, uint32_t* d_w, int scale_by_diag,
                                    void* stream) {
     return guarded([&] {
-        BW_REQUIRE(ctx && d_z && d_w, "bw_koszul_transpose: null argument");
+        BW_ARG(ctx && d_z && d_w, "bw_koszul_transpose: null argument");
         KoszulCtx& c = *ctx->impl;
         BW_REQUIRE(!c.in_session, "bw_koszul_transpose: a sequence session is open");
         BW_CUDA(cudaSetDevice(c.device));
@@ -698,7 +698,7 @@ extern "C" int bw_koszul_transpose(bw_koszul* ctx, const uint32_t* d_z, uint32_t
 
 extern "C" int bw_koszul_apply(bw_koszul* ctx, const uint32_t* d_y, uint32_t* d_out, void* stream) {
     return guarded([&] {
-        BW_REQUIRE(ctx && d_y && d_out, "bw_koszul_apply: null argument");
+        BW_ARG(ctx && d_y && d_out, "bw_koszul_apply: null argument");
         KoszulCtx& c = *ctx->impl;
         BW_REQUIRE(!c.in_session, "bw_koszul_apply: a sequence session is open");
         BW_CUDA(cudaSetDevice(c.device));
@@ -754,7 +754,7 @@ extern "C" int bw_koszul_seq_finish(bw_koszul* ctx, uint32_t* d_y_out, uint64_t*
 extern "C" int bw_koszul_sequence_host(bw_koszul* ctx, const uint32_t* h_x, const uint32_t* h_y0, uint64_t nlen,
                                        uint32_t* h_seq, uint32_t* h_y_final) {
     return guarded([&] {
-        BW_REQUIRE(ctx && h_x && h_y0 && h_seq, "bw_koszul_sequence_host: null argument");
+        BW_ARG(ctx && h_x && h_y0 && h_seq, "bw_koszul_sequence_host: null argument");
         BW_REQUIRE(nlen >= 1, "bw_koszul_sequence_host: nlen must be at least 1");
         KoszulCtx& c = *ctx->impl;
         BW_CUDA(cudaSetDevice(c.device));
@@ -775,7 +775,7 @@ extern "C" int bw_koszul_sequence_host(bw_koszul* ctx, const uint32_t* h_x, cons
 
 extern "C" int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* ms_out, void* stream) {
     return guarded([&] {
-        BW_REQUIRE(ctx != nullptr && ms_out != nullptr, "bw_koszul_seq_step_timed: null argument");
+        BW_ARG(ctx != nullptr && ms_out != nullptr, "bw_koszul_seq_step_timed: null argument");
         KoszulCtx& c = *ctx->impl;
         BW_REQUIRE(c.in_session, "bw_koszul_seq_step_timed: no sequence session");
         BW_REQUIRE(c.seq_len + steps <= c.seq_capacity, "bw_koszul_seq_step_timed: capacity exceeded");

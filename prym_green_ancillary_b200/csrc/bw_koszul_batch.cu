@@ -132,7 +132,7 @@ struct BatchStream {
 extern "C" int bw_koszul_batch_create(const bw_koszul_desc* descs, uint32_t count, int device,
                                       bw_koszul_batch** out) {
     return guarded([&] {
-        BW_REQUIRE(descs && out && count > 0, "bw_koszul_batch_create: null argument or empty batch");
+        BW_ARG(descs && out && count > 0, "bw_koszul_batch_create: null argument or empty batch");
         *out = nullptr;
         std::unique_ptr<KoszulBatch> b(new KoszulBatch());
         b->device = device;
@@ -166,7 +166,7 @@ extern "C" void bw_koszul_batch_destroy(bw_koszul_batch* batch) {
 
 extern "C" int bw_koszul_batch_sector(bw_koszul_batch* batch, uint32_t index, bw_koszul** out) {
     return guarded([&] {
-        BW_REQUIRE(batch && out, "bw_koszul_batch_sector: null argument");
+        BW_ARG(batch && out, "bw_koszul_batch_sector: null argument");
         BW_REQUIRE(index < batch->impl->sectors.size(), "bw_koszul_batch_sector: index out of range");
         *out = &batch->impl->handles[index];
     });
@@ -176,7 +176,7 @@ extern "C" int bw_koszul_batch_seq_start(bw_koszul_batch* batch, const uint32_t*
                                          const uint32_t* const* d_y0, uint32_t* const* d_seq,
                                          uint64_t seq_capacity, void* stream) {
     return guarded([&] {
-        BW_REQUIRE(batch && d_x && d_y0 && d_seq, "bw_koszul_batch_seq_start: null argument");
+        BW_ARG(batch && d_x && d_y0 && d_seq, "bw_koszul_batch_seq_start: null argument");
         KoszulBatch& b = *batch->impl;
         BW_CUDA(cudaSetDevice(b.device));
         BatchStream bs(b, stream);

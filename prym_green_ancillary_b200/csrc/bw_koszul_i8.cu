@@ -2,7 +2,7 @@
 //
 // Every residue x (balanced, |x| <= (p-1)/2 < 2^14) is stored in HBM as two
 // signed 8-bit limbs in base 255:  x = 255*hi + lo,  lo in [-127, 127],
-// hi in [-63, 63].  The symmetric range makes negation exact in int8, which
+// hi in [-64, 64] (|x| <= 16383 = 255 * 64 + 63).  The symmetric range makes negation exact in int8, which
 // is how the Koszul signs are applied while operands are staged.
 //
 // One gather-GEMM kernel serves both d and d^T.  For a tile of 128/n output
@@ -23,19 +23,22 @@
 // laid out [blk][h][u][16 bytes] (h = j / 16), so that every (block, h) is one
 // contiguous run of inner * 16 bytes.  The producers fill a stage with 16-byte
 // cp.async copies (one per K' row, limb and column group) from the +plane or
-// the -plane by the Koszul sign; the rows of an absent generator are zeroed
-// with shared-memory stores (about half of all rows: a common zero source in
-// global memory would funnel that half of the traffic through one L2 slice).
+// the -plane by the Koszul sign; the rows of an absent generator (about half
+// of all rows) are zero-filled by the same copy with source size 0, which
+// reads nothing (a common zero source in global memory would funnel that half
+// of the traffic through one L2 slice).
 // The epilogue writes all four planes of its output.
 //
 // Warp roles (persistent, one CTA per SM):
-//   warps 0-3   producers: each owns a quarter of the tile's output blocks and
-//               keeps their incidence rows in registers (one generator per
-//               lane); every thread arrives on the stage barrier through
-//               cp.async.mbarrier.arrive.noinc when its copies have landed;
-//   warp 4      allocates TMEM and issues tcgen05.mma / tcgen05.commit (after a
+//   warps 0-7   producers: each owns an eighth of the tile's output blocks (or,
+//               with fewer blocks per tile than producer warps, a share of one
+//               block's rows) and keeps their incidence rows in registers (one
+//               generator per lane); every thread arrives on the stage barrier
+//               through cp.async.mbarrier.arrive.noinc when its copies have
+//               landed;
+//   warp 8      allocates TMEM and issues tcgen05.mma / tcgen05.commit (after a
 //               proxy fence: the stage was written through the generic proxy);
-//   warps 5-12  epilogue, two warps per TMEM lane quadrant: tcgen05.ld the four
+//   warps 9-16  epilogue, two warps per TMEM lane quadrant: tcgen05.ld the four
 //               partials, recombine, reduce mod p, scale by D (d^T only), split
 //               into limbs, transpose 16 x 16 bytes per half-warp and store one
 //               16-byte plane row per lane.
@@ -47,7 +50,9 @@
 #include "tc_sm100.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 namespace bw {
@@ -83,6 +88,8 @@ struct I8Dir {
     uint32_t b_bytes, slot_bytes, limb_bytes;
     Mod mod;
     int32_t c1, c2;              // 255 and 255^2 mod p, balanced
+    uint32_t wait_limit;         // tries of every pipeline wait (tc::kWaitLimit outside the failure tests)
+    int hold_first_stage;        // failure tests only: CTA 0 never fills its first stage
 };
 
 // Position in a ring of pipeline slots: slot index and the parity of its
@@ -202,14 +209,14 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
 
     if (warp < kProducerWarps) {
         // ------------------------------------------------------------ producers
-        // Warp w stages the output blocks t = w, w + 4, ... of each tile.  Lane
+        // Warp w stages the output blocks t = w % GROUPS, + GROUPS, ... of each tile.  Lane
         // i holds the incidence entry of generator i for those blocks (read by
         // shuffle; the next tile's entries are loaded one tile ahead), and the
         // warp's lanes walk the K' rows of every (limb, block, column group):
         // a 16-byte cp.async from the +plane or -plane of the neighbour block,
-        // or a zero store for an absent generator.  Each thread arrives on the
-        // stage barrier twice: once through cp.async.mbarrier.arrive.noinc when
-        // its copies have landed, once with release semantics for its stores.
+        // or a zero-filling one (source size 0) for an absent generator.  Each
+        // thread arrives on the stage barrier once, through
+        // cp.async.mbarrier.arrive.noinc, when its copies have landed.
         // More producer warps than blocks: RPW warps share a block, interleaving its rows.
         constexpr int RPW = kProducerWarps > BT ? kProducerWarps / BT : 1;
         constexpr int GROUPS = kProducerWarps / RPW;                     // distinct block positions
@@ -236,12 +243,15 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                 const int slot = ring.slot;
                 const uint32_t ph = ring.phase;
                 int got = 1;
-                if (lane == 0) got = tc::mbar_wait(&empty[slot], ph ^ 1u, abort, P.err, tc::ERR_WAIT_EMPTY) ? 1 : 0;
+                if (lane == 0)
+                    got = tc::mbar_wait(&empty[slot], ph ^ 1u, abort, P.err, tc::ERR_WAIT_EMPTY, P.wait_limit) ? 1 : 0;
                 got = __shfl_sync(0xffffffffu, got, 0);
                 if (!got) {
                     ok = false;
                     break;
                 }
+                // failure tests: the first stage of CTA 0 is never filled, so its consumer's wait runs out
+                if (P.hold_first_stage && blockIdx.x == 0 && tile == blockIdx.x && s == 0) continue;
                 const int g_s = min(P.gi, P.r - s * P.gi);
                 const int rows = g_s * P.inner;             // K' rows filled in this stage
                 uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
@@ -287,13 +297,13 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
             for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
                 const int buf = static_cast<int>(tcount & 1);
                 const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
-                if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, abort, P.err, tc::ERR_WAIT_ACCUM_FREE)) break;
+                if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, abort, P.err, tc::ERR_WAIT_ACCUM_FREE, P.wait_limit)) break;
                 tc::tc_fence_after();
                 const uint32_t dbase = tmem + static_cast<uint32_t>(buf * 2 * N);
                 for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
                     const int slot = ring.slot;
                     const uint32_t ph = ring.phase;
-                    if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL)) {
+                    if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL, P.wait_limit)) {
                         ok = false;
                         break;
                     }
@@ -324,7 +334,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         __syncwarp();
     } else {
         // ------------------------------------------------------------ epilogue
-        // Warps 5..12: warp & 3 is the TMEM lane quadrant it may read; the two
+        // Warps 9..16: warp & 3 is the TMEM lane quadrant it may read; the two
         // warps of a quadrant split the 16-column output chunks between them.
         const int q = warp & 3;
         constexpr int EPQ = kEpilogueWarps / 4;                 // epilogue warps per quadrant
@@ -350,7 +360,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                 }
             };
             load_diag(half_id);
-            if (!tc::mbar_wait(&accfull[buf], aph, abort, P.err, tc::ERR_WAIT_ACCUM)) break;
+            if (!tc::mbar_wait(&accfull[buf], aph, abort, P.err, tc::ERR_WAIT_ACCUM, P.wait_limit)) break;
             tc::tc_fence_after();
             const uint32_t col0 = tmem + lane_off + static_cast<uint32_t>(buf * 2 * N);
             const long long base = blk * static_cast<long long>(NB) * P.outer;
@@ -480,6 +490,7 @@ struct I8Proj {
     uint32_t a_bytes, slot_bytes, pad_bytes;
     Mod mod;
     int32_t c1, c2;
+    uint32_t wait_limit;        // tries of every pipeline wait (tc::kWaitLimit outside the failure tests)
 };
 
 template <int NB>
@@ -535,7 +546,7 @@ __global__ void __launch_bounds__(kProjThreads, 1) i8_project_tc_kernel(I8Proj P
             const int nbh = static_cast<int>(min(static_cast<long long>(P.sb), P.n_blk - blk0));
             int got = 1;
             if (lane == 0) {
-                got = tc::mbar_wait(&empty[slot], ph ^ 1u, abort, P.err, tc::ERR_WAIT_EMPTY) ? 1 : 0;
+                got = tc::mbar_wait(&empty[slot], ph ^ 1u, abort, P.err, tc::ERR_WAIT_EMPTY, P.wait_limit) ? 1 : 0;
                 if (got)
                     tc::mbar_arrive_expect_tx(&full[slot], P.a_bytes + 2u * HG * nbh * run_bytes);
             }
@@ -571,14 +582,14 @@ __global__ void __launch_bounds__(kProjThreads, 1) i8_project_tc_kernel(I8Proj P
             for (long long c = 0; c < n_chunks && ok; ++c) {
                 const int buf = static_cast<int>(c & 1);
                 const uint32_t aph = static_cast<uint32_t>((c >> 1) & 1);
-                if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, abort, P.err, tc::ERR_WAIT_ACCUM_FREE)) break;
+                if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, abort, P.err, tc::ERR_WAIT_ACCUM_FREE, P.wait_limit)) break;
                 tc::tc_fence_after();
                 const uint32_t dcol = tmem + static_cast<uint32_t>(buf * N);
                 const long long i_end = min(n_my, (c + 1) * P.drain);
                 for (bool first = true; i < i_end; ++i, first = false, ring.next()) {
                     const int slot = ring.slot;
                     const uint32_t ph = ring.phase;
-                    if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL)) {
+                    if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL, P.wait_limit)) {
                         ok = false;
                         break;
                     }
@@ -608,7 +619,7 @@ __global__ void __launch_bounds__(kProjThreads, 1) i8_project_tc_kernel(I8Proj P
         for (long long c = 0; c < n_chunks; ++c) {
             const int buf = static_cast<int>(c & 1);
             const uint32_t aph = static_cast<uint32_t>((c >> 1) & 1);
-            if (!tc::mbar_wait(&accfull[buf], aph, abort, P.err, tc::ERR_WAIT_ACCUM)) break;
+            if (!tc::mbar_wait(&accfull[buf], aph, abort, P.err, tc::ERR_WAIT_ACCUM, P.wait_limit)) break;
             tc::tc_fence_after();
             if (active) {
                 const uint32_t col0 = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(buf * N);
@@ -913,9 +924,23 @@ void KoszulCtx::i8_setup() {
     plan_projection(*this, S);
     plan_direction(*this, S.fwd, ci, co, false);
     plan_direction(*this, S.bwd, co, ci, true);
+    // Failure tests only (the environment of the creating process): a short
+    // limit on every pipeline wait, and a first stage that CTA 0 of the d/d^T
+    // kernel never fills, so that its consumer's wait runs out and the kernel
+    // gives up, frees its TMEM and returns; the host then reports status 2.
+    uint32_t wait_limit = tc::kWaitLimit;
+    if (const char* e = std::getenv("BW_TEST_WAIT_LIMIT")) {
+        const unsigned long v = std::strtoul(e, nullptr, 10);
+        if (v >= 1 && v < tc::kWaitLimit) wait_limit = static_cast<uint32_t>(v);
+    }
+    int hold = 0;
+    if (const char* e = std::getenv("BW_TEST_HOLD_FIRST_STAGE")) hold = (*e && std::string(e) != "0") ? 1 : 0;
     for (I8State::Dir* D : {&S.fwd, &S.bwd}) {
         D->p.err = S.err;
+        D->p.wait_limit = wait_limit;
+        D->p.hold_first_stage = hold;
     }
+    S.proj.wait_limit = wait_limit;
     S.fwd.p.inc = S.fwd.inc;
     S.bwd.p.inc = S.bwd.inc;
     S.fwd.p.n_blk = static_cast<long long>(n_t);
@@ -950,7 +975,13 @@ void KoszulCtx::i8_check_error() {
     BW_CUDA(cudaMemcpy(&err, i8->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (err != 0) {
         cudaMemset(i8->err, 0, sizeof(int));
-        throw Error("INT8 tensor-core kernel gave up waiting (pipeline stage wait, code " + std::to_string(err) + ")", 2);
+        static const char* const names[] = {"", "ERR_WAIT_FULL: consumer waited for a loaded stage",
+                                            "ERR_WAIT_EMPTY: producer waited for a free stage",
+                                            "ERR_WAIT_ACCUM: epilogue waited for an accumulator",
+                                            "ERR_WAIT_ACCUM_FREE: MMA waited for a free accumulator",
+                                            "ERR_WAIT_FINAL: final drain of in-flight MMAs"};
+        const std::string what = (err >= 1 && err <= 5) ? names[err] : "code " + std::to_string(err);
+        throw Error("INT8 tensor-core kernel gave up waiting (" + what + ")", 2);
     }
 }
 

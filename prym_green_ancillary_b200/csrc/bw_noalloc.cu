@@ -17,6 +17,8 @@
 #include "bw_common.cuh"
 #include "../../include/bw_engine.h"
 
+#include <cuda.h>   // CUcontext, CUresult: the driver's cuCtxGetCurrent, reached through the runtime
+
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
@@ -35,20 +37,49 @@ constexpr size_t kScratchWords = kCounterWords + static_cast<size_t>(kNoAllocMax
 // device address obtained with cudaGetSymbolAddress.
 static __device__ __align__(256) int32_t bw_noalloc_scratch[kScratchWords];
 
-std::mutex g_symbol_mutex;
-void* g_symbol_address[64] = {};   // per device ordinal
+// The calling thread's current CUDA context.  The scratch address is only
+// valid in the context it was looked up in: after cudaDeviceReset the device's
+// primary context is a new one, with the library's module loaded anew.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
 
-// Device address of the scratch array on `device` (which must be current).
+void* current_context() {
+    static const CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    BW_REQUIRE(fn != nullptr, "bw_project_noalloc: cuCtxGetCurrent is not available from the driver");
+    CUcontext ctx = nullptr;
+    BW_REQUIRE(fn(&ctx) == CUDA_SUCCESS && ctx != nullptr, "bw_project_noalloc: no current CUDA context");
+    return ctx;
+}
+
+struct ScratchEntry {
+    void* context = nullptr;   // the context the address belongs to
+    void* address = nullptr;
+};
+std::mutex g_symbol_mutex;
+ScratchEntry g_symbol_address[64];   // per device ordinal
+
+// Device address of the scratch array on `device` (which must be current):
+// looked up once per device with cudaGetSymbolAddress, and again when the
+// device's current context has changed since (cudaDeviceReset).
 void* scratch_address(int device) {
-    BW_REQUIRE(device >= 0 && device < 64, "bw_project_noalloc: device ordinal out of range");
+    BW_ARG(device >= 0 && device < 64, "bw_project_noalloc: device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_symbol_mutex);
-    if (!g_symbol_address[device]) {
+    ScratchEntry& e = g_symbol_address[device];
+    void* ctx = current_context();
+    if (e.address == nullptr || e.context != ctx) {
         void* ptr = nullptr;
         BW_CUDA(cudaGetSymbolAddress(&ptr, bw_noalloc_scratch));
         BW_REQUIRE(ptr != nullptr, "bw_project_noalloc: scratch symbol has no device address");
-        g_symbol_address[device] = ptr;
+        e.context = ctx;
+        e.address = ptr;
     }
-    return g_symbol_address[device];
+    return e.address;
 }
 
 // Same decomposition as the engine's projection: every CTA folds a strided
@@ -131,13 +162,13 @@ using namespace bw;
 extern "C" int bw_project_noalloc(const uint32_t* d_x, const uint32_t* d_w, uint64_t rows, uint32_t m, uint32_t n,
                                   uint32_t prime, uint32_t* d_out, int device, void* stream) {
     return guarded([&] {
-        BW_REQUIRE(d_x && d_w && d_out, "bw_project_noalloc: null buffer");
+        BW_ARG(d_x && d_w && d_out, "bw_project_noalloc: null buffer");
         auto ok_w = [](uint32_t w) { return w == 4 || w == 8 || w == 16 || w == 32; };
-        BW_REQUIRE(ok_w(m) && ok_w(n),
+        BW_ARG(ok_w(m) && ok_w(n),
                    "bw_project_noalloc: m and n must be 4, 8, 16 or 32 (the scratch holds at most 32 x 32 sums per CTA)");
-        BW_REQUIRE(prime >= 3 && prime < 32768 && (prime & 1u), "bw_project_noalloc: prime must be odd and below 2^15");
-        BW_REQUIRE(rows >= 1 && rows < (1ull << 40), "bw_project_noalloc: rows must be in 1..2^40-1");
-        BW_REQUIRE(reinterpret_cast<uintptr_t>(d_w) % 16 == 0, "bw_project_noalloc: W must be 16-byte aligned");
+        BW_ARG(prime >= 3 && prime < 32768 && (prime & 1u), "bw_project_noalloc: prime must be odd and below 2^15");
+        BW_ARG(rows >= 1 && rows < (1ull << 40), "bw_project_noalloc: rows must be in 1..2^40-1");
+        BW_ARG(reinterpret_cast<uintptr_t>(d_w) % 16 == 0, "bw_project_noalloc: W must be 16-byte aligned");
         BW_CUDA(cudaSetDevice(device));
         int32_t* scratch = static_cast<int32_t*>(scratch_address(device));
         const int sms = sm_count(device);

@@ -60,13 +60,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Wait for the phase with the given parity to complete, at most kWaitLimit
+// Wait for the phase with the given parity to complete, at most `limit`
 // tries.  `abort` (shared memory, or null) is the CTA's give-up flag: the wait
 // returns false once another role of the CTA has given up, and a wait that
 // runs out sets it and records `code` in the global error word.  Polling only
 // the shared flag keeps every spin on-chip.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort, int* err, int code) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort, int* err, int code,
+                                          uint32_t limit = kWaitLimit) {
+    for (uint32_t i = 0; i < limit; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
         if (abort != nullptr && *abort != 0) return false;
     }

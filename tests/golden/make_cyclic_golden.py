@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Generate the paper-mode golden fixtures from the reference's own code.
 
-    python tests/golden/make_cyclic_golden.py --reference /root/reference
+    python tests/golden/make_cyclic_golden.py --reference <reference checkout>
 
 * ``g12_p661.json`` / ``g12_p109.json``: genus-12 instances made by the
   reference's ``scripts.prepare_deformation.build_instance`` (the instance its

@@ -4,7 +4,7 @@
 Run in a container that holds the reference checkout (it imports the
 reference's explicit sparse-matrix oracle):
 
-    python tests/golden/make_koszul_golden.py --reference /root/reference
+    python tests/golden/make_koszul_golden.py --reference <reference checkout>
 
 The operator d is assembled as an explicit scipy CSR matrix by the
 reference's own ``differential()`` (tests/deformation_reference.py:75-89 of
