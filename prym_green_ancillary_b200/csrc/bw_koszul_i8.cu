@@ -49,6 +49,8 @@
 #include "bw_koszul.cuh"
 #include "tc_sm100.cuh"
 
+#include <cuda.h>   // CUtensorMap and cuTensorMapEncodeTiled's types (the function is reached through the runtime)
+
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -90,6 +92,13 @@ struct I8Dir {
     int32_t c1, c2;              // 255 and 255^2 mod p, balanced
     uint32_t wait_limit;         // tries of every pipeline wait (tc::kWaitLimit outside the failure tests)
     int hold_first_stage;        // failure tests only: CTA 0 never fills its first stage
+    // TMA gather producer (i8_gather4_kernel)
+    const int4* rows4;           // [n_blk][groups]: plane rows of the four generators of a group (h = 0)
+    int groups;                  // ceil(r / 4)
+    int gs;                      // groups per stage
+    int inner_pad;               // K' rows of a generator: inner rounded up to even (128-byte aligned groups)
+    int32_t row_oob;             // a plane row past the input tensor (2 * input blocks * HG): zero-filled
+    uint32_t tx_full, tx_last;   // bytes a full / the last stage of a tile receives
 };
 
 // Position in a ring of pipeline slots: slot index and the parity of its
@@ -416,6 +425,265 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
     }
 }
 
+// ---- gather-GEMM with a TMA gather producer
+//
+// Same tile, MMA issue and epilogue as i8_gather_gemm_kernel; the stage is
+// filled by the tensor-memory accelerator instead of cp.async warps.  The
+// +plane and the -plane of a limb are one 2-D tensor (rows = (block, h) runs of
+// inner * 16 bytes, the -plane's rows after the +plane's), so one tile::gather4
+// copies the runs of four neighbour blocks, each from the plane its Koszul sign
+// selects, into the four generators' K' rows of one (output block, limb, h)
+// core-matrix column: row = neg * n_blk * HG + nbr * HG + h, precomputed on the
+// host per group of four generators (rows4).  An absent generator (or a padding
+// generator past r) has a row beyond the tensor: the copy fills its rows with
+// zeros and reads nothing.  A generator spans inner_pad (even) K' rows, so every
+// gather starts 128-byte aligned; the odd padding row is beyond the tensor's
+// row width (zero-filled) and meets zero rows of the maps.
+//
+// Warp roles: warp 0 producer (one gather per lane and stage), warp 1 MMA
+// issuer (allocates TMEM), warps 2-9 epilogue.  On a give-up the producer
+// still waits (bounded) for the copies it issued before the CTA exits.
+constexpr int kG4Threads = (2 + kEpilogueWarps) * 32;
+
+template <int NB>
+__global__ void __launch_bounds__(kG4Threads, 1)
+    i8_gather4_kernel(const __grid_constant__ CUtensorMap map_lo, const __grid_constant__ CUtensorMap map_hi,
+                      I8Dir P) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    constexpr int BT = 128 / NB;        // output blocks per tile
+    constexpr int HG = NB / 16;         // 16-byte column groups per block row
+    constexpr int kMaxSlots = 8;
+    const int N = 2 * P.half;
+    uint8_t* sB = smem;
+    uint8_t* sA = smem + P.b_bytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sA + static_cast<size_t>(P.slots) * P.slot_bytes);
+    uint64_t* empty = full + P.slots;
+    uint64_t* accfull = empty + P.slots;
+    uint64_t* accempty = accfull + 2;
+    uint64_t* drained = accempty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
+    volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);   // CTA give-up flag
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const long long n_tiles = (P.n_blk + BT - 1) / BT;
+    // every gather destination is 128-byte aligned relative to the base
+    if ((tc::smem_u32(smem) & 127u) != 0 || P.slots > kMaxSlots) {
+        if (threadIdx.x == 0) atomicCAS(P.err, tc::ERR_NONE, tc::ERR_LAYOUT);
+        return;
+    }
+
+    for (uint32_t off = threadIdx.x * 16; off < P.b_bytes; off += blockDim.x * 16)
+        *reinterpret_cast<int4*>(sB + off) = __ldg(reinterpret_cast<const int4*>(P.b_tiles + off));
+    tc::fence_proxy_async_smem();
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < P.slots; ++s) {
+            tc::mbar_init(&full[s], 1);     // the producer's arrive.expect_tx; the copies complete the bytes
+            tc::mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            tc::mbar_init(&accfull[b], 1);
+            tc::mbar_init(&accempty[b], kEpilogueWarps * 32);
+        }
+        tc::mbar_init(drained, 1);
+        tc::fence_mbar_init();
+        *abort = 0;
+    }
+    const uint32_t tmem_cols = (4 * N <= 256) ? 256u : 512u;
+    if (warp == 1) {
+        tc::tmem_alloc(tmem_slot, tmem_cols);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int KS = P.ks_full * 32;                    // K' rows of a slot's column (full stage, padded)
+    const uint32_t gbytes = static_cast<uint32_t>(P.inner_pad) * 64;   // one group: 4 generators x inner_pad rows
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        // Stage s of a tile holds the groups s * gs .. s * gs + gs - 1 of every
+        // (output block t, limb, h): 2 * BT * HG * gs gathers, lane j issues
+        // j, j + 32, ...  Lane 0 posts the stage's byte count first.
+        tc::prefetch_tmap(&map_lo);
+        tc::prefetch_tmap(&map_hi);
+        const int32_t oob = P.row_oob;   // beyond the input tensor: zero rows, nothing read
+        SlotRing ring(P.slots);
+        uint32_t issued_phase[kMaxSlots];
+        bool issued[kMaxSlots];
+#pragma unroll
+        for (int q = 0; q < kMaxSlots; ++q) issued[q] = false, issued_phase[q] = 0;
+        bool ok = true;
+        for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+            for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
+                const int slot = ring.slot;
+                const uint32_t ph = ring.phase;
+                int got = 1;
+                if (lane == 0)
+                    got = tc::mbar_wait(&empty[slot], ph ^ 1u, abort, P.err, tc::ERR_WAIT_EMPTY, P.wait_limit) ? 1 : 0;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) {
+                    ok = false;
+                    break;
+                }
+                // failure tests: the first stage of CTA 0 is never filled, so its consumer's wait runs out
+                if (P.hold_first_stage && blockIdx.x == 0 && tile == blockIdx.x && s == 0) continue;
+                const bool last = s == P.stages_per_tile - 1;
+                const int g_n = last ? P.groups - s * P.gs : P.gs;   // groups in this stage
+                if (lane == 0) tc::mbar_arrive_expect_tx(&full[slot], last ? P.tx_last : P.tx_full);
+                __syncwarp();
+                uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
+                const int n_g = 2 * BT * HG * g_n;
+                for (int j = lane; j < n_g; j += 32) {
+                    const int gl = j % g_n;                 // group within the stage
+                    const int rest = j / g_n;
+                    const int limb = rest & 1;
+                    const int col = rest >> 1;              // t * HG + h
+                    const int t = col / HG, h = col - (col / HG) * HG;
+                    const long long blk = tile * BT + t;
+                    int4 rr = make_int4(oob, oob, oob, oob);
+                    if (blk < P.n_blk) rr = __ldg(P.rows4 + blk * P.groups + s * P.gs + gl);
+                    uint8_t* dst = slotA + static_cast<size_t>(limb) * P.limb_bytes +
+                                   static_cast<size_t>(col) * KS * 16 + static_cast<size_t>(gl) * gbytes;
+                    tc::tma_gather4(dst, limb ? static_cast<const void*>(&map_hi) : static_cast<const void*>(&map_lo),
+                                    0, rr.x + h, rr.y + h, rr.z + h, rr.w + h, &full[slot]);
+                }
+                issued[slot] = true;
+                issued_phase[slot] = ph;
+            }
+        }
+        // no copy may still be landing when the CTA exits: wait (bounded) for
+        // the last stage issued into every slot (a consumed stage has completed)
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < kMaxSlots; ++q)
+                if (q < P.slots && issued[q]) tc::mbar_wait(&full[q], issued_phase[q], nullptr, P.err, tc::ERR_WAIT_FINAL);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_i8(128, N, true, false);
+            const uint32_t sA0 = tc::smem_u32(sA), sB0 = tc::smem_u32(sB);
+            long long tcount = 0;
+            SlotRing ring(P.slots);
+            bool ok = true;
+            for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
+                const int buf = static_cast<int>(tcount & 1);
+                const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
+                if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, abort, P.err, tc::ERR_WAIT_ACCUM_FREE, P.wait_limit)) break;
+                tc::tc_fence_after();
+                const uint32_t dbase = tmem + static_cast<uint32_t>(buf * 2 * N);
+                for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
+                    const int slot = ring.slot;
+                    const uint32_t ph = ring.phase;
+                    if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL, P.wait_limit)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::tc_fence_after();
+                    const int ks_n = (s == P.stages_per_tile - 1) ? P.ks_last : P.ks_full;
+                    for (int limb = 0; limb < 2; ++limb) {
+                        const uint32_t a_base = sA0 + static_cast<uint32_t>(slot) * P.slot_bytes +
+                                                static_cast<uint32_t>(limb) * P.limb_bytes;
+                        for (int ks = 0; ks < ks_n; ++ks) {
+                            const uint64_t ad = tc::smem_desc(a_base + ks * 512u, 128u, static_cast<uint32_t>(KS) * 16u);
+                            const uint32_t gks = static_cast<uint32_t>(s * P.ks_full + ks);
+                            const uint64_t bd = tc::smem_desc(sB0 + gks * static_cast<uint32_t>(N) * 32u, 128u, 256u);
+                            tc::mma_i8(dbase + static_cast<uint32_t>(limb * N), ad, bd, idesc,
+                                       (s > 0 || ks > 0) ? 1u : 0u);
+                        }
+                    }
+                    tc::mma_commit(&empty[slot]);
+                }
+                if (!ok) break;
+                tc::mma_commit(&accfull[buf]);
+            }
+            // drain: every MMA issued above completes before TMEM is released
+            tc::mma_commit(drained);
+            tc::mbar_wait(drained, 0, nullptr, P.err, tc::ERR_WAIT_FINAL);
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------------ epilogue
+        // Warps 2..9: warp & 3 is the TMEM lane quadrant it may read; the two
+        // warps of a quadrant split the 16-column output chunks between them.
+        const int q = warp & 3;
+        constexpr int EPQ = kEpilogueWarps / 4;
+        const int half_id = (warp - 2) >> 2;
+        const int m = q * 32 + lane;               // tile row = (block t, column j)
+        const int t = m / NB, j = m % NB;
+        const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
+        const int chunks = P.half / 16;
+        const uint32_t h_off = static_cast<uint32_t>((j >> 4) * P.outer * 16);
+        long long tcount = 0;
+        for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++tcount) {
+            const int buf = static_cast<int>(tcount & 1);
+            const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
+            const long long blk = tile * BT + t;
+            const bool valid = blk < P.n_blk;
+            int32_t dg[16];
+            auto load_diag = [&](int c) {
+#pragma unroll
+                for (int oo = 0; oo < 16; ++oo) {
+                    const int o = c * 16 + oo;
+                    dg[oo] = (P.diag && valid && o < P.outer) ? __ldg(P.diag + blk * P.outer + o) : 0;
+                }
+            };
+            load_diag(half_id);
+            if (!tc::mbar_wait(&accfull[buf], aph, abort, P.err, tc::ERR_WAIT_ACCUM, P.wait_limit)) break;
+            tc::tc_fence_after();
+            const uint32_t col0 = tmem + lane_off + static_cast<uint32_t>(buf * 2 * N);
+            const long long base = blk * static_cast<long long>(NB) * P.outer;
+            int8_t* o_lo = P.out[PL_LO] + base;
+            int8_t* o_hi = P.out[PL_HI] + base;
+            int8_t* o_nlo = P.out[PL_NLO] + base;
+            int8_t* o_nhi = P.out[PL_NHI] + base;
+            for (int c = half_id; c < chunks; c += EPQ) {
+                const int o0 = c * 16;
+                if (c != half_id) load_diag(c);
+                int32_t ll[16], lh[16], hl[16], hh[16];
+                tc::tmem_ld16(col0 + o0, ll);
+                tc::tmem_ld16(col0 + P.half + o0, lh);
+                tc::tmem_ld16(col0 + N + o0, hl);
+                tc::tmem_ld16(col0 + N + P.half + o0, hh);
+                tc::tmem_ld_wait();
+                uint32_t lw[4] = {0, 0, 0, 0}, hw[4] = {0, 0, 0, 0};
+#pragma unroll
+                for (int oo = 0; oo < 16; ++oo) {
+                    int32_t v = combine(ll[oo], lh[oo] + hl[oo], hh[oo], P.mod, P.c1, P.c2);
+                    if (P.diag) v = reduce_balanced(v * dg[oo], P.mod);
+                    int8_t lo, hi;
+                    split_limbs(v, lo, hi);
+                    lw[oo >> 2] |= static_cast<uint32_t>(static_cast<uint8_t>(lo)) << (8 * (oo & 3));
+                    hw[oo >> 2] |= static_cast<uint32_t>(static_cast<uint8_t>(hi)) << (8 * (oo & 3));
+                }
+                transpose16(lw, lane);
+                transpose16(hw, lane);
+                const int o = o0 + (lane & 15);
+                if (valid && o < P.outer) {
+                    const uint32_t off = h_off + static_cast<uint32_t>(o) * 16u;
+                    *reinterpret_cast<uint4*>(o_lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                    *reinterpret_cast<uint4*>(o_hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    *reinterpret_cast<uint4*>(o_nlo + off) = make_uint4(__vsub4(0u, lw[0]), __vsub4(0u, lw[1]),
+                                                                        __vsub4(0u, lw[2]), __vsub4(0u, lw[3]));
+                    *reinterpret_cast<uint4*>(o_nhi + off) = make_uint4(__vsub4(0u, hw[0]), __vsub4(0u, hw[1]),
+                                                                        __vsub4(0u, hw[2]), __vsub4(0u, hw[3]));
+                }
+            }
+            tc::tc_fence_before();
+            tc::mbar_arrive(&accempty[buf]);
+        }
+    }
+
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, tmem_cols);
+    }
+}
+
 // ---- limb conversions and the projection on limb planes
 
 // canonical row-major (rows = n_blk * dim, w_in columns) -> four planes of NB
@@ -725,10 +993,15 @@ struct KoszulCtx::I8State {
         I8Dir p{};
         int8_t* b_tiles = nullptr;
         uint32_t* inc = nullptr;
+        int4* rows4 = nullptr;     // TMA gather rows per group of four generators
+        bool gather4 = false;      // stages filled by TMA gathers (else cp.async warps)
         size_t smem = 0;
         unsigned grid = 0;
     } fwd, bwd;
-    int8_t* planes[3][4] = {};     // Y_a, Y_b, Z: lo, hi, -lo, -hi
+    // Y_a, Y_b, Z: lo, hi, -lo, -hi; each -plane directly follows its +plane in
+    // memory, so that one tensor map covers both signs of a limb
+    int8_t* planes[3][4] = {};
+    CUtensorMap maps[3][2];        // [block array][limb]: rows = (sign, block, h) runs
     I8Proj proj{};             // projection plan (X tiles, stage shape, grid)
     int8_t* xt = nullptr;
     size_t proj_smem = 0;
@@ -739,7 +1012,15 @@ struct KoszulCtx::I8State {
 namespace {
 
 // Plans one direction: stage size, pipeline depth, B operand (host layout).
-void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int outer, bool transpose_maps) {
+//
+// A generator spans `inner_pad` K' rows (inner, rounded up to even for the TMA
+// gather producer so that every group of four generators starts 128-byte
+// aligned).  A stage holds `gps` generators (gather producer: gs groups of
+// four), padded to whole K-steps of 32 rows; B is zero in every padding row
+// and for every generator past r, so the A rows there may hold anything.
+// Returns false when the maps and stages do not fit in shared memory.
+bool plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int outer, bool transpose_maps,
+                    bool gather4) {
     I8Dir& P = D.p;
     P.r = c.r;
     P.inner = inner;
@@ -747,53 +1028,83 @@ void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     P.half = (outer + 15) / 16 * 16;
     const int N = 2 * P.half;
     BW_REQUIRE(N <= 256, "INT8 form: output dimension above 128 is not supported");
-    // Stage = gi generators: gi * inner K' rows, padded to whole K-steps of 32
-    // (the padding rows of B are zero, so the A rows there may hold anything).
-    // Pick the best-filled stage of at most 56 KB of A per slot, the largest
-    // such gi on ties.
-    int gi = 1;
-    double best_fill = -1;
-    for (int g = 1; g <= c.r; ++g) {
-        const int rows = g * inner, padded = (rows + 31) / 32 * 32;
-        if (g > 1 && static_cast<size_t>(2) * 8 * padded * 16 > 56 * 1024) break;
-        const double fill = static_cast<double>(rows) / padded;
-        if (fill > best_fill - 1e-9) {
-            best_fill = std::max(best_fill, fill);
-            gi = g;
+    const size_t extra = (2 * 8 + 2 * 2 + 1) * 8 + 16 + (gather4 ? 0 : kMaxRowTable);
+    const int inner_pad = gather4 ? inner + (inner & 1) : inner;
+    auto b_bytes_of = [&](int gps) {
+        const int stages = (c.r + gps - 1) / gps;
+        const int ks_full = (gps * inner_pad + 31) / 32;
+        const int last = c.r - (stages - 1) * gps;
+        const int last_rows = gather4 ? (last + 3) / 4 * 4 * inner_pad : last * inner_pad;
+        return static_cast<size_t>((stages - 1) * ks_full + (last_rows + 31) / 32) * N * 32;
+    };
+    int gps = 0;
+    if (gather4) {
+        // groups of four generators per stage: the best-filled choice that
+        // leaves at least three pipeline slots, the fewer stages on ties
+        P.groups = (c.r + 3) / 4;
+        double best = -1;
+        for (int gs = 1; gs <= P.groups; ++gs) {
+            const int rows = gs * 4 * inner_pad, padded = (rows + 31) / 32 * 32;
+            const size_t slot = static_cast<size_t>(2) * 8 * padded * 16;
+            const size_t bb = b_bytes_of(4 * gs);
+            if (bb + 3 * slot + extra > static_cast<size_t>(kMaxSmem)) break;
+            const double fill = static_cast<double>(rows) / padded;
+            if (fill > best + 1e-9) {
+                best = fill;
+                gps = 4 * gs;
+            }
         }
+        if (gps == 0) return false;
+        P.gs = gps / 4;
+    } else {
+        // the best-filled stage of at most 56 KB of A per slot, the largest such on ties
+        double best_fill = -1;
+        for (int g = 1; g <= c.r; ++g) {
+            const int rows = g * inner, padded = (rows + 31) / 32 * 32;
+            if (g > 1 && static_cast<size_t>(2) * 8 * padded * 16 > 56 * 1024) break;
+            const double fill = static_cast<double>(rows) / padded;
+            if (fill > best_fill - 1e-9) {
+                best_fill = std::max(best_fill, fill);
+                gps = g;
+            }
+        }
+        BW_REQUIRE(gps * inner <= kMaxRowTable, "INT8 form: stage too deep for the row table");
     }
-    P.gi = gi;
-    P.stages_per_tile = (c.r + gi - 1) / gi;
-    P.ks_full = (gi * inner + 31) / 32;
-    const int last_g = c.r - (P.stages_per_tile - 1) * gi;
-    P.ks_last = (last_g * inner + 31) / 32;
+    P.inner_pad = inner_pad;
+    P.gi = gps;
+    P.stages_per_tile = (c.r + gps - 1) / gps;
+    P.ks_full = (gps * inner_pad + 31) / 32;
+    const int last_g = c.r - (P.stages_per_tile - 1) * gps;
+    const int last_rows = gather4 ? (last_g + 3) / 4 * 4 * inner_pad : last_g * inner_pad;
+    P.ks_last = (last_rows + 31) / 32;
     const int total_ks = (P.stages_per_tile - 1) * P.ks_full + P.ks_last;
     P.b_bytes = static_cast<uint32_t>(total_ks) * N * 32;
     P.limb_bytes = static_cast<uint32_t>(8 * P.ks_full * 32 * 16);
     P.slot_bytes = 2 * P.limb_bytes;
-    BW_REQUIRE(gi * inner <= kMaxRowTable, "INT8 form: stage too deep for the row table");
-    const size_t extra = (2 * 8 + 2 * 2 + 1) * 8 + 16 + kMaxRowTable;
-    int slots = 4;
+    P.tx_full = static_cast<uint32_t>(16 * gps * inner_pad * 16);              // 2 limbs x 8 columns x rows x 16 B
+    P.tx_last = static_cast<uint32_t>(16 * ((last_g + 3) / 4 * 4) * inner_pad * 16);
+    int slots = gather4 ? 8 : 4;
     while (slots > 1 && P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra > static_cast<size_t>(kMaxSmem))
         --slots;
-    BW_REQUIRE(P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra <= static_cast<size_t>(kMaxSmem),
-               "INT8 form: maps too large for shared memory");
+    if (P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra > static_cast<size_t>(kMaxSmem)) return false;
     P.slots = slots;
     D.smem = P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra;
+    D.gather4 = gather4;
     P.mod = c.mod;
     P.c1 = to_balanced(255u % c.p, c.mod);
     P.c2 = to_balanced(static_cast<uint32_t>((255ull * 255ull) % c.p), c.mod);
 
     // B: row n < half -> lo limb, n >= half -> hi limb of map coefficient (o = n mod half),
-    // column K' = i * inner + u; K-major, 8x16-byte core matrices, LBO 128, SBO 256.
+    // column K' = stage row base + (generator in stage) * inner_pad + u; K-major,
+    // 8x16-byte core matrices, LBO 128, SBO 256.
     std::vector<int8_t> B(P.b_bytes, 0);
     const int kp_total = total_ks * 32;
     for (int kp = 0; kp < kp_total; ++kp) {
         const int s = std::min(kp / (P.ks_full * 32), P.stages_per_tile - 1);
         const int local = kp - s * P.ks_full * 32;
-        const int gen_local = local / inner, u = local % inner;
-        const int i = s * gi + gen_local;
-        if (gen_local >= (s == P.stages_per_tile - 1 ? last_g : gi)) continue;   // padding
+        const int gen_local = local / inner_pad, u = local % inner_pad;
+        const int i = s * gps + gen_local;
+        if (u >= inner || gen_local >= (s == P.stages_per_tile - 1 ? last_g : gps) || i >= c.r) continue;   // padding
         for (int n = 0; n < N; ++n) {
             const int o = n % P.half;
             if (o >= outer) continue;
@@ -812,6 +1123,60 @@ void plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     BW_CUDA(cudaMemcpyAsync(D.b_tiles, B.data(), B.size(), cudaMemcpyHostToDevice, c.own_stream));
     BW_CUDA(cudaStreamSynchronize(c.own_stream));
     P.b_tiles = D.b_tiles;
+    return true;
+}
+
+// Rows of the TMA gathers: for output block blk and group g (generators
+// 4g..4g+3), the plane row of each generator's neighbour run at h = 0:
+// neg * n_blk_in * HG + nbr * HG, or one past the last row (zero-filled) for an
+// absent generator or one past r.
+std::vector<int4> gather_rows(const std::vector<uint32_t>& inc, uint64_t n_blk, int r, uint64_t n_blk_in, int hg) {
+    const int groups = (r + 3) / 4;
+    const int64_t oob = static_cast<int64_t>(2 * n_blk_in * hg);
+    BW_REQUIRE(oob + hg < (1ll << 31), "INT8 form: plane rows above the TMA coordinate range");
+    std::vector<int4> out(n_blk * groups);
+    for (uint64_t b = 0; b < n_blk; ++b)
+        for (int g = 0; g < groups; ++g) {
+            int32_t v[4];
+            for (int q = 0; q < 4; ++q) {
+                const int i = 4 * g + q;
+                const uint32_t e = i < r ? inc[b * r + i] : kAbsent;
+                v[q] = static_cast<int32_t>(e == kAbsent ? oob
+                                                         : static_cast<int64_t>(e >> 31) * n_blk_in * hg +
+                                                               static_cast<int64_t>(e & 0x7FFFFFFFu) * hg);
+            }
+            out[b * groups + g] = make_int4(v[0], v[1], v[2], v[3]);
+        }
+    return out;
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// One limb of a block array as a 2-D tensor for the gathers: rows = the
+// (sign, block, h) runs of dim * 16 bytes (the -plane's rows after the
+// +plane's), 8-byte elements; box = one run of dim_pad * 16 bytes.
+void encode_plane_map(CUtensorMap* map, const int8_t* base, uint64_t n_blk, int dim, int dim_pad, int hg) {
+    static const EncodeTiledFn encode = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    BW_REQUIRE(encode != nullptr, "INT8 form: cuTensorMapEncodeTiled is not available from the driver");
+    BW_REQUIRE(reinterpret_cast<uintptr_t>(base) % 16 == 0, "INT8 form: plane not 16-byte aligned");
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(2 * dim), static_cast<cuuint64_t>(2 * n_blk * hg)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(dim) * 16};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(2 * dim_pad), 1};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult rc = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<int8_t*>(base), dims, strides, box,
+                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    BW_REQUIRE(rc == CUDA_SUCCESS, "INT8 form: cuTensorMapEncodeTiled failed (code " + std::to_string(rc) + ")");
 }
 
 // Projection stage shape: SB whole source blocks per stage, KP = SB * dim
@@ -867,8 +1232,11 @@ void plan_projection(KoszulCtx& c, KoszulCtx::I8State& S) {
 }
 
 template <int NB>
-void launch_i8(KoszulCtx& c, KoszulCtx::I8State::Dir& D, cudaStream_t st) {
-    i8_gather_gemm_kernel<NB><<<D.grid, kI8Threads, D.smem, st>>>(D.p);
+void launch_i8(KoszulCtx& c, KoszulCtx::I8State::Dir& D, const CUtensorMap* maps, cudaStream_t st) {
+    if (D.gather4)
+        i8_gather4_kernel<NB><<<D.grid, kG4Threads, D.smem, st>>>(maps[0], maps[1], D.p);
+    else
+        i8_gather_gemm_kernel<NB><<<D.grid, kI8Threads, D.smem, st>>>(D.p);
     BW_CHECK_LAUNCH();
     ++c.launches;
 }
@@ -913,17 +1281,60 @@ void KoszulCtx::i8_setup() {
             bwd[s * r + Sx[pos]] = static_cast<uint32_t>(lex_rank(T, r, k - 1)) | ((pos & 1) ? 0x80000000u : 0u);
         }
     }
-    S.fwd.inc = alloc<uint32_t>(fwd.size());
-    S.bwd.inc = alloc<uint32_t>(bwd.size());
-    BW_CUDA(cudaMemcpyAsync(S.fwd.inc, fwd.data(), fwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
-    BW_CUDA(cudaMemcpyAsync(S.bwd.inc, bwd.data(), bwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
-    for (int b = 0; b < 3; ++b)
-        for (int pl = 0; pl < 4; ++pl) S.planes[b][pl] = alloc<int8_t>((b < 2 ? n_src : n_tgt) * nbi);
+    // each limb's -plane directly after its +plane (one tensor map covers both signs)
+    for (int b = 0; b < 3; ++b) {
+        const uint64_t plane = (b < 2 ? n_src : n_tgt) * nbi;
+        for (int limb = 0; limb < 2; ++limb) {
+            int8_t* pair = alloc<int8_t>(2 * plane);
+            S.planes[b][limb] = pair;
+            S.planes[b][limb + 2] = pair + plane;
+        }
+    }
     S.err = alloc<int>(1);
     BW_CUDA(cudaMemsetAsync(S.err, 0, sizeof(int), own_stream));
     plan_projection(*this, S);
-    plan_direction(*this, S.fwd, ci, co, false);
-    plan_direction(*this, S.bwd, co, ci, true);
+    // Stages are filled by TMA gathers (tile::gather4) unless the plan does not
+    // fit or BW_I8_PRODUCER=cpasync asks for the cp.async producer warps.
+    bool gather4 = true;
+    if (const char* e = std::getenv("BW_I8_PRODUCER")) gather4 = std::string(e) != "cpasync";
+    for (int dir = 0; dir < 2; ++dir) {
+        I8State::Dir& D = dir == 0 ? S.fwd : S.bwd;
+        const int inner = dir == 0 ? ci : co, outer = dir == 0 ? co : ci;
+        if (!(gather4 && plan_direction(*this, D, inner, outer, dir == 1, true)))
+            BW_REQUIRE(plan_direction(*this, D, inner, outer, dir == 1, false),
+                       "INT8 form: maps too large for shared memory");
+    }
+    const int hg = nbi / 16;
+    if (S.fwd.gather4 || S.bwd.gather4) {
+        for (int b = 0; b < 3; ++b) {
+            const uint64_t n_blk = b < 2 ? n_s : n_t;
+            const int dim = b < 2 ? ci : co;
+            for (int limb = 0; limb < 2; ++limb)
+                encode_plane_map(&S.maps[b][limb], S.planes[b][limb], n_blk, dim, dim + (dim & 1), hg);
+        }
+    }
+    if (S.fwd.gather4) {
+        const std::vector<int4> rows = gather_rows(fwd, n_t, r, n_s, hg);
+        S.fwd.rows4 = alloc<int4>(rows.size());
+        BW_CUDA(cudaMemcpyAsync(S.fwd.rows4, rows.data(), rows.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                                own_stream));
+        BW_CUDA(cudaStreamSynchronize(own_stream));
+    } else {
+        S.fwd.inc = alloc<uint32_t>(fwd.size());
+        BW_CUDA(cudaMemcpyAsync(S.fwd.inc, fwd.data(), fwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
+        BW_CUDA(cudaStreamSynchronize(own_stream));
+    }
+    if (S.bwd.gather4) {
+        const std::vector<int4> rows = gather_rows(bwd, n_s, r, n_t, hg);
+        S.bwd.rows4 = alloc<int4>(rows.size());
+        BW_CUDA(cudaMemcpyAsync(S.bwd.rows4, rows.data(), rows.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                                own_stream));
+        BW_CUDA(cudaStreamSynchronize(own_stream));
+    } else {
+        S.bwd.inc = alloc<uint32_t>(bwd.size());
+        BW_CUDA(cudaMemcpyAsync(S.bwd.inc, bwd.data(), bwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
+        BW_CUDA(cudaStreamSynchronize(own_stream));
+    }
     // Failure tests only (the environment of the creating process): a short
     // limit on every pipeline wait, and a first stage that CTA 0 of the d/d^T
     // kernel never fills, so that its consumer's wait runs out and the kernel
@@ -943,14 +1354,20 @@ void KoszulCtx::i8_setup() {
     S.proj.wait_limit = wait_limit;
     S.fwd.p.inc = S.fwd.inc;
     S.bwd.p.inc = S.bwd.inc;
+    S.fwd.p.rows4 = S.fwd.rows4;
+    S.bwd.p.rows4 = S.bwd.rows4;
     S.fwd.p.n_blk = static_cast<long long>(n_t);
     S.bwd.p.n_blk = static_cast<long long>(n_s);
+    S.fwd.p.row_oob = static_cast<int32_t>(2 * n_s * hg);   // the forward gathers Y (source blocks)
+    S.bwd.p.row_oob = static_cast<int32_t>(2 * n_t * hg);   // d^T gathers Z (target blocks)
     dispatch_i8_nb(nbi, [&](auto NBc) {
         const int cap_g = allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value>, device);
+        const int cap_4 = allow_dynamic_smem(i8_gather4_kernel<decltype(NBc)::value>, device);
         const int cap_p = allow_dynamic_smem(i8_project_tc_kernel<decltype(NBc)::value>, device);
-        BW_REQUIRE(static_cast<int>(std::max(S.fwd.smem, S.bwd.smem)) <= cap_g &&
-                       static_cast<int>(S.proj_smem) <= cap_p,
-                   "INT8 form: shared-memory plan above the device limit");
+        for (const I8State::Dir* D : {&S.fwd, &S.bwd})
+            BW_REQUIRE(static_cast<int>(D->smem) <= (D->gather4 ? cap_4 : cap_g),
+                       "INT8 form: shared-memory plan above the device limit");
+        BW_REQUIRE(static_cast<int>(S.proj_smem) <= cap_p, "INT8 form: shared-memory plan above the device limit");
     });
     const int bt = 128 / nbi;
     S.fwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_t + bt - 1) / bt, sms)));
@@ -967,7 +1384,7 @@ void KoszulCtx::i8_run(bool forward_dir, int in_buf, int out_buf, bool scale, cu
         D.p.out[pl] = i8->planes[out_buf][pl];
     }
     D.p.diag = (!forward_dir && scale) ? d_diag : nullptr;
-    dispatch_i8_nb(nbi, [&](auto NBc) { launch_i8<decltype(NBc)::value>(*this, D, st); });
+    dispatch_i8_nb(nbi, [&](auto NBc) { launch_i8<decltype(NBc)::value>(*this, D, i8->maps[in_buf], st); });
 }
 
 void KoszulCtx::i8_check_error() {
@@ -979,8 +1396,9 @@ void KoszulCtx::i8_check_error() {
                                             "ERR_WAIT_EMPTY: producer waited for a free stage",
                                             "ERR_WAIT_ACCUM: epilogue waited for an accumulator",
                                             "ERR_WAIT_ACCUM_FREE: MMA waited for a free accumulator",
-                                            "ERR_WAIT_FINAL: final drain of in-flight MMAs"};
-        const std::string what = (err >= 1 && err <= 5) ? names[err] : "code " + std::to_string(err);
+                                            "ERR_WAIT_FINAL: final drain of in-flight MMAs",
+                                            "ERR_LAYOUT: shared-memory layout check failed"};
+        const std::string what = (err >= 1 && err <= 6) ? names[err] : "code " + std::to_string(err);
         throw Error("INT8 tensor-core kernel gave up waiting (" + what + ")", 2);
     }
 }

@@ -21,6 +21,7 @@ enum WaitError : int {
     ERR_WAIT_ACCUM = 3,     // epilogue waited for an accumulator
     ERR_WAIT_ACCUM_FREE = 4,// MMA waited for the epilogue to free an accumulator
     ERR_WAIT_FINAL = 5,     // final drain of in-flight MMAs
+    ERR_LAYOUT = 6,         // shared-memory layout check failed before any copy was issued
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -83,6 +84,25 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                      smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
+}
+
+// TMA gather of four rows of a 2-D tensor map (sm_100 tile::gather4): rows
+// y0..y3 (any order; a row outside the tensor is filled with zeros and read
+// from nowhere), columns from x for the map's box width, written back to back
+// at dst (128-byte aligned shared memory of this CTA), completing on `bar`
+// (tx bytes = 4 x box bytes).  No multicast: the map covers this GPU's memory.
+__device__ __forceinline__ void tma_gather4(void* dst, const void* tmap, int32_t x, int32_t y0, int32_t y1,
+                                            int32_t y2, int32_t y3, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y0), "r"(y1), "r"(y2), "r"(y3), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Prefetch a tensor map (kernel parameter) into the descriptor cache.
+__device__ __forceinline__ void prefetch_tmap(const void* tmap) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
 }
 
 // 16-byte asynchronous copy global -> shared through L2 (cp.async.cg).

@@ -1,5 +1,8 @@
 """Multi-process plumbing on CPU (gloo, world size 2): per-rank seeds and sector
-shares, and the maximum over ranks that every multi-GPU bench figure uses."""
+shares, the maximum over ranks that every multi-GPU bench figure uses, and
+sector sharding with real engine output: each rank opens host-only contexts
+for its share of the g12 sectors and writes their row-mixing sidecars; the
+union of the ranks' files equals one process's files byte for byte."""
 import multiprocessing as mp
 import os
 import socket
@@ -51,3 +54,58 @@ def test_two_gloo_ranks():
 def test_single_process_is_identity():
     assert sharding.max_over_ranks([3.5]) == [3.5]
     assert sharding.assign_sectors(4, 1, 0) == [0, 1, 2, 3]
+
+
+
+def _sidecar_worker(rank, world_size, port, out_dir, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world_size),
+                      LOCAL_RANK=str(rank))
+    import torch.distributed as dist
+    from datetime import timedelta
+    from pathlib import Path
+    from prym_green_ancillary_b200 import CyclicEngine
+    dist.init_process_group("gloo", rank=rank, world_size=world_size, timeout=timedelta(seconds=60))
+    try:
+        instance = Path(__file__).resolve().parent / "golden" / "g12_p661.json"
+        written = []
+        for sector in sharding.assign_sectors(6, world_size, rank):   # g12 has 6 sectors
+            with CyclicEngine(instance, sector, device=-1) as eng:
+                wdm = eng.output_path(out_dir)
+                eng.write_sidecar(wdm)
+                written.append(Path(wdm).name)
+        dist.barrier()
+        out.put((rank, written))
+    finally:
+        dist.destroy_process_group()
+
+
+def _sidecars(directory):
+    from pathlib import Path
+    return {f.name: f.read_text().replace(str(directory), "<out>")
+            for f in sorted(Path(directory).glob("*.rowmix.json"))}
+
+
+def test_sector_shards_write_the_single_process_sidecars(tmp_path):
+    from pathlib import Path
+    from prym_green_ancillary_b200 import CyclicEngine
+    instance = Path(__file__).resolve().parent / "golden" / "g12_p661.json"
+    single = tmp_path / "single"
+    for sector in range(6):
+        with CyclicEngine(instance, sector, device=-1) as eng:
+            eng.write_sidecar(eng.output_path(single))
+    sharded = tmp_path / "sharded"
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sidecar_worker, args=(r, 2, port, str(sharded), q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = sorted(q.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, files0), (r1, files1) = results
+    assert files0 and files1 and not set(files0) & set(files1)   # disjoint shares, both ranks did work
+    want = _sidecars(single)
+    assert len(want) == 6
+    assert _sidecars(sharded) == want
