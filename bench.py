@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["config3"] + sorted(PAPER), default="config2")
     ap.add_argument("--sector", type=int, default=0, help="paper workloads: the sector")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--min-ms", type=float, default=1000.0,
+                    help="timed regions of K steps repeat until they add up to this much device time "
+                         "(0: one region; for profiling runs)")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the other form and (config2) the config-5 figures")
     args = ap.parse_args()
@@ -416,6 +419,20 @@ def run_batch(args):
     torch.cuda.synchronize()
     (ms,) = max_over_ranks([ms], device=dev)
 
+    # Each sector alone (its own 16-step graphs, no other sector beside it):
+    # the sum of these step times against the batch step shows what running
+    # the sectors side by side in one graph gains or loses.
+    alone_ms = []
+    for i, e in enumerate(batch.engines):
+        e.seq_start(xs[i], ys[i], seqs[i], stream=stream)
+        e.seq_step(16, stream=stream)
+        ev0.record(stream)
+        e.seq_step(16, stream=stream)
+        ev1.record(stream)
+        e.seq_finish(stream=stream)
+        torch.cuda.synchronize()
+        alone_ms.append(ev0.elapsed_time(ev1) / 16)
+
     # End to end: X and Y0 of every sector from pinned host memory, sequences back, K batch steps.
     xh = [torch.empty(x.shape, dtype=torch.int32, pin_memory=True).copy_(x) for x in xs]
     yh = [torch.empty(y.shape, dtype=torch.int32, pin_memory=True).copy_(y) for y in ys]
@@ -465,6 +482,9 @@ def run_batch(args):
             "step": "one batch step advances all sectors by one step; value counts sector-steps "
                     "(batch steps/s x sectors)",
             "batch_steps_per_s": world * K / (ms / 1e3),
+            "plans": [e.plan for e in batch.engines],
+            "sector_alone_ms_per_step": [round(v, 4) for v in alone_ms],
+            "sum_alone_ms_per_step": sum(alone_ms),
             "parallelism": f"replicas{world}" if world > 1 else "single",
             "l2": "working set per batch step far exceeds the 126 MB L2; no flush needed",
             "step_bytes": step_bytes, "step_macs": macs,
@@ -600,7 +620,7 @@ def timed_reps(run_k, stream, world, dev, min_ms=1000.0, max_reps=256):
     return [region() for _ in range(reps)]
 
 
-def time_form(sh, seed, form, K, W, dev, stream, world, local, kernel_steps=16, sampler=None):
+def time_form(sh, seed, form, K, W, dev, stream, world, local, kernel_steps=16, sampler=None, min_ms=1000.0):
     """Engine of one form on a seeded workload: median device ms of K-step regions.
 
     Returns a dict with the engine still open under "engine" (the caller
@@ -633,14 +653,16 @@ def time_form(sh, seed, form, K, W, dev, stream, world, local, kernel_steps=16, 
     launches = eng.launch_count - l0
     if sampler is not None:
         with sampler:
-            reps = timed_reps(lambda: eng.seq_step(K, stream=stream), stream, world, dev, max_reps=max_reps)
+            reps = timed_reps(lambda: eng.seq_step(K, stream=stream), stream, world, dev, min_ms=min_ms,
+                              max_reps=max_reps)
     else:
-        reps = timed_reps(lambda: eng.seq_step(K, stream=stream), stream, world, dev, max_reps=max_reps)
+        reps = timed_reps(lambda: eng.seq_step(K, stream=stream), stream, world, dev, min_ms=min_ms,
+                          max_reps=max_reps)
     kern_ms = eng.seq_step_timed(kernel_steps, stream=stream)
     eng.seq_finish(stream=stream)
     torch.cuda.synchronize()
     return dict(engine=eng, x=x, y=y, reps=reps, ms=statistics.median(reps), launches=launches,
-                kernel_ms=kern_ms)
+                kernel_ms=kern_ms, plan=eng.plan)
 
 
 def run_engine(args):
@@ -665,7 +687,7 @@ def run_engine(args):
     stream = torch.cuda.Stream(device=dev)
 
     clocks = ClockSampler(local)
-    run = time_form(sh, seed, form, K, W, dev, stream, world, local, sampler=clocks)
+    run = time_form(sh, seed, form, K, W, dev, stream, world, local, sampler=clocks, min_ms=args.min_ms)
     eng = run["engine"]
     (ms,) = max_over_ranks([run["ms"]], device=dev)
     value = world * K / (ms / 1e3)
@@ -680,7 +702,7 @@ def run_engine(args):
     xh_np, yh_np = xh.numpy().view(np.uint32), yh.numpy().view(np.uint32)
     seq_h, yf_h = eng.sequence_host(xh_np, yh_np, K + 1)
     e2e_calls = []
-    while sum(e2e_calls) < 1.0 or len(e2e_calls) < 3:
+    while sum(e2e_calls) < args.min_ms / 1e3 or len(e2e_calls) < 3:
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -707,11 +729,12 @@ def run_engine(args):
     other = "plain" if form == "int8" else "int8"
     extras = {}
     if not args.no_compare:
-        o = time_form(sh, seed, other, K, W, dev, stream, world, local)
+        o = time_form(sh, seed, other, K, W, dev, stream, world, local, min_ms=args.min_ms)
         o["engine"].close()
         (o_ms,) = max_over_ranks([o["ms"]], device=dev)
         extras[other] = dict(value=world * K / (o_ms / 1e3), ms_per_step=o_ms / K, reps=len(o["reps"]),
-                             kernel_ms=dict(zip(["forward", "transpose", "projection"], o["kernel_ms"])))
+                             kernel_ms=dict(zip(["forward", "transpose", "projection"], o["kernel_ms"])),
+                             plan=o["plan"])
         del o
         torch.cuda.empty_cache()
     big = {}
@@ -720,11 +743,13 @@ def run_engine(args):
         seed5 = rank_seed(sh5["seed"], rank)
         K5 = min(K, 20)
         for f in ("int8", "plain"):
-            r5 = time_form(sh5, seed5, f, K5, min(W, 3), dev, stream, world, local, kernel_steps=2)
+            r5 = time_form(sh5, seed5, f, K5, min(W, 3), dev, stream, world, local, kernel_steps=2,
+                           min_ms=args.min_ms)
             r5["engine"].close()
             (ms5,) = max_over_ranks([r5["ms"]], device=dev)
             big[f] = dict(value=world * K5 / (ms5 / 1e3), ms_per_step=ms5 / K5, steps=K5, reps=len(r5["reps"]),
-                          kernel_ms=dict(zip(["forward", "transpose", "projection"], r5["kernel_ms"])))
+                          kernel_ms=dict(zip(["forward", "transpose", "projection"], r5["kernel_ms"])),
+                          plan=r5["plan"])
             del r5
             torch.cuda.empty_cache()
 
@@ -756,6 +781,7 @@ def run_engine(args):
             "data": "synthetic (seeded uniform residues, counter-based stream)",
             "config": workload_config(args.workload),
             "form": form,
+            "plan": run["plan"],
             "parallelism": f"replicas{world}" if world > 1 else "single",
             "l2": "working set per step (X, Y, Z, S Y) exceeds the 126 MB L2; no flush needed",
             "timing": {"regions": len(run["reps"]), "steps_per_region": K,

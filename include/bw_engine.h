@@ -140,6 +140,15 @@ BW_API int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* ms_ou
 /* Number of engine kernel launches issued by this context since creation. */
 BW_API uint64_t bw_koszul_launch_count(const bw_koszul* ctx);
 
+/* The context's kernel plan as text: for the INT8 form, each direction's
+ * producer (TMA gathers or cp.async warps), generators per stage, pipeline
+ * slots and shared memory, with the set-up autotuner's timing of every
+ * candidate when it ran (a shape already tuned in this process reuses the
+ * choice), and the projection's stage.  No reference counterpart (the
+ * reference has one fixed kernel configuration per block width,
+ * cuda/cyclic_cuda_helpers.h:552-631). */
+BW_API int bw_koszul_plan(const bw_koszul* ctx, char* buf, size_t cap);
+
 /* Batch of synthetic operators ("sectors" of uneven shapes, block widths and
  * forms) whose sequences advance together: every batch step advances every
  * sector by one step, and 16 steps of all sectors run as one CUDA graph with

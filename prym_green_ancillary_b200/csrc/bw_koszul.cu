@@ -774,6 +774,18 @@ extern "C" int bw_koszul_sequence_host(bw_koszul* ctx, const uint32_t* h_x, cons
     });
 }
 
+extern "C" int bw_koszul_plan(const bw_koszul* ctx, char* buf, size_t cap) {
+    return guarded([&] {
+        BW_ARG(ctx && buf && cap > 0, "bw_koszul_plan: null argument");
+        const KoszulCtx& c = *ctx->impl;
+        const std::string text = c.form == BW_FORM_INT8 ? c.i8_plan_text()
+                                                        : std::string("plain: one CTA per 16 output rows, maps in "
+                                                                      "shared memory");
+        BW_ARG(text.size() < cap, "bw_koszul_plan: buffer too small");
+        std::memcpy(buf, text.c_str(), text.size() + 1);
+    });
+}
+
 extern "C" int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* ms_out, void* stream) {
     return guarded([&] {
         BW_ARG(ctx != nullptr && ms_out != nullptr, "bw_koszul_seq_step_timed: null argument");

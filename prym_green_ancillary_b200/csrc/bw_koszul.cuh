@@ -5,6 +5,7 @@
 #include "../../include/bw_engine.h"
 
 #include <memory>
+#include <string>
 #include <vector>
 
 namespace bw {
@@ -85,6 +86,8 @@ struct KoszulCtx {
     enum { I8_YA = 0, I8_YB = 1, I8_Z = 2 };   // limb-plane block arrays
     void i8_run(bool forward_dir, int in_buf, int out_buf, bool scale, cudaStream_t st);
     void i8_check_error();
+    double i8_time_direction(bool forward_dir, int in_buf, int out_buf);
+    const std::string& i8_plan_text() const;
     void i8_to_limbs(const uint32_t* in, int buf, cudaStream_t st);
     void i8_from_limbs(int buf, uint32_t* out, cudaStream_t st);
     void i8_load_x(const uint32_t* x, cudaStream_t st);

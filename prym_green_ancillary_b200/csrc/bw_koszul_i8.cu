@@ -52,9 +52,13 @@
 #include <cuda.h>   // CUtensorMap and cuTensorMapEncodeTiled's types (the function is reached through the runtime)
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 namespace bw {
@@ -1002,6 +1006,7 @@ struct KoszulCtx::I8State {
     // memory, so that one tensor map covers both signs of a limb
     int8_t* planes[3][4] = {};
     CUtensorMap maps[3][2];        // [block array][limb]: rows = (sign, block, h) runs
+    std::string plan_text;         // the chosen stage plans and the autotuner's timings
     I8Proj proj{};             // projection plan (X tiles, stage shape, grid)
     int8_t* xt = nullptr;
     size_t proj_smem = 0;
@@ -1010,6 +1015,36 @@ struct KoszulCtx::I8State {
 };
 
 namespace {
+
+// Autotuner cache: the chosen producer and stage size per operator shape and
+// device, shared by every context of the process.
+struct TuneKey {
+    int r, k, inner, outer, nbi, dir, sms, allowed;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(r, k, inner, outer, nbi, dir, sms, allowed) <
+               std::tie(o.r, o.k, o.inner, o.outer, o.nbi, o.dir, o.sms, o.allowed);
+    }
+};
+struct TuneChoice {
+    bool gather4 = false;
+    int gps = 0;
+    double ms = 0;
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, TuneChoice> g_tune_cache;
+
+bool tune_lookup(const TuneKey& k, TuneChoice& out) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    const auto it = g_tune_cache.find(k);
+    if (it == g_tune_cache.end()) return false;
+    out = it->second;
+    return true;
+}
+
+void tune_store(const TuneKey& k, const TuneChoice& c) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[k] = c;
+}
 
 // Plans one direction: stage size, pipeline depth, B operand (host layout).
 //
@@ -1020,7 +1055,7 @@ namespace {
 // and for every generator past r, so the A rows there may hold anything.
 // Returns false when the maps and stages do not fit in shared memory.
 bool plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int outer, bool transpose_maps,
-                    bool gather4) {
+                    bool gather4, int gps_forced = 0) {
     I8Dir& P = D.p;
     P.r = c.r;
     P.inner = inner;
@@ -1038,7 +1073,17 @@ bool plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
         return static_cast<size_t>((stages - 1) * ks_full + (last_rows + 31) / 32) * N * 32;
     };
     int gps = 0;
-    if (gather4) {
+    if (gps_forced > 0) {
+        // a stage size chosen by the autotuner (checked below against shared memory)
+        if (gather4 && gps_forced % 4 != 0) return false;
+        gps = std::min(gps_forced, gather4 ? (c.r + 3) / 4 * 4 : c.r);
+        if (gather4) {
+            P.groups = (c.r + 3) / 4;
+            P.gs = gps / 4;
+        } else if (gps * inner > kMaxRowTable) {
+            return false;
+        }
+    } else if (gather4) {
         // groups of four generators per stage: the best-filled choice that
         // leaves at least three pipeline slots, the fewer stages on ties
         P.groups = (c.r + 3) / 4;
@@ -1293,52 +1338,37 @@ void KoszulCtx::i8_setup() {
     S.err = alloc<int>(1);
     BW_CUDA(cudaMemsetAsync(S.err, 0, sizeof(int), own_stream));
     plan_projection(*this, S);
-    // Stages are filled by TMA gathers (tile::gather4) unless the plan does not
-    // fit or BW_I8_PRODUCER=cpasync asks for the cp.async producer warps.
-    bool gather4 = true;
-    if (const char* e = std::getenv("BW_I8_PRODUCER")) gather4 = std::string(e) != "cpasync";
-    for (int dir = 0; dir < 2; ++dir) {
-        I8State::Dir& D = dir == 0 ? S.fwd : S.bwd;
-        const int inner = dir == 0 ? ci : co, outer = dir == 0 ? co : ci;
-        if (!(gather4 && plan_direction(*this, D, inner, outer, dir == 1, true)))
-            BW_REQUIRE(plan_direction(*this, D, inner, outer, dir == 1, false),
-                       "INT8 form: maps too large for shared memory");
-    }
     const int hg = nbi / 16;
-    if (S.fwd.gather4 || S.bwd.gather4) {
-        for (int b = 0; b < 3; ++b) {
-            const uint64_t n_blk = b < 2 ? n_s : n_t;
-            const int dim = b < 2 ? ci : co;
-            for (int limb = 0; limb < 2; ++limb)
-                encode_plane_map(&S.maps[b][limb], S.planes[b][limb], n_blk, dim, dim + (dim & 1), hg);
-        }
-    }
-    if (S.fwd.gather4) {
-        const std::vector<int4> rows = gather_rows(fwd, n_t, r, n_s, hg);
-        S.fwd.rows4 = alloc<int4>(rows.size());
-        BW_CUDA(cudaMemcpyAsync(S.fwd.rows4, rows.data(), rows.size() * sizeof(int4), cudaMemcpyHostToDevice,
-                                own_stream));
+    // Both gather tables (TMA rows per group of four generators, and the
+    // per-generator words of the cp.async producer) until the plans are chosen.
+    auto upload_rows = [&](const std::vector<uint32_t>& inc, uint64_t n_out, uint64_t n_in) {
+        const std::vector<int4> rows = gather_rows(inc, n_out, r, n_in, hg);
+        int4* d = alloc<int4>(rows.size());
+        BW_CUDA(cudaMemcpyAsync(d, rows.data(), rows.size() * sizeof(int4), cudaMemcpyHostToDevice, own_stream));
         BW_CUDA(cudaStreamSynchronize(own_stream));
-    } else {
-        S.fwd.inc = alloc<uint32_t>(fwd.size());
-        BW_CUDA(cudaMemcpyAsync(S.fwd.inc, fwd.data(), fwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
+        return d;
+    };
+    auto upload_inc = [&](const std::vector<uint32_t>& inc) {
+        uint32_t* d = alloc<uint32_t>(inc.size());
+        BW_CUDA(cudaMemcpyAsync(d, inc.data(), inc.size() * 4, cudaMemcpyHostToDevice, own_stream));
         BW_CUDA(cudaStreamSynchronize(own_stream));
-    }
-    if (S.bwd.gather4) {
-        const std::vector<int4> rows = gather_rows(bwd, n_s, r, n_t, hg);
-        S.bwd.rows4 = alloc<int4>(rows.size());
-        BW_CUDA(cudaMemcpyAsync(S.bwd.rows4, rows.data(), rows.size() * sizeof(int4), cudaMemcpyHostToDevice,
-                                own_stream));
-        BW_CUDA(cudaStreamSynchronize(own_stream));
-    } else {
-        S.bwd.inc = alloc<uint32_t>(bwd.size());
-        BW_CUDA(cudaMemcpyAsync(S.bwd.inc, bwd.data(), bwd.size() * 4, cudaMemcpyHostToDevice, own_stream));
-        BW_CUDA(cudaStreamSynchronize(own_stream));
+        return d;
+    };
+    S.fwd.rows4 = upload_rows(fwd, n_t, n_s);
+    S.bwd.rows4 = upload_rows(bwd, n_s, n_t);
+    S.fwd.inc = upload_inc(fwd);
+    S.bwd.inc = upload_inc(bwd);
+    for (int b = 0; b < 3; ++b) {
+        const uint64_t n_blk = b < 2 ? n_s : n_t;
+        const int dim = b < 2 ? ci : co;
+        for (int limb = 0; limb < 2; ++limb)
+            encode_plane_map(&S.maps[b][limb], S.planes[b][limb], n_blk, dim, dim + (dim & 1), hg);
     }
     // Failure tests only (the environment of the creating process): a short
     // limit on every pipeline wait, and a first stage that CTA 0 of the d/d^T
     // kernel never fills, so that its consumer's wait runs out and the kernel
     // gives up, frees its TMEM and returns; the host then reports status 2.
+    // (The hold starts after the set-up's own timing launches.)
     uint32_t wait_limit = tc::kWaitLimit;
     if (const char* e = std::getenv("BW_TEST_WAIT_LIMIT")) {
         const unsigned long v = std::strtoul(e, nullptr, 10);
@@ -1346,33 +1376,128 @@ void KoszulCtx::i8_setup() {
     }
     int hold = 0;
     if (const char* e = std::getenv("BW_TEST_HOLD_FIRST_STAGE")) hold = (*e && std::string(e) != "0") ? 1 : 0;
-    for (I8State::Dir* D : {&S.fwd, &S.bwd}) {
-        D->p.err = S.err;
-        D->p.wait_limit = wait_limit;
-        D->p.hold_first_stage = hold;
-    }
     S.proj.wait_limit = wait_limit;
-    S.fwd.p.inc = S.fwd.inc;
-    S.bwd.p.inc = S.bwd.inc;
-    S.fwd.p.rows4 = S.fwd.rows4;
-    S.bwd.p.rows4 = S.bwd.rows4;
+    int cap_g = 0, cap_4 = 0;
+    dispatch_i8_nb(nbi, [&](auto NBc) {
+        cap_g = allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value>, device);
+        cap_4 = allow_dynamic_smem(i8_gather4_kernel<decltype(NBc)::value>, device);
+        const int cap_p = allow_dynamic_smem(i8_project_tc_kernel<decltype(NBc)::value>, device);
+        BW_REQUIRE(static_cast<int>(S.proj_smem) <= cap_p, "INT8 form: shared-memory plan above the device limit");
+    });
+    const int bt = 128 / nbi;
     S.fwd.p.n_blk = static_cast<long long>(n_t);
     S.bwd.p.n_blk = static_cast<long long>(n_s);
     S.fwd.p.row_oob = static_cast<int32_t>(2 * n_s * hg);   // the forward gathers Y (source blocks)
     S.bwd.p.row_oob = static_cast<int32_t>(2 * n_t * hg);   // d^T gathers Z (target blocks)
-    dispatch_i8_nb(nbi, [&](auto NBc) {
-        const int cap_g = allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value>, device);
-        const int cap_4 = allow_dynamic_smem(i8_gather4_kernel<decltype(NBc)::value>, device);
-        const int cap_p = allow_dynamic_smem(i8_project_tc_kernel<decltype(NBc)::value>, device);
-        for (const I8State::Dir* D : {&S.fwd, &S.bwd})
-            BW_REQUIRE(static_cast<int>(D->smem) <= (D->gather4 ? cap_4 : cap_g),
-                       "INT8 form: shared-memory plan above the device limit");
-        BW_REQUIRE(static_cast<int>(S.proj_smem) <= cap_p, "INT8 form: shared-memory plan above the device limit");
-    });
-    const int bt = 128 / nbi;
     S.fwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_t + bt - 1) / bt, sms)));
     S.bwd.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n_s + bt - 1) / bt, sms)));
+
+    // Stage plans.  Each direction's producer (TMA gathers or cp.async warps)
+    // and stage size are chosen by timing every candidate that fits in shared
+    // memory on this device, at set-up, on the context's own buffers (the
+    // kernels' work does not depend on the values); the choice is cached per
+    // shape for the life of the process.  BW_I8_TUNE=0 takes the fill
+    // heuristic instead; BW_I8_PRODUCER=cpasync or =gather4 restricts the
+    // producer.
+    bool allow_g4 = true, allow_cp = true, tune = true;
+    if (const char* e = std::getenv("BW_I8_PRODUCER")) {
+        allow_g4 = std::string(e) != "cpasync";
+        allow_cp = std::string(e) != "gather4";
+    }
+    if (const char* e = std::getenv("BW_I8_TUNE")) tune = std::string(e) != "0";
+    std::string text;
+    for (int dir = 0; dir < 2; ++dir) {
+        I8State::Dir& D = dir == 0 ? S.fwd : S.bwd;
+        const int inner = dir == 0 ? ci : co, outer = dir == 0 ? co : ci;
+        const int in_buf = dir == 0 ? I8_YA : I8_Z, out_buf = dir == 0 ? I8_Z : I8_YB;
+        auto plan = [&](bool g4, int gps) {
+            if (D.b_tiles) release(D.b_tiles);
+            D.b_tiles = nullptr;
+            if (!plan_direction(*this, D, inner, outer, dir == 1, g4, gps)) return false;
+            if (static_cast<int>(D.smem) > (g4 ? cap_4 : cap_g)) return false;
+            D.p.err = S.err;
+            D.p.wait_limit = wait_limit;
+            D.p.hold_first_stage = 0;
+            D.p.inc = D.inc;
+            D.p.rows4 = D.rows4;
+            return true;
+        };
+        const TuneKey key{r, k, inner, outer, nbi, dir, sms, (allow_g4 ? 1 : 0) | (allow_cp ? 2 : 0)};
+        TuneChoice choice{};
+        bool have = tune && tune_lookup(key, choice);
+        std::string tried;
+        if (!have && tune) {
+            // candidates: TMA gathers with 1..4 groups of four generators a stage; cp.async's heuristic stage
+            std::vector<std::pair<bool, int>> cands;
+            if (allow_g4)
+                for (int gs = 1; gs <= std::min(4, (r + 3) / 4); ++gs) cands.push_back({true, 4 * gs});
+            if (allow_cp) cands.push_back({false, 0});
+            double best = 1e30;
+            for (const auto& cand : cands) {
+                if (!plan(cand.first, cand.second)) continue;
+                const double ms = i8_time_direction(dir == 0, in_buf, out_buf);
+                char buf[96];
+                std::snprintf(buf, sizeof buf, "%s%s stage=%d: %.4f ms", tried.empty() ? "" : ", ",
+                              cand.first ? "gather4" : "cp.async", D.p.gi, ms);
+                tried += buf;
+                if (ms < best) {
+                    best = ms;
+                    choice = TuneChoice{cand.first, D.p.gi, ms};
+                }
+            }
+            BW_REQUIRE(best < 1e30, "INT8 form: no stage plan fits in shared memory");
+            tune_store(key, choice);
+            have = true;
+        }
+        bool ok = false;
+        if (have) ok = plan(choice.gather4, choice.gps);
+        if (!ok) ok = (allow_g4 && plan(true, 0)) || (allow_cp && plan(false, 0));
+        BW_REQUIRE(ok, "INT8 form: maps too large for shared memory");
+        char buf[192];
+        std::snprintf(buf, sizeof buf, "%s: %s stage=%d generators, %d slots, %zu B shared", dir == 0 ? "d" : "d^T",
+                      D.gather4 ? "gather4" : "cp.async", D.p.gi, D.p.slots, D.smem);
+        text += (text.empty() ? "" : "; ") + std::string(buf);
+        if (!tried.empty()) text += " (tuned: " + tried + ")";
+    }
+    // the table the chosen producer does not read is freed
+    for (I8State::Dir* D : {&S.fwd, &S.bwd}) {
+        if (D->gather4) {
+            release(D->inc);
+            D->inc = nullptr;
+        } else {
+            release(D->rows4);
+            D->rows4 = nullptr;
+        }
+        D->p.inc = D->inc;
+        D->p.rows4 = D->rows4;
+        D->p.hold_first_stage = hold;
+    }
+    char pbuf[160];
+    std::snprintf(pbuf, sizeof pbuf, "; projection: %d blocks a stage (%d rows), %d slots", S.proj.sb, S.proj.kp,
+                  S.proj.slots);
+    S.plan_text = text + pbuf;
     BW_CUDA(cudaStreamSynchronize(own_stream));
+}
+
+const std::string& KoszulCtx::i8_plan_text() const { return i8->plan_text; }
+
+// Device time of one direction's gather-GEMM on the context's buffers: one
+// warm-up launch, then the mean of three (CUDA events on the own stream).
+double KoszulCtx::i8_time_direction(bool forward_dir, int in_buf, int out_buf) {
+    cudaEvent_t e0, e1;
+    BW_CUDA(cudaEventCreate(&e0));
+    BW_CUDA(cudaEventCreate(&e1));
+    i8_run(forward_dir, in_buf, out_buf, !forward_dir, own_stream);
+    BW_CUDA(cudaEventRecord(e0, own_stream));
+    for (int i = 0; i < 3; ++i) i8_run(forward_dir, in_buf, out_buf, !forward_dir, own_stream);
+    BW_CUDA(cudaEventRecord(e1, own_stream));
+    BW_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    BW_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    i8_check_error();
+    return ms / 3.0;
 }
 
 uint64_t KoszulCtx::i8_kernels_per_step() const { return 3; }

@@ -68,6 +68,7 @@ SIGNATURES = {
     "bw_koszul_sequence_host": (_INT, [_VP, _VP, _VP, _U64, _VP, _VP]),
     "bw_koszul_seq_step_timed": (_INT, [_VP, _U64, ctypes.POINTER(ctypes.c_float), _VP]),
     "bw_koszul_launch_count": (_U64, [_VP]),
+    "bw_koszul_plan": (_INT, [_VP, ctypes.c_char_p, ctypes.c_size_t]),
     "bw_koszul_batch_create": (_INT, [_VP, _U32, _INT, ctypes.POINTER(_VP)]),
     "bw_koszul_batch_destroy": (None, [_VP]),
     "bw_koszul_batch_sector": (_INT, [_VP, _U32, ctypes.POINTER(_VP)]),
@@ -268,6 +269,13 @@ class KoszulEngine:
     @property
     def launch_count(self):
         return int(load().bw_koszul_launch_count(self._h))
+
+    @property
+    def plan(self):
+        """The kernel plan and the set-up autotuner's timings (bw_koszul_plan)."""
+        buf = ctypes.create_string_buffer(4096)
+        _check(load().bw_koszul_plan(self._h, buf, len(buf)))
+        return buf.value.decode()
 
 
 class KoszulBatch:
