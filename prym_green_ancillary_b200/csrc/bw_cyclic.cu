@@ -292,6 +292,8 @@ __global__ void __launch_bounds__(kThreads) cyc_gram_kernel(
     const int32_t* __restrict__ C2, int count, long long rows, int32_t* __restrict__ partials,
     unsigned int* __restrict__ counter, uint32_t* __restrict__ seq, unsigned long long* __restrict__ seq_index,
     Mod mod) {
+    cyc::pdl_trigger();
+    cyc::pdl_wait();
     int32_t acc[20];
 #pragma unroll
     for (int e = 0; e < 20; ++e) acc[e] = 0;
@@ -800,9 +802,8 @@ void CyclicCtx::apply_square(const int32_t* in, int32_t* out) {
 }
 
 void CyclicCtx::gram(const int32_t* a1, const int32_t* c1, const int32_t* a2, const int32_t* c2, int count) {
-    cyc_gram_kernel<<<gram_grid, kThreads, 0, stream>>>(a1, c1, a2 ? a2 : a1, c2 ? c2 : c1, count,
-                                                        static_cast<long long>(op_cols), d_partials,
-                                                        d_counter, d_seq, d_seq_index, mod);
+    launch_pdl(cyc_gram_kernel, gram_grid, 0, a1, c1, a2 ? a2 : a1, c2 ? c2 : c1, count,
+               static_cast<long long>(op_cols), d_partials, d_counter, d_seq, d_seq_index, mod);
     BW_CHECK_LAUNCH();
     ++launches;
 }

@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace bw {
@@ -117,6 +118,9 @@ struct CyclicCtx {
     bool subset_path = false;    // the subset-major gathers run (bw_cyclic_subset.cu)
     std::string subset_reason;   // why not, when they do not
     bool stream_tables = false;  // its tables exceed half the L2: read them evict-first
+    // The round's kernels start while the kernel before them finishes
+    // (programmatic dependent launch; BW_CYCLIC_PDL=0 turns it off).
+    bool pdl = true;
     SubsetDev S{};
     uint4 *d_xs16 = nullptr, *d_y16 = nullptr, *d_t16 = nullptr, *d_u16 = nullptr, *d_u2_16 = nullptr;
     int32_t* d_zs = nullptr;     // compact z rows and extra columns of the scaled source
@@ -152,6 +156,24 @@ struct CyclicCtx {
     T* alloc(size_t count);
     unsigned grid_for(size_t rows) const;
     uint32_t* scratch_canonical();
+
+    // Launches a kernel of 256-thread CTAs on the context's stream, as a
+    // programmatic dependent launch when `pdl` is set (the kernel must call
+    // cyc::pdl_wait() before touching data of the kernels before it).
+    template <class... P, class... A>
+    void launch_pdl(void (*kernel)(P...), unsigned grid, size_t smem, A&&... args) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr{};
+        attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr.val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = pdl ? 1 : 0;
+        BW_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+    }
 
     void to_balanced(const uint32_t* in, int32_t* out, size_t count);
     void to_canonical(const int32_t* in, uint32_t* out, size_t count);

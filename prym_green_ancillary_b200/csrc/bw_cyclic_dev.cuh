@@ -7,6 +7,16 @@
 namespace bw {
 namespace cyc {
 
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// stream-serialization attribute may begin (stage its constant tables) while
+// the kernel before it on the stream is still finishing; pdl_wait() blocks
+// until that kernel has completed and its writes are visible, so it must come
+// before the first access to any buffer an earlier kernel reads or writes.
+// pdl_trigger() lets the next kernel begin early.  Launched without the
+// attribute, both are no-ops.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ int32_t red64(long long x, const Mod& m) {
     long long r = x % m.p;
     if (r > m.half) r -= m.p;

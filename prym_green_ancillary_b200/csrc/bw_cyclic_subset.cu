@@ -70,9 +70,13 @@ struct Tables {
     const int32_t *R, *B, *a0off, *a0idx, *a1off, *a1idx, *koff, *kidx, *ych;
 };
 
+// Staging reads only the constant tables, so it overlaps the end of the kernel
+// before (programmatic dependent launch); the wait follows it.
 __device__ __forceinline__ Tables stage(const SubsetDev& D, const int32_t* __restrict__ blob, int32_t* sm) {
+    cyc::pdl_trigger();
     for (int w = threadIdx.x; w < D.blob_words; w += blockDim.x) sm[w] = __ldg(blob + w);
     __syncthreads();
+    cyc::pdl_wait();
     Tables t;
     t.coef = reinterpret_cast<const int4*>(sm);
     t.R = sm + D.o_R;
@@ -296,6 +300,8 @@ __global__ void __launch_bounds__(kThreads) sub_d2_forward_kernel(SubsetDev D, c
 template <bool SMALL, bool STREAM>
 __global__ void __launch_bounds__(kThreads) sub_ell_kernel(SubsetDev D, const uint2* __restrict__ u,
                                                            uint2* __restrict__ u2) {
+    cyc::pdl_trigger();
+    cyc::pdl_wait();
     const long long rows = 2 * static_cast<long long>(D.n2);
     BW_ITEMS(row, rows) {
         Acc4<SMALL> acc;
@@ -677,6 +683,7 @@ void CyclicCtx::setup_subset_path() {
     int l2 = 0;
     BW_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
     stream_tables = table_bytes > static_cast<size_t>(l2) / 2;
+    if (const char* env = std::getenv("BW_CYCLIC_PDL")) pdl = std::string(env) != "0";
     // BW_CYCLIC_STREAM_TABLES=1 / =0 forces the evict-first (or the cached)
     // table reads at any size, so that small sectors run either instantiation.
     if (const char* env = std::getenv("BW_CYCLIC_STREAM_TABLES")) {
@@ -722,10 +729,11 @@ void CyclicCtx::subset_source16(const int32_t* in, const int32_t* dc) {
 
 void CyclicCtx::subset_forward16() {
     const size_t smem = static_cast<size_t>(S.blob_words) * 4;
-#define BW_LAUNCH(A, B)                                                                                      \
-    sub_dm_forward_elim_kernel<A, B><<<grid_for(S.n1), kThreads, smem, stream>>>(S, d_xs16, d_zs, d_y16); \
-    sub_d2_forward_kernel<A, B><<<grid_for(S.n2), kThreads, smem, stream>>>(S, d_y16, d_zs,               \
-                                                                             reinterpret_cast<uint2*>(d_u16))
+#define BW_LAUNCH(A, B)                                                                                    \
+    launch_pdl(sub_dm_forward_elim_kernel<A, B>, grid_for(S.n1), smem, S, static_cast<const uint4*>(d_xs16), \
+               static_cast<const int32_t*>(d_zs), d_y16);                                                  \
+    launch_pdl(sub_d2_forward_kernel<A, B>, grid_for(S.n2), smem, S, static_cast<const uint4*>(d_y16),     \
+               static_cast<const int32_t*>(d_zs), reinterpret_cast<uint2*>(d_u16))
     BW_SUBSET_DISPATCH(BW_LAUNCH);
 #undef BW_LAUNCH
     BW_CHECK_LAUNCH();
@@ -736,7 +744,7 @@ void CyclicCtx::subset_precondition16() {
     const uint2* u = reinterpret_cast<const uint2*>(d_u16);
     uint2* u2 = reinterpret_cast<uint2*>(d_u2_16);
     const unsigned grid = grid_for(2 * static_cast<size_t>(S.n2));
-#define BW_LAUNCH(A, B) sub_ell_kernel<A, B><<<grid, kThreads, 0, stream>>>(S, u, u2)
+#define BW_LAUNCH(A, B) launch_pdl(sub_ell_kernel<A, B>, grid, 0, S, u, u2)
     BW_SUBSET_DISPATCH(BW_LAUNCH);
 #undef BW_LAUNCH
     BW_CHECK_LAUNCH();
@@ -749,17 +757,18 @@ void CyclicCtx::subset_backward16(const int32_t* dc, int32_t* out, bool next_sou
     // also write the next application's source from `out`
     uint4* nxs = next_source ? d_xs16 : nullptr;
     int32_t* nzs = next_source ? d_zs : nullptr;
-#define BW_LAUNCH(A, B)                                                                                           \
-    sub_d2_transpose_adjoint_kernel<A, B><<<grid_for(S.n1), kThreads, smem, stream>>>(S, d_u2_16, dc, d_t16, out, \
-                                                                                     nzs);                        \
-    sub_dm_transpose_kernel<A, B><<<grid_for(S.n0), kThreads, smem, stream>>>(S, d_t16, dc, out, nxs)
+#define BW_LAUNCH(A, B)                                                                                       \
+    launch_pdl(sub_d2_transpose_adjoint_kernel<A, B>, grid_for(S.n1), smem, S,                               \
+               static_cast<const uint4*>(d_u2_16), dc, d_t16, out, nzs);                                      \
+    launch_pdl(sub_dm_transpose_kernel<A, B>, grid_for(S.n0), smem, S, static_cast<const uint4*>(d_t16), dc, \
+               out, nxs)
     BW_SUBSET_DISPATCH(BW_LAUNCH);
 #undef BW_LAUNCH
     BW_CHECK_LAUNCH();
     launches += 2;
     if (S.n_extra) {
-        sub_dense_t_kernel<<<dense_grid, kThreads, smem, stream>>>(S, reinterpret_cast<const uint2*>(d_u2_16), dc,
-                                                                   out, d_dpart, d_dcounter, nzs);
+        launch_pdl(sub_dense_t_kernel, dense_grid, smem, S, reinterpret_cast<const uint2*>(d_u2_16), dc, out,
+                   d_dpart, d_dcounter, nzs);
         BW_CHECK_LAUNCH();
         ++launches;
     }
