@@ -281,6 +281,15 @@ def paper_instance(name):
     return path
 
 
+def paper_traffic(name):
+    """DRAM bytes (read + write) of one application of S and its share of the
+    moments, summed over the kernels of an ncu capture (profiles/), or None."""
+    tfile = ROOT / "profiles" / f"traffic_{name}_paper.json"
+    if not tfile.exists():
+        return None
+    return json.loads(tfile.read_text()).get("application")
+
+
 def cpu_paper(name, sector, budget_s):
     """The reference's own CPU square operator (cpu_apply_eliminated_square,
     built from its source by oracle/build_ref.sh) applied repeatedly to the
@@ -576,7 +585,7 @@ def run_paper(args):
             "hbm_frac_step": achieved / peak,
             "roofline": {"bound": "hbm", "kernel": "apply of S + moments (one CUDA graph per round)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None,
+                         "traffic": paper_traffic(args.workload),
                          "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
             "cpu_baseline": cpu,
             "e2e": {"value": world * K / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": cols * 4 * 4 / K,

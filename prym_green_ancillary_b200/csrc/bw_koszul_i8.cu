@@ -246,6 +246,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         };
         SlotRing ring(P.slots);
         bool ok = true;
+        bool held = P.hold_first_stage && blockIdx.x == 0;
         uint32_t incr[TPW], incn[TPW];
         load_inc(blockIdx.x, incn);
         for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
@@ -264,7 +265,10 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                     break;
                 }
                 // failure tests: the first stage of CTA 0 is never filled, so its consumer's wait runs out
-                if (P.hold_first_stage && blockIdx.x == 0 && tile == blockIdx.x && s == 0) continue;
+                if (held) {   // failure tests: CTA 0's first stage is never filled
+                    held = false;
+                    continue;
+                }
                 const int g_s = min(P.gi, P.r - s * P.gi);
                 const int rows = g_s * P.inner;             // K' rows filled in this stage
                 uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
@@ -518,6 +522,7 @@ __global__ void __launch_bounds__(kG4Threads, 1)
 #pragma unroll
         for (int q = 0; q < kMaxSlots; ++q) issued[q] = false, issued_phase[q] = 0;
         bool ok = true;
+        bool held = P.hold_first_stage && blockIdx.x == 0;
         for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
             for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
                 const int slot = ring.slot;
@@ -531,7 +536,10 @@ __global__ void __launch_bounds__(kG4Threads, 1)
                     break;
                 }
                 // failure tests: the first stage of CTA 0 is never filled, so its consumer's wait runs out
-                if (P.hold_first_stage && blockIdx.x == 0 && tile == blockIdx.x && s == 0) continue;
+                if (held) {   // failure tests: CTA 0's first stage is never filled
+                    held = false;
+                    continue;
+                }
                 const bool last = s == P.stages_per_tile - 1;
                 const int g_n = last ? P.groups - s * P.gs : P.gs;   // groups in this stage
                 if (lane == 0) tc::mbar_arrive_expect_tx(&full[slot], last ? P.tx_last : P.tx_full);
