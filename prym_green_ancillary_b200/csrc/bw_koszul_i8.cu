@@ -96,12 +96,13 @@ struct I8Dir {
     int32_t c1, c2;              // 255 and 255^2 mod p, balanced
     uint32_t wait_limit;         // tries of every pipeline wait (tc::kWaitLimit outside the failure tests)
     int hold_first_stage;        // failure tests only: CTA 0 never fills its first stage
-    // TMA gather producer (i8_gather4_kernel)
+    // hybrid producer (i8_gather_hybrid_kernel)
     const int4* rows4;           // [n_blk][groups]: plane rows of the four generators of a group (h = 0)
     int groups;                  // ceil(r / 4)
     int gs;                      // groups per stage
     int inner_pad;               // K' rows of a generator: inner rounded up to even (128-byte aligned groups)
     int32_t row_oob;             // a plane row past the input tensor (2 * input blocks * HG): zero-filled
+    int t_tma;                   // hybrid producer: output blocks of a tile gathered by TMA (the rest by cp.async)
     uint32_t tx_full, tx_last;   // bytes a full / the last stage of a tile receives
 };
 
@@ -433,30 +434,44 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
     }
 }
 
-// ---- gather-GEMM with a TMA gather producer
+// ---- gather-GEMM with a hybrid producer: TMA gathers beside cp.async warps
 //
-// Same tile, MMA issue and epilogue as i8_gather_gemm_kernel; the stage is
-// filled by the tensor-memory accelerator instead of cp.async warps.  The
-// +plane and the -plane of a limb are one 2-D tensor (rows = (block, h) runs of
-// inner * 16 bytes, the -plane's rows after the +plane's), so one tile::gather4
-// copies the runs of four neighbour blocks, each from the plane its Koszul sign
-// selects, into the four generators' K' rows of one (output block, limb, h)
-// core-matrix column: row = neg * n_blk * HG + nbr * HG + h, precomputed on the
-// host per group of four generators (rows4).  An absent generator (or a padding
-// generator past r) has a row beyond the tensor: the copy fills its rows with
-// zeros and reads nothing.  A generator spans inner_pad (even) K' rows, so every
-// gather starts 128-byte aligned; the odd padding row is beyond the tensor's
-// row width (zero-filled) and meets zero rows of the maps.
+// Same tile, MMA issue and epilogue as i8_gather_gemm_kernel; a stage holds
+// gs groups of four generators, each generator inner_pad (inner rounded up to
+// even) K' rows, so that every group starts 128-byte aligned.  The tile's
+// output blocks t < t_tma are filled by the tensor-memory accelerator, the
+// others by eight cp.async warps, both into the same stage and completing on
+// the same barrier (257 arrivals: one per cp.async thread when its copies have
+// landed, one from the TMA warp with the stage's TMA byte count), so the two
+// copy engines work side by side.
 //
-// Warp roles: warp 0 producer (one gather per lane and stage), warp 1 MMA
-// issuer (allocates TMEM), warps 2-9 epilogue.  On a give-up the producer
+// TMA part: the +plane and the -plane of a limb are one 2-D tensor (rows =
+// (block, h) runs of inner * 16 bytes, the -plane's rows after the +plane's),
+// so one tile::gather4 copies the runs of four neighbour blocks, each from the
+// plane its Koszul sign selects: row = neg * n_blk_in * HG + nbr * HG + h,
+// precomputed on the host per group of four generators (rows4).  An absent
+// generator (or a padding generator past r) has a row beyond the tensor: the
+// copy fills its rows with zeros and reads nothing.  The odd padding row of a
+// generator is beyond the tensor's row width (zero-filled) and meets zero rows
+// of the maps.
+//
+// cp.async part: as in i8_gather_gemm_kernel (16-byte copies from the +plane
+// or -plane, zero-filling ones for absent generators), with the rows of a
+// block shared by 8 / (BT - t_tma) warps.
+//
+// Warp roles: warps 0-7 cp.async producers, warp 8 TMA producer, warp 9 MMA
+// issuer (allocates TMEM), warps 10-17 epilogue.  On a give-up every producer
 // still waits (bounded) for the copies it issued before the CTA exits.
-constexpr int kG4Threads = (2 + kEpilogueWarps) * 32;
+constexpr int kCpWarps = 8;
+constexpr int kTmaWarp = kCpWarps;
+constexpr int kHyMmaWarp = kCpWarps + 1;
+constexpr int kHyEpi0 = kCpWarps + 2;
+constexpr int kHyThreads = (kCpWarps + 2 + kEpilogueWarps) * 32;
 
 template <int NB>
-__global__ void __launch_bounds__(kG4Threads, 1)
-    i8_gather4_kernel(const __grid_constant__ CUtensorMap map_lo, const __grid_constant__ CUtensorMap map_hi,
-                      I8Dir P) {
+__global__ void __launch_bounds__(kHyThreads, 1)
+    i8_gather_hybrid_kernel(const __grid_constant__ CUtensorMap map_lo, const __grid_constant__ CUtensorMap map_hi,
+                            I8Dir P) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int BT = 128 / NB;        // output blocks per tile
     constexpr int HG = NB / 16;         // 16-byte column groups per block row
@@ -471,11 +486,14 @@ __global__ void __launch_bounds__(kG4Threads, 1)
     uint64_t* drained = accempty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
     volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);   // CTA give-up flag
+    uint8_t* il_of_row = reinterpret_cast<uint8_t*>(tmem_slot + 4);        // K' row -> generator in stage (255: pad)
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const long long n_tiles = (P.n_blk + BT - 1) / BT;
-    // every gather destination is 128-byte aligned relative to the base
-    if ((tc::smem_u32(smem) & 127u) != 0 || P.slots > kMaxSlots) {
+    const int KS = P.ks_full * 32;                    // K' rows of a slot's column (full stage, padded)
+    // every TMA destination is 128-byte aligned relative to the base
+    if ((tc::smem_u32(smem) & 127u) != 0 || P.slots > kMaxSlots || P.t_tma < 0 || P.t_tma > BT ||
+        KS > kMaxRowTable) {
         if (threadIdx.x == 0) atomicCAS(P.err, tc::ERR_NONE, tc::ERR_LAYOUT);
         return;
     }
@@ -483,9 +501,13 @@ __global__ void __launch_bounds__(kG4Threads, 1)
     for (uint32_t off = threadIdx.x * 16; off < P.b_bytes; off += blockDim.x * 16)
         *reinterpret_cast<int4*>(sB + off) = __ldg(reinterpret_cast<const int4*>(P.b_tiles + off));
     tc::fence_proxy_async_smem();
+    for (int w = threadIdx.x; w < KS; w += blockDim.x) {
+        const int il = w / P.inner_pad, u = w - il * P.inner_pad;
+        il_of_row[w] = static_cast<uint8_t>(u < P.inner ? il : 255);
+    }
     if (threadIdx.x == 0) {
         for (int s = 0; s < P.slots; ++s) {
-            tc::mbar_init(&full[s], 1);     // the producer's arrive.expect_tx; the copies complete the bytes
+            tc::mbar_init(&full[s], kCpWarps * 32 + 1);   // cp.async threads + the TMA warp's expect_tx arrive
             tc::mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -497,7 +519,7 @@ __global__ void __launch_bounds__(kG4Threads, 1)
         *abort = 0;
     }
     const uint32_t tmem_cols = (4 * N <= 256) ? 256u : 512u;
-    if (warp == 1) {
+    if (warp == kHyMmaWarp) {
         tc::tmem_alloc(tmem_slot, tmem_cols);
         tc::tmem_relinquish();
     }
@@ -505,17 +527,86 @@ __global__ void __launch_bounds__(kG4Threads, 1)
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const int KS = P.ks_full * 32;                    // K' rows of a slot's column (full stage, padded)
-    const uint32_t gbytes = static_cast<uint32_t>(P.inner_pad) * 64;   // one group: 4 generators x inner_pad rows
+    const uint32_t block_bytes = static_cast<uint32_t>(P.inner) * 16;
 
-    if (warp == 0) {
-        // ------------------------------------------------------------ producer
-        // Stage s of a tile holds the groups s * gs .. s * gs + gs - 1 of every
-        // (output block t, limb, h): 2 * BT * HG * gs gathers, lane j issues
-        // j, j + 32, ...  Lane 0 posts the stage's byte count first.
+    if (warp < kCpWarps) {
+        // ------------------------------------------------------------ cp.async producers
+        // Blocks t_tma..BT-1 of every tile; a block's stage rows are shared by
+        // wpb = 8 / n_cp warps (interleaved by 32 rows); lane i holds the
+        // incidence entry of generator i for its warp's block (the next tile's
+        // entry is loaded one tile ahead).  Every producer thread arrives once
+        // per stage, after waiting for the slot to be free.
+        const int n_cp = BT - P.t_tma;
+        const int wpb = n_cp > 0 ? kCpWarps / n_cp : 1;
+        const bool active = n_cp > 0 && warp < n_cp * wpb;
+        const int t = active ? P.t_tma + warp / wpb : 0, sub = active ? warp % wpb : 0;
+        auto load_inc = [&](long long tile) -> uint32_t {
+            const long long blk = tile * BT + t;
+            return (active && tile < n_tiles && blk < P.n_blk && lane < P.r) ? __ldg(P.inc + blk * P.r + lane)
+                                                                              : kAbsent;
+        };
+        SlotRing ring(P.slots);
+        bool ok = true;
+        bool held = P.hold_first_stage && blockIdx.x == 0;
+        uint32_t incn = load_inc(blockIdx.x);
+        for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+            const uint32_t incr = incn;
+            incn = load_inc(tile + gridDim.x);
+            for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
+                const int slot = ring.slot;
+                const uint32_t ph = ring.phase;
+                int got = 1;
+                if (lane == 0)
+                    got = tc::mbar_wait(&empty[slot], ph ^ 1u, abort, P.err, tc::ERR_WAIT_EMPTY, P.wait_limit) ? 1 : 0;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) {
+                    ok = false;
+                    break;
+                }
+                if (held) {   // failure tests: CTA 0's first stage is never filled
+                    held = false;
+                    continue;
+                }
+                if (active) {
+                    const bool last = s == P.stages_per_tile - 1;
+                    const int rows = (last ? P.groups - s * P.gs : P.gs) * 4 * P.inner_pad;
+                    uint8_t* col0 = sA + static_cast<size_t>(slot) * P.slot_bytes + static_cast<size_t>(t * HG) * KS * 16;
+                    for (int w0 = sub * 32; w0 < rows; w0 += wpb * 32) {
+                        const int w = w0 + lane;
+                        const int il = il_of_row[min(w, rows - 1)];
+                        const int gen = s * P.gi + (il == 255 ? 0 : il);
+                        const uint32_t e = __shfl_sync(0xffffffffu, incr, min(gen, 31));
+                        // padding rows and generators past r: their B rows are zero, nothing to copy
+                        if (w >= rows || il == 255 || gen >= P.r) continue;
+                        const int u = w - il * P.inner_pad;
+                        const bool present = e != kAbsent;
+                        const long long nbr = present ? static_cast<long long>(e & 0x7FFFFFFFu) : 0;
+                        const int neg = (present && (e >> 31)) ? 2 : 0;
+                        const uint32_t nbytes = present ? 16u : 0u;
+                        uint8_t* dst0 = col0 + static_cast<size_t>(w) * 16;
+#pragma unroll
+                        for (int limb = 0; limb < 2; ++limb)
+#pragma unroll
+                            for (int h = 0; h < HG; ++h)
+                                tc::cp_async16_zfill(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
+                                                         static_cast<size_t>(h) * KS * 16,
+                                                     P.in[limb + neg] + (nbr * HG + h) * block_bytes + u * 16, nbytes);
+                    }
+                }
+                tc::cp_async_arrive_noinc(&full[slot]);   // when this thread's copies have landed
+            }
+        }
+        tc::cp_async_wait_all();   // no copy may still be landing when the CTA exits
+    } else if (warp == kTmaWarp) {
+        // ------------------------------------------------------------ TMA producer
+        // Blocks 0..t_tma-1: stage s holds groups s * gs .. of every (block,
+        // limb, h): 2 * t_tma * HG * g_n gathers; lane j issues j, j + 32, ...
+        // Lane 0 posts the stage's TMA byte count first (an arrive with zero
+        // bytes when t_tma = 0).
         tc::prefetch_tmap(&map_lo);
         tc::prefetch_tmap(&map_hi);
         const int32_t oob = P.row_oob;   // beyond the input tensor: zero rows, nothing read
+        const uint32_t gbytes = static_cast<uint32_t>(P.inner_pad) * 64;   // one group: 4 generators x inner_pad rows
         SlotRing ring(P.slots);
         uint32_t issued_phase[kMaxSlots];
         bool issued[kMaxSlots];
@@ -535,24 +626,23 @@ __global__ void __launch_bounds__(kG4Threads, 1)
                     ok = false;
                     break;
                 }
-                // failure tests: the first stage of CTA 0 is never filled, so its consumer's wait runs out
-                if (held) {   // failure tests: CTA 0's first stage is never filled
+                if (held) {
                     held = false;
                     continue;
                 }
                 const bool last = s == P.stages_per_tile - 1;
                 const int g_n = last ? P.groups - s * P.gs : P.gs;   // groups in this stage
-                if (lane == 0) tc::mbar_arrive_expect_tx(&full[slot], last ? P.tx_last : P.tx_full);
+                const int n_g = 2 * P.t_tma * HG * g_n;
+                if (lane == 0) tc::mbar_arrive_expect_tx(&full[slot], static_cast<uint32_t>(n_g) * gbytes);
                 __syncwarp();
                 uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
-                const int n_g = 2 * BT * HG * g_n;
                 for (int j = lane; j < n_g; j += 32) {
                     const int gl = j % g_n;                 // group within the stage
                     const int rest = j / g_n;
                     const int limb = rest & 1;
-                    const int col = rest >> 1;              // t * HG + h
-                    const int t = col / HG, h = col - (col / HG) * HG;
-                    const long long blk = tile * BT + t;
+                    const int col = rest >> 1;              // t * HG + h, t < t_tma
+                    const int tt = col / HG, h = col - (col / HG) * HG;
+                    const long long blk = tile * BT + tt;
                     int4 rr = make_int4(oob, oob, oob, oob);
                     if (blk < P.n_blk) rr = __ldg(P.rows4 + blk * P.groups + s * P.gs + gl);
                     uint8_t* dst = slotA + static_cast<size_t>(limb) * P.limb_bytes +
@@ -560,19 +650,21 @@ __global__ void __launch_bounds__(kG4Threads, 1)
                     tc::tma_gather4(dst, limb ? static_cast<const void*>(&map_hi) : static_cast<const void*>(&map_lo),
                                     0, rr.x + h, rr.y + h, rr.z + h, rr.w + h, &full[slot]);
                 }
-                issued[slot] = true;
-                issued_phase[slot] = ph;
+                if (n_g > 0) {
+                    issued[slot] = true;
+                    issued_phase[slot] = ph;
+                }
             }
         }
         // no copy may still be landing when the CTA exits: wait (bounded) for
-        // the last stage issued into every slot (a consumed stage has completed)
+        // the last stage with gathers in every slot (a consumed stage has completed)
         if (lane == 0) {
 #pragma unroll
             for (int q = 0; q < kMaxSlots; ++q)
                 if (q < P.slots && issued[q]) tc::mbar_wait(&full[q], issued_phase[q], nullptr, P.err, tc::ERR_WAIT_FINAL);
         }
         __syncwarp();
-    } else if (warp == 1) {
+    } else if (warp == kHyMmaWarp) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_i8(128, N, true, false);
@@ -593,6 +685,8 @@ __global__ void __launch_bounds__(kG4Threads, 1)
                         ok = false;
                         break;
                     }
+                    // the cp.async part was written through the generic proxy
+                    tc::fence_proxy_async_smem();
                     tc::tc_fence_after();
                     const int ks_n = (s == P.stages_per_tile - 1) ? P.ks_last : P.ks_full;
                     for (int limb = 0; limb < 2; ++limb) {
@@ -618,11 +712,11 @@ __global__ void __launch_bounds__(kG4Threads, 1)
         __syncwarp();
     } else {
         // ------------------------------------------------------------ epilogue
-        // Warps 2..9: warp & 3 is the TMEM lane quadrant it may read; the two
+        // Warps 10..17: warp & 3 is the TMEM lane quadrant it may read; the two
         // warps of a quadrant split the 16-column output chunks between them.
         const int q = warp & 3;
         constexpr int EPQ = kEpilogueWarps / 4;
-        const int half_id = (warp - 2) >> 2;
+        const int half_id = (warp - kHyEpi0) >> 2;
         const int m = q * 32 + lane;               // tile row = (block t, column j)
         const int t = m / NB, j = m % NB;
         const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
@@ -690,7 +784,7 @@ __global__ void __launch_bounds__(kG4Threads, 1)
 
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 1) {
+    if (warp == kHyMmaWarp) {
         tc::tc_fence_after();
         tc::tmem_dealloc(tmem, tmem_cols);
     }
@@ -1006,7 +1100,7 @@ struct KoszulCtx::I8State {
         int8_t* b_tiles = nullptr;
         uint32_t* inc = nullptr;
         int4* rows4 = nullptr;     // TMA gather rows per group of four generators
-        bool gather4 = false;      // stages filled by TMA gathers (else cp.async warps)
+        bool gather4 = false;      // hybrid producer (TMA gathers beside cp.async warps), else cp.async only
         size_t smem = 0;
         unsigned grid = 0;
     } fwd, bwd;
@@ -1034,8 +1128,9 @@ struct TuneKey {
     }
 };
 struct TuneChoice {
-    bool gather4 = false;
-    int gps = 0;
+    bool gather4 = false;   // the hybrid producer
+    int gps = 0;            // generators per stage
+    int t_tma = 0;          // hybrid: blocks of a tile gathered by TMA
     double ms = 0;
 };
 std::mutex g_tune_mutex;
@@ -1071,7 +1166,7 @@ bool plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     P.half = (outer + 15) / 16 * 16;
     const int N = 2 * P.half;
     BW_REQUIRE(N <= 256, "INT8 form: output dimension above 128 is not supported");
-    const size_t extra = (2 * 8 + 2 * 2 + 1) * 8 + 16 + (gather4 ? 0 : kMaxRowTable);
+    const size_t extra = (2 * 8 + 2 * 2 + 1) * 8 + 16 + kMaxRowTable;
     const int inner_pad = gather4 ? inner + (inner & 1) : inner;
     auto b_bytes_of = [&](int gps) {
         const int stages = (c.r + gps - 1) / gps;
@@ -1140,6 +1235,7 @@ bool plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     while (slots > 1 && P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra > static_cast<size_t>(kMaxSmem))
         --slots;
     if (P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra > static_cast<size_t>(kMaxSmem)) return false;
+    if (gather4 && P.ks_full * 32 > kMaxRowTable) return false;
     P.slots = slots;
     D.smem = P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra;
     D.gather4 = gather4;
@@ -1287,7 +1383,7 @@ void plan_projection(KoszulCtx& c, KoszulCtx::I8State& S) {
 template <int NB>
 void launch_i8(KoszulCtx& c, KoszulCtx::I8State::Dir& D, const CUtensorMap* maps, cudaStream_t st) {
     if (D.gather4)
-        i8_gather4_kernel<NB><<<D.grid, kG4Threads, D.smem, st>>>(maps[0], maps[1], D.p);
+        i8_gather_hybrid_kernel<NB><<<D.grid, kHyThreads, D.smem, st>>>(maps[0], maps[1], D.p);
     else
         i8_gather_gemm_kernel<NB><<<D.grid, kI8Threads, D.smem, st>>>(D.p);
     BW_CHECK_LAUNCH();
@@ -1388,7 +1484,7 @@ void KoszulCtx::i8_setup() {
     int cap_g = 0, cap_4 = 0;
     dispatch_i8_nb(nbi, [&](auto NBc) {
         cap_g = allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value>, device);
-        cap_4 = allow_dynamic_smem(i8_gather4_kernel<decltype(NBc)::value>, device);
+        cap_4 = allow_dynamic_smem(i8_gather_hybrid_kernel<decltype(NBc)::value>, device);
         const int cap_p = allow_dynamic_smem(i8_project_tc_kernel<decltype(NBc)::value>, device);
         BW_REQUIRE(static_cast<int>(S.proj_smem) <= cap_p, "INT8 form: shared-memory plan above the device limit");
     });
@@ -1405,12 +1501,12 @@ void KoszulCtx::i8_setup() {
     // memory on this device, at set-up, on the context's own buffers (the
     // kernels' work does not depend on the values); the choice is cached per
     // shape for the life of the process.  BW_I8_TUNE=0 takes the fill
-    // heuristic instead; BW_I8_PRODUCER=cpasync or =gather4 restricts the
+    // heuristic instead; BW_I8_PRODUCER=cpasync or =hybrid restricts the
     // producer.
     bool allow_g4 = true, allow_cp = true, tune = true;
     if (const char* e = std::getenv("BW_I8_PRODUCER")) {
         allow_g4 = std::string(e) != "cpasync";
-        allow_cp = std::string(e) != "gather4";
+        allow_cp = std::string(e) != "hybrid";
     }
     if (const char* e = std::getenv("BW_I8_TUNE")) tune = std::string(e) != "0";
     std::string text;
@@ -1418,11 +1514,12 @@ void KoszulCtx::i8_setup() {
         I8State::Dir& D = dir == 0 ? S.fwd : S.bwd;
         const int inner = dir == 0 ? ci : co, outer = dir == 0 ? co : ci;
         const int in_buf = dir == 0 ? I8_YA : I8_Z, out_buf = dir == 0 ? I8_Z : I8_YB;
-        auto plan = [&](bool g4, int gps) {
+        auto plan = [&](bool g4, int gps, int t_tma) {
             if (D.b_tiles) release(D.b_tiles);
             D.b_tiles = nullptr;
             if (!plan_direction(*this, D, inner, outer, dir == 1, g4, gps)) return false;
             if (static_cast<int>(D.smem) > (g4 ? cap_4 : cap_g)) return false;
+            D.p.t_tma = g4 ? t_tma : 0;
             D.p.err = S.err;
             D.p.wait_limit = wait_limit;
             D.p.hold_first_stage = 0;
@@ -1435,22 +1532,32 @@ void KoszulCtx::i8_setup() {
         bool have = tune && tune_lookup(key, choice);
         std::string tried;
         if (!have && tune) {
-            // candidates: TMA gathers with 1..4 groups of four generators a stage; cp.async's heuristic stage
-            std::vector<std::pair<bool, int>> cands;
+            // candidates: the cp.async producer with its heuristic stage; the
+            // hybrid producer with 1..3 groups of four generators a stage and a
+            // quarter, half or three quarters of a tile's blocks gathered by TMA
+            struct Cand {
+                bool g4;
+                int gps, t_tma;
+            };
+            std::vector<Cand> cands;
+            if (allow_cp) cands.push_back({false, 0, 0});
             if (allow_g4)
-                for (int gs = 1; gs <= std::min(4, (r + 3) / 4); ++gs) cands.push_back({true, 4 * gs});
-            if (allow_cp) cands.push_back({false, 0});
+                for (int gs = 1; gs <= std::min(3, (r + 3) / 4); ++gs)
+                    for (int qt = 1; qt <= 3; ++qt) cands.push_back({true, 4 * gs, qt * bt / 4});
             double best = 1e30;
-            for (const auto& cand : cands) {
-                if (!plan(cand.first, cand.second)) continue;
+            for (const Cand& cand : cands) {
+                if (!plan(cand.g4, cand.gps, cand.t_tma)) continue;
                 const double ms = i8_time_direction(dir == 0, in_buf, out_buf);
                 char buf[96];
-                std::snprintf(buf, sizeof buf, "%s%s stage=%d: %.4f ms", tried.empty() ? "" : ", ",
-                              cand.first ? "gather4" : "cp.async", D.p.gi, ms);
+                if (cand.g4)
+                    std::snprintf(buf, sizeof buf, "%shybrid stage=%d tma=%d/%d: %.4f ms", tried.empty() ? "" : ", ",
+                                  D.p.gi, cand.t_tma, bt, ms);
+                else
+                    std::snprintf(buf, sizeof buf, "%scp.async stage=%d: %.4f ms", tried.empty() ? "" : ", ", D.p.gi, ms);
                 tried += buf;
                 if (ms < best) {
                     best = ms;
-                    choice = TuneChoice{cand.first, D.p.gi, ms};
+                    choice = TuneChoice{cand.g4, D.p.gi, cand.t_tma, ms};
                 }
             }
             BW_REQUIRE(best < 1e30, "INT8 form: no stage plan fits in shared memory");
@@ -1458,12 +1565,16 @@ void KoszulCtx::i8_setup() {
             have = true;
         }
         bool ok = false;
-        if (have) ok = plan(choice.gather4, choice.gps);
-        if (!ok) ok = (allow_g4 && plan(true, 0)) || (allow_cp && plan(false, 0));
+        if (have) ok = plan(choice.gather4, choice.gps, choice.t_tma);
+        if (!ok) ok = (allow_cp && plan(false, 0, 0)) || (allow_g4 && plan(true, 0, bt / 2));
         BW_REQUIRE(ok, "INT8 form: maps too large for shared memory");
         char buf[192];
-        std::snprintf(buf, sizeof buf, "%s: %s stage=%d generators, %d slots, %zu B shared", dir == 0 ? "d" : "d^T",
-                      D.gather4 ? "gather4" : "cp.async", D.p.gi, D.p.slots, D.smem);
+        if (D.gather4)
+            std::snprintf(buf, sizeof buf, "%s: hybrid (TMA gathers for %d of %d blocks) stage=%d generators, %d slots, "
+                          "%zu B shared", dir == 0 ? "d" : "d^T", D.p.t_tma, bt, D.p.gi, D.p.slots, D.smem);
+        else
+            std::snprintf(buf, sizeof buf, "%s: cp.async stage=%d generators, %d slots, %zu B shared",
+                          dir == 0 ? "d" : "d^T", D.p.gi, D.p.slots, D.smem);
         text += (text.empty() ? "" : "; ") + std::string(buf);
         if (!tried.empty()) text += " (tuned: " + tried + ")";
     }
