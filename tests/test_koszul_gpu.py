@@ -23,6 +23,20 @@ pytestmark = pytest.mark.gpu
 GOLDEN = np.load(Path(__file__).parent / "golden" / "koszul_golden.npz")
 CASES = sorted({k.split("/")[0] for k in GOLDEN.files})
 FORMS = ["plain", "int8"]
+# The INT8 form's two stage producers (the set-up autotuner picks one per
+# shape; BW_I8_PRODUCER restricts the choice): cp.async warps alone, or TMA
+# gathers beside them.
+PRODUCER_FORMS = ["plain", "int8:cpasync", "int8:hybrid"]
+
+
+@pytest.fixture
+def producer_form(request, monkeypatch):
+    form, _, producer = request.param.partition(":")
+    if producer:
+        monkeypatch.setenv("BW_I8_PRODUCER", producer)
+    else:
+        monkeypatch.delenv("BW_I8_PRODUCER", raising=False)
+    return form, producer
 
 
 def _supported(form, nb):
@@ -65,9 +79,10 @@ SHAPES = [
 ]
 
 
-@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("producer_form", PRODUCER_FORMS, indirect=True)
 @pytest.mark.parametrize("dims", SHAPES)
-def test_operators_match_oracle(dims, form):
+def test_operators_match_oracle(dims, producer_form):
+    form, producer = producer_form
     shape = oracle.KoszulShape(*dims)
     _supported(form, shape.nb)
     maps, diag, X, Y = oracle.seeded_problem(shape, 99)
@@ -75,6 +90,8 @@ def test_operators_match_oracle(dims, form):
     Z = rng.integers(0, shape.p, (shape.n_tgt, shape.nb), dtype=np.uint32)
     dev = torch.device("cuda", 0)
     with _engine(shape, maps, diag, form) as eng:
+        if producer:
+            assert ("hybrid" in eng.plan) == (producer == "hybrid"), eng.plan
         y = torch.from_numpy(Y.view(np.int32)).to(dev)
         z = torch.from_numpy(Z.view(np.int32)).to(dev)
         out_z = torch.empty((shape.n_tgt, shape.nb), dtype=torch.int32, device=dev)
@@ -143,14 +160,15 @@ def _projection(x, w, p):
     return acc.to(torch.int64).cpu().numpy().astype(np.uint32)
 
 
-@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("producer_form", PRODUCER_FORMS, indirect=True)
 @pytest.mark.parametrize("cfg", [
     # r = 19, k = 9, dim 20 -> 28, p = 32003, block 16 x 16 (N = 1,847,560)
     ("config2", 19, 9, 20, 28, 32003, 16, 16, 3),
     # r = 23, k = 11, dim 32 -> 40, block 32 x 32 (N = 43,266,496)
     ("config5", 23, 11, 32, 40, 32003, 32, 32, 1),
 ])
-def test_full_size_apply_and_session(cfg, form):
+def test_full_size_apply_and_session(cfg, producer_form):
+    form, producer = producer_form
     name, r, k, ci, co, p, nb, m, steps = cfg
     shape = oracle.KoszulShape(r, k, ci, co, p, nb, m)
     dev = torch.device("cuda", 0)
