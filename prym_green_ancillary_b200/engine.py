@@ -257,11 +257,25 @@ class KoszulEngine:
         return tuple(float(v) for v in ms)
 
     # -- host-buffer API ---------------------------------------------------
-    def sequence_host(self, X, Y0, nlen, want_final=True):
+    def sequence_host(self, X, Y0, nlen, want_final=True, out=None):
+        """Sequence of nlen entries through host buffers (bw_koszul_sequence_host).
+
+        ``out`` = (seq, final) lets the caller supply the output arrays (for
+        example views of pinned host memory, which the copies back reach
+        directly); by default they are allocated here.
+        """
         X = np.ascontiguousarray(X, dtype=np.uint32)
         Y0 = np.ascontiguousarray(Y0, dtype=np.uint32)
-        seq = np.empty((nlen, self.m, self.nb), dtype=np.uint32)
-        yf = np.empty((self.n_src, self.nb), dtype=np.uint32) if want_final else None
+        if out is not None:
+            seq, yf = out
+            assert seq.dtype == np.uint32 and seq.shape == (nlen, self.m, self.nb) and seq.flags.c_contiguous
+            if want_final:
+                assert yf.dtype == np.uint32 and yf.shape == (self.n_src, self.nb) and yf.flags.c_contiguous
+            else:
+                yf = None
+        else:
+            seq = np.empty((nlen, self.m, self.nb), dtype=np.uint32)
+            yf = np.empty((self.n_src, self.nb), dtype=np.uint32) if want_final else None
         _check(load().bw_koszul_sequence_host(self._h, _host_ptr(X), _host_ptr(Y0), nlen, _host_ptr(seq),
                                               _host_ptr(yf) if yf is not None else None))
         return seq, yf
