@@ -535,12 +535,16 @@ void KoszulCtx::seq_start(const uint32_t* x, const uint32_t* y0, uint32_t* seq, 
         project(d_ya, st);
     }
     seq_len = 1;
-    // Graphs capture device pointers; a new session may bring a new d_seq.
-    for (auto& g : graphs)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
+    // The step graphs capture device pointers: all are the context's own but
+    // the sequence buffer, so a session with another buffer recaptures them.
+    if (seq != graph_seq) {
+        for (auto& g : graphs)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        graph_seq = seq;
+    }
     in_session = true;
 }
 

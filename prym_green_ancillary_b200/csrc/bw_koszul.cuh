@@ -42,6 +42,7 @@ struct KoszulCtx {
     uint64_t seq_capacity = 0, seq_len = 0;
     static constexpr int kGraphPairs = 8;
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+    const uint32_t* graph_seq = nullptr;   // the sequence buffer the step graphs write
     uint64_t graph_launch_kernels = 0;
     uint64_t launches = 0;
 
