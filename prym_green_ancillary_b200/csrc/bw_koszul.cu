@@ -92,8 +92,13 @@ __global__ void __launch_bounds__(256) gather_mac_kernel(
             for (int b = 0; b < 4; ++b) acc[a][b] = 0;
         bool neg_state = false;
         const uint32_t* binc = inc + blk * width;
+        // The incidence word of the next neighbour is loaded one neighbour
+        // ahead, and a chunk's eight input rows are all in flight before its
+        // multiply-adds: the gathers' L2 latency overlaps instead of chaining.
+        uint32_t e_next = width > 0 ? __ldg(binc) : 0u;
         for (int q = 0; q < width; ++q) {
-            const uint32_t e = __ldg(binc + q);
+            const uint32_t e = e_next;
+            if (q + 1 < width) e_next = __ldg(binc + q + 1);
             const bool neg = (e >> 31) != 0;
             const int i = static_cast<int>((e >> 26) & 31u);
             const long long s = static_cast<long long>(e & 0x3FFFFFFu);
@@ -104,12 +109,15 @@ __global__ void __launch_bounds__(256) gather_mac_kernel(
             const int4* irow = reinterpret_cast<const int4*>(in + s * inner * NB) + jg;
             const int4* crow = sm4 + static_cast<size_t>(i) * inner * OG + og;
             for (int u0 = 0; u0 < inner; u0 += 8) {
-                const int uend = min(u0 + 8, inner);
-#pragma unroll 4
-                for (int u = u0; u < uend; ++u) {
-                    const int4 y = __ldg(irow + u * JG);
-                    const int4 a = crow[u * OG];
-                    mac4x4(acc, a, y);
+                int4 y[8];
+#pragma unroll
+                for (int uu = 0; uu < 8; ++uu)
+                    y[uu] = u0 + uu < inner ? __ldg(irow + (u0 + uu) * JG) : make_int4(0, 0, 0, 0);
+#pragma unroll
+                for (int uu = 0; uu < 8; ++uu) {
+                    if (u0 + uu >= inner) break;
+                    const int4 a = crow[(u0 + uu) * OG];
+                    mac4x4(acc, a, y[uu]);
                 }
                 reduce4x4(acc, mod);
             }
