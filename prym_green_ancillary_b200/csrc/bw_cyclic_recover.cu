@@ -373,7 +373,21 @@ extern "C" int bw_cyclic_recover(const char* instance_path, const char* op, uint
         std::cout << "A*(source-preconditioned candidate) nonzeros by vector: ";
         for (size_t i = 0; i < v; ++i) std::cout << (i ? ", " : "") << i << ":" << prod_nnz[i];
         std::cout << std::endl;
-        if (prod_total != 0) throw Error("kernel-vector certificate failed", 3);
+        if (prod_total != 0) {
+            // the first ten nonzero entries of F Dc D in row-major order, as
+            // the reference prints them (cuda/cuprym_cyclic_kernel_vectors.cu:1390-1407, 2638-2641)
+            std::cout << "First nonzero entries of certificate product:" << std::endl;
+            size_t printed = 0;
+            for (size_t row = 0; row < nr && printed < 10; ++row)
+                for (size_t col = 0; col < v && printed < 10; ++col) {
+                    const uint32_t value = prod[row * v + col] % p;
+                    if (value != 0) {
+                        std::cout << "  (" << row << ", " << col << ") = " << value << std::endl;
+                        ++printed;
+                    }
+                }
+            throw Error("kernel-vector certificate failed", 3);
+        }
         std::cout << "Kernel-vector certificate passed." << std::endl;
         const std::vector<size_t> cand_nnz = recovery::column_nonzeros(cand, nc, v, p);
         size_t cand_total = 0;

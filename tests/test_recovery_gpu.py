@@ -77,3 +77,42 @@ def test_recovery_matches_reference_binary(sector, tmp_path):
     assert ra == rb
     if sector == 0:
         assert ra["candidate_rank"] >= 1 and sum(ra["product_nonzeros"]) == 0
+
+
+@pytest.mark.parametrize("genus, sector", [(20, 0), (22, 1)])
+def test_paper_size_recovery_arithmetic_matches_reference_binary(genus, sector, tmp_path):
+    """At paper size no generator is known without the bcw solver, so both
+    executables get the same seeded random 4 x 4 generator matrices: then
+    D = sum_k S^k V G_k^t is not in the kernel and both must refuse with the
+    certificate failure, printing the same nonzero count of F Dc D per column
+    (over all rows) and the same first ten nonzero entries."""
+    if not REF_REC.exists():
+        pytest.skip("reference binary not built (oracle/build_ref.sh)")
+    inst = ROOT / "oracle" / "_ref" / "data" / f"g{genus}.json"
+    if not inst.exists():
+        pytest.skip("paper inputs not staged (oracle/build_ref.sh)")
+    seq_dir = tmp_path / "seq"
+    res = _run([str(OUR_SEQ), str(inst), "--sector", str(sector), "--out", str(seq_dir), *RECIPE])
+    assert res.returncode == 0, res.stderr
+    stem = STEM.format(sector)
+    p = json.loads(inst.read_text())["modulus"]
+    rng = np.random.default_rng(genus * 100 + sector)
+    lines = [" ".join(str(int(v)) for v in rng.integers(-p + 1, p, 16)) for _ in range(37)]
+    outs = {}
+    for name, exe in (("ours", OUR_REC), ("ref", REF_REC)):
+        d = tmp_path / f"r_{name}"
+        d.mkdir()
+        for suffix in (".wdm.zst", ".rowmix.json"):
+            shutil.copy(seq_dir / (stem + suffix), d / (stem + suffix))
+        (d / (stem + "_generators.txt")).write_text("\n".join(lines) + "\n")
+        res = _run([str(exe), str(inst), "-f", str(d / (stem + ".wdm.zst")), "--operator", "eliminated",
+                    "--sector", str(sector), "-d", "0"])
+        assert res.returncode == 1, (name, res.stdout[-1000:], res.stderr[-1000:])
+        assert "kernel-vector certificate failed" in res.stderr
+        out = res.stdout.splitlines()
+        counts = next(l for l in out if l.startswith("A*(source-preconditioned candidate) nonzeros by vector:"))
+        first = out.index("First nonzero entries of certificate product:")
+        dims = next(l for l in out if l.startswith("Recovery dimensions:"))
+        outs[name] = (dims, counts, out[first + 1:first + 11])
+    assert outs["ours"] == outs["ref"]
+    assert len(outs["ref"][2]) == 10
