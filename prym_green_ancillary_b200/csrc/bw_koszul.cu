@@ -145,9 +145,11 @@ __global__ void __launch_bounds__(256) gather_mac_kernel(
     }
 }
 
-// Projection a = X^T W (m x n) of one block into seq[*seq_index], with the
-// cross-CTA reduction done by the last CTA to finish (deterministic order).
-//   partials : gridDim.x x m x n  int32 scratch
+// Projection a = X^T W (m x n) of one block into seq[*seq_index].  Every CTA
+// adds its m x n balanced sums into one int32 accumulator with atomics (at
+// most 4 * 148 CTAs x (p-1)/2, far below 2^31: exact, and the same whatever
+// the order of the additions); the last CTA to finish reads and clears it.
+//   partials : m x n int32 accumulator, left at 0 after every launch
 //   counter  : arrival counter, left at 0 after every launch
 template <int NB>
 __global__ void __launch_bounds__(256) project_kernel(
@@ -195,9 +197,9 @@ __global__ void __launch_bounds__(256) project_kernel(
             }
         }
         const int xx = threadIdx.x / JG, jj = threadIdx.x - xx * JG;
-        int32_t* dst = partials + (static_cast<size_t>(blockIdx.x) * m + xx) * NB + jj * 4;
+        int32_t* dst = partials + (static_cast<size_t>(xx) * NB + jj * 4);
 #pragma unroll
-        for (int a = 0; a < 4; ++a) dst[a] = reduce_balanced(s[a], mod);
+        for (int a = 0; a < 4; ++a) atomicAdd(dst + a, reduce_balanced(s[a], mod));
     }
     __threadfence();
     __syncthreads();
@@ -210,14 +212,8 @@ __global__ void __launch_bounds__(256) project_kernel(
     __threadfence();
     const unsigned long long pos = *reinterpret_cast<volatile unsigned long long*>(seq_index);
     const int entries = m * NB;
-    for (int e = threadIdx.x; e < entries; e += blockDim.x) {
-        int32_t s = 0;
-        for (unsigned int b = 0; b < gridDim.x; ++b) {
-            s += reinterpret_cast<volatile int32_t*>(partials)[static_cast<size_t>(b) * entries + e];
-            if ((b & 7) == 7) s = reduce_partial(s, mod);
-        }
-        seq[pos * entries + e] = to_canonical(reduce_balanced(s, mod), mod);
-    }
+    for (int e = threadIdx.x; e < entries; e += blockDim.x)
+        seq[pos * entries + e] = to_canonical(reduce_balanced(atomicExch(partials + e, 0), mod), mod);
     __syncthreads();
     if (threadIdx.x == 0) {
         *seq_index = pos + 1;
@@ -533,6 +529,7 @@ void KoszulCtx::seq_start(const uint32_t* x, const uint32_t* y0, uint32_t* seq, 
     cur_is_a = true;
     BW_CUDA(cudaMemsetAsync(d_seq_index, 0, sizeof(unsigned long long), st));
     BW_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), st));
+    BW_CUDA(cudaMemsetAsync(d_partials, 0, static_cast<size_t>(m) * std::max(nb, nbi) * sizeof(int32_t), st));
     if (form == BW_FORM_INT8) {
         i8_load_x(x, st);
         i8_to_limbs(y0, I8_YA, st);

@@ -845,15 +845,15 @@ __global__ void from_limbs_kernel(const int8_t* __restrict__ lo, const int8_t* _
 //
 // Warps: 0 producer (bulk copies: the stage's X tile and W block runs), 1 MMA
 // issuer (allocates TMEM), 2-5 epilogue (tcgen05.ld + reduction mod p).  The
-// CTA's combined partial goes to partials[blockIdx]; the last CTA to finish
-// reduces them into seq[*seq_index] and advances the index.
+// CTA's combined sums are added into an m x n int32 accumulator; the last CTA
+// to finish writes them to seq[*seq_index], clears them and advances the index.
 constexpr int kProjThreads = 6 * 32;
 constexpr int kProjStageTarget = 32 * 1024;   // bytes of X tile + W runs per stage
 
 struct I8Proj {
     const int8_t* xt;           // [stage][2 MG][KP][16]
     const int8_t* w[2];         // W lo, hi planes: [blk][h][u][16]
-    int32_t* partials;          // [grid][m][NB]
+    int32_t* partials;          // [m][NB] accumulator, zero between launches
     unsigned int* counter;
     uint32_t* seq;
     unsigned long long* seq_index;
@@ -1020,14 +1020,17 @@ __global__ void __launch_bounds__(kProjThreads, 1) i8_project_tc_kernel(I8Proj P
         tc::tc_fence_after();
         tc::tmem_dealloc(tmem, tmem_cols);
     }
-    // x * w = lo*lo + 255 (lo*hi + hi*lo) + 255^2 hi*hi, per (x, j)
+    // x * w = lo*lo + 255 (lo*hi + hi*lo) + 255^2 hi*hi, per (x, j); the
+    // CTA's balanced sums meet in one int32 accumulator by atomics (148 CTAs x
+    // (p-1)/2 stay far below 2^31: exact and order-independent), which the
+    // last CTA reads and clears
     const int entries = P.m * NB;
     const int hi_row = 16 * P.mg;
     for (int e = threadIdx.x; e < entries; e += blockDim.x) {
         const int x = e / NB, j = e - (e / NB) * NB;
         const int32_t ll = red[x * N + j], lh = red[x * N + NB + j];
         const int32_t hl = red[(hi_row + x) * N + j], hh = red[(hi_row + x) * N + NB + j];
-        P.partials[static_cast<size_t>(blockIdx.x) * entries + e] = combine(ll, lh + hl, hh, P.mod, P.c1, P.c2);
+        atomicAdd(P.partials + e, combine(ll, lh + hl, hh, P.mod, P.c1, P.c2));
     }
     __threadfence();
     __syncthreads();
@@ -1038,12 +1041,8 @@ __global__ void __launch_bounds__(kProjThreads, 1) i8_project_tc_kernel(I8Proj P
     const unsigned long long pos = *reinterpret_cast<volatile unsigned long long*>(P.seq_index);
     for (int e = threadIdx.x; e < entries; e += blockDim.x) {
         const int x = e / NB, j = e - (e / NB) * NB;
+        const int32_t sum = atomicExch(P.partials + e, 0);
         if (j >= P.n_out) continue;
-        int32_t sum = 0;
-        for (unsigned b = 0; b < gridDim.x; ++b) {
-            sum += reinterpret_cast<volatile int32_t*>(P.partials)[static_cast<size_t>(b) * entries + e];
-            if ((b & 7) == 7) sum = reduce_partial(sum, P.mod);
-        }
         P.seq[pos * (static_cast<unsigned long long>(P.m) * P.n_out) + x * P.n_out + j] =
             to_canonical(reduce_balanced(sum, P.mod), P.mod);
     }
