@@ -1230,7 +1230,7 @@ bool plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     P.slot_bytes = 2 * P.limb_bytes;
     P.tx_full = static_cast<uint32_t>(16 * gps * inner_pad * 16);              // 2 limbs x 8 columns x rows x 16 B
     P.tx_last = static_cast<uint32_t>(16 * ((last_g + 3) / 4 * 4) * inner_pad * 16);
-    int slots = gather4 ? 8 : 4;
+    int slots = 8;
     while (slots > 1 && P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra > static_cast<size_t>(kMaxSmem))
         --slots;
     if (P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra > static_cast<size_t>(kMaxSmem)) return false;
@@ -1381,6 +1381,8 @@ void plan_projection(KoszulCtx& c, KoszulCtx::I8State& S) {
 
 template <int NB>
 void launch_i8(KoszulCtx& c, KoszulCtx::I8State::Dir& D, const CUtensorMap* maps, cudaStream_t st) {
+    BW_REQUIRE(D.p.inc != nullptr && (!D.gather4 || D.p.rows4 != nullptr) && D.p.b_tiles != nullptr,
+               "internal: INT8 gather tables missing for the chosen producer");
     if (D.gather4)
         i8_gather_hybrid_kernel<NB><<<D.grid, kHyThreads, D.smem, st>>>(maps[0], maps[1], D.p);
     else
@@ -1539,7 +1541,13 @@ void KoszulCtx::i8_setup() {
                 int gps, t_tma;
             };
             std::vector<Cand> cands;
-            if (allow_cp) cands.push_back({false, 0, 0});
+            if (allow_cp) {
+                // the fill heuristic's stage, and fewer or more generators a stage
+                // (smaller stages leave room for more pipeline slots)
+                cands.push_back({false, 0, 0});
+                for (int g : {4, 6, 8, 12})
+                    if (g < r) cands.push_back({false, g, 0});
+            }
             if (allow_g4)
                 for (int gs = 1; gs <= std::min(3, (r + 3) / 4); ++gs)
                     for (int qt = 1; qt <= 3; ++qt) cands.push_back({true, 4 * gs, qt * bt / 4});
@@ -1577,12 +1585,10 @@ void KoszulCtx::i8_setup() {
         text += (text.empty() ? "" : "; ") + std::string(buf);
         if (!tried.empty()) text += " (tuned: " + tried + ")";
     }
-    // the table the chosen producer does not read is freed
+    // the TMA rows are freed when the cp.async producer alone was chosen (the
+    // hybrid producer reads both tables)
     for (I8State::Dir* D : {&S.fwd, &S.bwd}) {
-        if (D->gather4) {
-            release(D->inc);
-            D->inc = nullptr;
-        } else {
+        if (!D->gather4) {
             release(D->rows4);
             D->rows4 = nullptr;
         }
