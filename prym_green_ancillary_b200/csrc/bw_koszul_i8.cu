@@ -79,6 +79,7 @@ enum : int { PL_LO = 0, PL_HI = 1, PL_NLO = 2, PL_NHI = 3 };
 
 struct I8Dir {
     const int8_t* in[4];      // input planes lo, hi, -lo, -hi: [blk][h][inner][16]
+    long long in_neg_off;     // bytes from an input +plane to its -plane (they share one allocation)
     int8_t* out[4];           // output planes, same layout with `outer`
     const uint32_t* inc;      // [n_blk][r]: neighbour rank | negative << 31, or kAbsent
     const int8_t* b_tiles;    // B operand, already in its shared-memory layout
@@ -95,7 +96,7 @@ struct I8Dir {
     Mod mod;
     int32_t c1, c2;              // 255 and 255^2 mod p, balanced
     uint32_t wait_limit;         // tries of every pipeline wait (tc::kWaitLimit outside the failure tests)
-    int hold_first_stage;        // failure tests only: CTA 0 never fills its first stage
+    int hold_first_stage;        // failure tests only: CTA 0's MMA thread never sees its first stage
     // hybrid producer (i8_gather_hybrid_kernel)
     const int4* rows4;           // [n_blk][groups]: plane rows of the four generators of a group (h = 0)
     int groups;                  // ceil(r / 4)
@@ -171,8 +172,9 @@ __host__ __device__ __forceinline__ long long plane_offset(long long blk, int u,
     return blk * (static_cast<long long>(NB) * dim) + static_cast<long long>(j >> 4) * dim * 16 + u * 16 + (j & 15);
 }
 
+// 544 threads x 120 registers fit the SM's 64K (one CTA per SM).
 template <int NB>
-__global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) {
+__global__ void __maxnreg__(120) i8_gather_gemm_kernel(I8Dir P) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int BT = 128 / NB;        // output blocks per tile
     constexpr int HG = NB / 16;         // 16-byte column groups per block row
@@ -247,7 +249,6 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         };
         SlotRing ring(P.slots);
         bool ok = true;
-        bool held = P.hold_first_stage && blockIdx.x == 0;
         uint32_t incr[TPW], incn[TPW];
         load_inc(blockIdx.x, incn);
         for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
@@ -266,10 +267,6 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                     break;
                 }
                 // failure tests: the first stage of CTA 0 is never filled, so its consumer's wait runs out
-                if (held) {   // failure tests: CTA 0's first stage is never filled
-                    held = false;
-                    continue;
-                }
                 const int g_s = min(P.gi, P.r - s * P.gi);
                 const int rows = g_s * P.inner;             // K' rows filled in this stage
                 uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
@@ -288,7 +285,8 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                         // the copy itself (source size 0: nothing is read), so the warp does not diverge
                         const bool present = e != kAbsent;
                         const long long nbr = present ? static_cast<long long>(e & 0x7FFFFFFFu) : 0;
-                        const int neg = (present && (e >> 31)) ? 2 : 0;
+                        // the -plane of a limb lies in_neg_off bytes after its +plane
+                        const long long negoff = (present && (e >> 31)) ? P.in_neg_off : 0;
                         const uint32_t nbytes = present ? 16u : 0u;
 #pragma unroll
                         for (int limb = 0; limb < 2; ++limb)
@@ -296,7 +294,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                             for (int h = 0; h < HG; ++h)
                                 tc::cp_async16_zfill(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
                                                          static_cast<size_t>(h) * KS * 16,
-                                                     P.in[limb + neg] + (nbr * HG + h) * block_bytes + b * 16,
+                                                     P.in[limb] + negoff + (nbr * HG + h) * block_bytes + b * 16,
                                                      nbytes);
                     }
                 }
@@ -312,6 +310,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
             long long tcount = 0;
             SlotRing ring(P.slots);
             bool ok = true;
+            bool held = P.hold_first_stage && blockIdx.x == 0;
             for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
                 const int buf = static_cast<int>(tcount & 1);
                 const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
@@ -321,7 +320,12 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                 for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
                     const int slot = ring.slot;
                     const uint32_t ph = ring.phase;
-                    if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL, P.wait_limit)) {
+                    // failure tests: CTA 0 waits for its first stage on a barrier that
+                    // nothing completes before the final drain, so the wait runs out
+                    uint64_t* wait_bar = (held && s == 0) ? drained : &full[slot];
+                    const uint32_t wait_ph = (held && s == 0) ? 0u : ph;
+                    held = false;
+                    if (!tc::mbar_wait(wait_bar, wait_ph, abort, P.err, tc::ERR_WAIT_FULL, P.wait_limit)) {
                         ok = false;
                         break;
                     }
@@ -468,8 +472,9 @@ constexpr int kHyMmaWarp = kCpWarps + 1;
 constexpr int kHyEpi0 = kCpWarps + 2;
 constexpr int kHyThreads = (kCpWarps + 2 + kEpilogueWarps) * 32;
 
+// 576 threads x 112 registers fit the SM's 64K (one CTA per SM).
 template <int NB>
-__global__ void __launch_bounds__(kHyThreads, 1)
+__global__ void __maxnreg__(112)
     i8_gather_hybrid_kernel(const __grid_constant__ CUtensorMap map_lo, const __grid_constant__ CUtensorMap map_hi,
                             I8Dir P) {
     extern __shared__ __align__(1024) uint8_t smem[];
@@ -547,7 +552,6 @@ __global__ void __launch_bounds__(kHyThreads, 1)
         };
         SlotRing ring(P.slots);
         bool ok = true;
-        bool held = P.hold_first_stage && blockIdx.x == 0;
         uint32_t incn = load_inc(blockIdx.x);
         for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
             const uint32_t incr = incn;
@@ -563,10 +567,6 @@ __global__ void __launch_bounds__(kHyThreads, 1)
                     ok = false;
                     break;
                 }
-                if (held) {   // failure tests: CTA 0's first stage is never filled
-                    held = false;
-                    continue;
-                }
                 if (active) {
                     const bool last = s == P.stages_per_tile - 1;
                     const int rows = (last ? P.groups - s * P.gs : P.gs) * 4 * P.inner_pad;
@@ -581,7 +581,8 @@ __global__ void __launch_bounds__(kHyThreads, 1)
                         const int u = w - il * P.inner_pad;
                         const bool present = e != kAbsent;
                         const long long nbr = present ? static_cast<long long>(e & 0x7FFFFFFFu) : 0;
-                        const int neg = (present && (e >> 31)) ? 2 : 0;
+                        // the -plane of a limb lies in_neg_off bytes after its +plane
+                        const long long negoff = (present && (e >> 31)) ? P.in_neg_off : 0;
                         const uint32_t nbytes = present ? 16u : 0u;
                         uint8_t* dst0 = col0 + static_cast<size_t>(w) * 16;
 #pragma unroll
@@ -590,7 +591,7 @@ __global__ void __launch_bounds__(kHyThreads, 1)
                             for (int h = 0; h < HG; ++h)
                                 tc::cp_async16_zfill(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
                                                          static_cast<size_t>(h) * KS * 16,
-                                                     P.in[limb + neg] + (nbr * HG + h) * block_bytes + u * 16, nbytes);
+                                                     P.in[limb] + negoff + (nbr * HG + h) * block_bytes + u * 16, nbytes);
                     }
                 }
                 tc::cp_async_arrive_noinc(&full[slot]);   // when this thread's copies have landed
@@ -613,7 +614,6 @@ __global__ void __launch_bounds__(kHyThreads, 1)
 #pragma unroll
         for (int q = 0; q < kMaxSlots; ++q) issued[q] = false, issued_phase[q] = 0;
         bool ok = true;
-        bool held = P.hold_first_stage && blockIdx.x == 0;
         for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
             for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
                 const int slot = ring.slot;
@@ -625,10 +625,6 @@ __global__ void __launch_bounds__(kHyThreads, 1)
                 if (!got) {
                     ok = false;
                     break;
-                }
-                if (held) {
-                    held = false;
-                    continue;
                 }
                 const bool last = s == P.stages_per_tile - 1;
                 const int g_n = last ? P.groups - s * P.gs : P.gs;   // groups in this stage
@@ -672,6 +668,7 @@ __global__ void __launch_bounds__(kHyThreads, 1)
             long long tcount = 0;
             SlotRing ring(P.slots);
             bool ok = true;
+            bool held = P.hold_first_stage && blockIdx.x == 0;
             for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
                 const int buf = static_cast<int>(tcount & 1);
                 const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
@@ -681,7 +678,12 @@ __global__ void __launch_bounds__(kHyThreads, 1)
                 for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
                     const int slot = ring.slot;
                     const uint32_t ph = ring.phase;
-                    if (!tc::mbar_wait(&full[slot], ph, abort, P.err, tc::ERR_WAIT_FULL, P.wait_limit)) {
+                    // failure tests: CTA 0 waits for its first stage on a barrier that
+                    // nothing completes before the final drain, so the wait runs out
+                    uint64_t* wait_bar = (held && s == 0) ? drained : &full[slot];
+                    const uint32_t wait_ph = (held && s == 0) ? 0u : ph;
+                    held = false;
+                    if (!tc::mbar_wait(wait_bar, wait_ph, abort, P.err, tc::ERR_WAIT_FULL, P.wait_limit)) {
                         ok = false;
                         break;
                     }
@@ -1632,6 +1634,7 @@ void KoszulCtx::i8_run(bool forward_dir, int in_buf, int out_buf, bool scale, cu
         D.p.in[pl] = i8->planes[in_buf][pl];
         D.p.out[pl] = i8->planes[out_buf][pl];
     }
+    D.p.in_neg_off = i8->planes[in_buf][PL_NLO] - i8->planes[in_buf][PL_LO];
     D.p.diag = (!forward_dir && scale) ? d_diag : nullptr;
     dispatch_i8_nb(nbi, [&](auto NBc) { launch_i8<decltype(NBc)::value>(*this, D, i8->maps[in_buf], st); });
 }
