@@ -714,24 +714,24 @@ def run_engine(args):
     yf_pin = torch.empty((sh["n_src"], sh["n"]), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     pinned_out = (seq_pin, yf_pin)
     seq_h, yf_h = eng.sequence_host(xh_np, yh_np, K + 1, out=pinned_out)
-    e2e_calls = []
-    while sum(e2e_calls) < args.min_ms / 1e3 or len(e2e_calls) < 3:
+
+    def e2e_call():
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         t0 = time.perf_counter()
-        seq_h, yf_h = eng.sequence_host(xh_np, yh_np, K + 1, out=pinned_out)
-        e2e_calls.append(time.perf_counter() - t0)
-        if len(e2e_calls) >= 64:
-            break
-    n_calls = len(e2e_calls)
-    (n_calls,) = max_over_ranks([n_calls], device=dev)
-    while len(e2e_calls) < n_calls:     # every rank makes the same number of barrier calls
-        torch.cuda.synchronize()
-        dist.barrier()
-        t0 = time.perf_counter()
-        seq_h, yf_h = eng.sequence_host(xh_np, yh_np, K + 1, out=pinned_out)
-        e2e_calls.append(time.perf_counter() - t0)
+        out = eng.sequence_host(xh_np, yh_np, K + 1, out=pinned_out)
+        return time.perf_counter() - t0, out
+
+    # one calibration call decides how many timed calls make a second (the
+    # same count on every rank, so the barriers pair up)
+    t_cal, _ = e2e_call()
+    (t_cal,) = max_over_ranks([t_cal], device=dev)
+    n_calls = int(min(64, max(3, -(-args.min_ms / 1e3 // max(t_cal, 1e-6)))))
+    e2e_calls = []
+    for _ in range(n_calls):
+        t, (seq_h, yf_h) = e2e_call()
+        e2e_calls.append(t)
     (e2e_s,) = max_over_ranks([statistics.median(e2e_calls)], device=dev)
     e2e_value = world * K / e2e_s
     h2d = (xh_np.nbytes + yh_np.nbytes) / K
