@@ -808,33 +808,9 @@ void CyclicCtx::gram(const int32_t* a1, const int32_t* c1, const int32_t* a2, co
     ++launches;
 }
 
-// apply_square on the subset path with the application's two Gram moments
-// computed by its backward kernels as they write the output rows: in^t out
-// (out^t in when out_first) and out^t out are appended to the sequence.
-void CyclicCtx::apply_square_moments(const int32_t* in, int32_t* out, bool out_first) {
-    if (xs_for != in) subset_source16(in, d_dc);
-    subset_forward16();
-    subset_precondition16();
-    MomentSink M;
-    M.in = in;
-    M.out_first = out_first ? 1 : 0;
-    M.acc = d_partials;
-    M.counter = d_counter;
-    M.seq = d_seq;
-    M.seq_index = d_seq_index;
-    subset_backward16(d_dc, out, true, &M);
-}
-
 // One round of the reference's loop (cuda/cuprym_cyclic.cu:2443-2449):
-// D = S B; push B^t D, D^t D; B = S D; push B^t D, B^t B.  On the subset
-// path without extra dense columns the moments come from the backward
-// kernels (BW_CYCLIC_FUSED_MOMENTS=0: a Gram kernel after each application).
+// D = S B; push B^t D, D^t D; B = S D; push B^t D, B^t B.
 void CyclicCtx::round() {
-    if (subset_path && S.n_extra == 0 && fused_moments) {
-        apply_square_moments(d_b, d_d, false);   // B^t D, D^t D
-        apply_square_moments(d_d, d_b, true);    // B'^t D, B'^t B'
-        return;
-    }
     apply_square(d_b, d_d);
     gram(d_b, d_d, d_d, d_d, 2);
     apply_square(d_d, d_b);

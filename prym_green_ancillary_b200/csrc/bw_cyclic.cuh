@@ -52,19 +52,6 @@ struct ElimDev {
 //   R [g][n], B [g][kdim], a0 offsets [r+1], a0 indices [g], a1 offsets [r+1],
 //   a1 indices [n], kernel-weight offsets [r+1], indices [kdim], ych [r]
 //   (ych[c] = y character of an (m-1)-subset whose t character is c).
-// Gram moments of one application of S fused into the two kernels that write
-// its output rows (bw_cyclic_subset.cu): the moments in^t out (or out^t in)
-// and out^t out, accumulated as the rows are produced.
-struct MomentSink {
-    const int32_t* in = nullptr;          // the application's input block (compact rows); nullptr: off
-    int out_first = 0;                    // the first moment is out^t in (else in^t out)
-    int32_t* acc = nullptr;               // 20 int32 sums, zero between applications
-    unsigned int* counter = nullptr;      // CTAs of both kernels that have added their sums
-    unsigned int ctas = 0;                // both kernels' CTAs together
-    uint32_t* seq = nullptr;              // packed moments; two are appended at *seq_index
-    unsigned long long* seq_index = nullptr;
-};
-
 struct SubsetDev {
     Mod mod;
     int n, g, kdim, r;
@@ -134,9 +121,6 @@ struct CyclicCtx {
     // The round's kernels start while the kernel before them finishes
     // (programmatic dependent launch; BW_CYCLIC_PDL=0 turns it off).
     bool pdl = true;
-    // The round's Gram moments come from the backward kernels (subset path,
-    // no extra dense columns; BW_CYCLIC_FUSED_MOMENTS=0 runs Gram kernels).
-    bool fused_moments = true;
     SubsetDev S{};
     uint4 *d_xs16 = nullptr, *d_y16 = nullptr, *d_t16 = nullptr, *d_u16 = nullptr, *d_u2_16 = nullptr;
     int32_t* d_zs = nullptr;     // compact z rows and extra columns of the scaled source
@@ -199,8 +183,7 @@ struct CyclicCtx {
     void subset_source16(const int32_t* in, const int32_t* dc);   // d_xs16 / d_zs = dc (.) in
     void subset_forward16();                                        // d_xs16 / d_zs -> d_u16
     void subset_precondition16();
-    void subset_backward16(const int32_t* dc, int32_t* out, bool next_source, const MomentSink* moments = nullptr);
-    void apply_square_moments(const int32_t* in, int32_t* out, bool out_first);
+    void subset_backward16(const int32_t* dc, int32_t* out, bool next_source);
     void subset_pack_u(const int32_t* u32, uint4* u16);       // compact -> padded (u2)
     void subset_unpack_u(const uint4* u16, int32_t* u32);
     void subset_u_to_walk(const int32_t* u32);                 // compact -> d_u16 in locality order

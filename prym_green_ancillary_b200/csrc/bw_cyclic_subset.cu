@@ -341,76 +341,6 @@ __global__ void __launch_bounds__(kThreads) sub_ell_kernel(SubsetDev D, const ui
     }
 }
 
-__device__ __forceinline__ int tri4(int row, int col) { return row * (2 * 4 - row + 1) / 2 + (col - row); }
-
-// Per-thread Gram sums of the rows a thread wrote: m[0..9] = the upper
-// triangle of in^t out (or out^t in), m[10..19] that of out^t out.  Products
-// of balanced residues are below 2^28, so eight of them beside a partially
-// reduced value stay inside int32: reduced every eight rows.
-struct MomAcc {
-    int32_t m[20];
-    int cnt;
-    __device__ __forceinline__ MomAcc() : cnt(0) {
-#pragma unroll
-        for (int e = 0; e < 20; ++e) m[e] = 0;
-    }
-    __device__ __forceinline__ void add(const MomentSink& M, long long row, const int4& o, const Mod& mod) {
-        const int4 i = cyc::ld4(M.in, row);
-        const int4 a = M.out_first ? o : i, c = M.out_first ? i : o;
-        const int av[4] = {a.x, a.y, a.z, a.w}, cv[4] = {c.x, c.y, c.z, c.w}, ov[4] = {o.x, o.y, o.z, o.w};
-#pragma unroll
-        for (int r0 = 0; r0 < 4; ++r0)
-#pragma unroll
-            for (int c0 = r0; c0 < 4; ++c0) {
-                m[tri4(r0, c0)] += av[r0] * cv[c0];
-                m[10 + tri4(r0, c0)] += ov[r0] * ov[c0];
-            }
-        if (++cnt == 8) {
-            cnt = 0;
-#pragma unroll
-            for (int e = 0; e < 20; ++e) m[e] = reduce_partial(m[e], mod);
-        }
-    }
-    // The CTA's sums join the accumulator; the last CTA of both kernels (the
-    // counter reaches M.ctas) writes the two moments, canonical, at *seq_index
-    // and *seq_index + 1, and leaves accumulator and counter at zero.  Every
-    // thread of the CTA calls it.
-    __device__ __forceinline__ void finish(const MomentSink& M, const Mod& mod) {
-        __shared__ int32_t red[kThreads / 32][20];
-        __shared__ bool am_last;
-        const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-#pragma unroll
-        for (int e = 0; e < 20; ++e) {
-            int32_t v = reduce_balanced(m[e], mod);   // 32 values below p/2 in magnitude: no overflow
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-            if (lane == 0) red[warp][e] = reduce_balanced(v, mod);
-        }
-        __syncthreads();
-        if (threadIdx.x < 20) {
-            int32_t v = 0;
-            for (int w = 0; w < kThreads / 32; ++w) v += red[w][threadIdx.x];
-            atomicAdd(M.acc + threadIdx.x, reduce_balanced(v, mod));   // all CTAs: below 3552 * p / 2
-        }
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) am_last = atomicAdd(M.counter, 1u) == M.ctas - 1;
-        __syncthreads();
-        if (!am_last) return;
-        __threadfence();
-        const unsigned long long pos = *reinterpret_cast<volatile unsigned long long*>(M.seq_index);
-        if (threadIdx.x < 20) {
-            const int32_t total = atomicExch(M.acc + threadIdx.x, 0);
-            M.seq[pos * 10 + threadIdx.x] = to_canonical(reduce_balanced(total, mod), mod);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            *M.seq_index = pos + 2;
-            *M.counter = 0;
-            __threadfence();
-        }
-    }
-};
-
 // (m-1)-subset S: its h rows h(S, a) = (D_(m-1)^t u2)(S, a), then
 //   t_adj(S, beta) = sum_a R[a,beta] h(S, a)               (padded t block)
 //   out_z(S, kappa) = dc * sum_a B[a,kappa] h(S, a)        (compact, through op_col)
@@ -422,8 +352,7 @@ __global__ void __launch_bounds__(kThreads) sub_d2_transpose_adjoint_kernel(Subs
                                                                             const int32_t* __restrict__ dc,
                                                                             uint4* __restrict__ t_adj,
                                                                             int32_t* __restrict__ out,
-                                                                            int32_t* __restrict__ next_zs,
-                                                                            MomentSink M) {
+                                                                            int32_t* __restrict__ next_zs) {
     extern __shared__ int32_t sm[];
     const Tables T = stage(D, D.blob_t, sm);
     BW_ITEMS(item, D.n1) {
@@ -467,22 +396,6 @@ __global__ void __launch_bounds__(kThreads) sub_d2_transpose_adjoint_kernel(Subs
             if (next_zs) st4(next_zs, zq0 + q, scale4(o, __ldg(dc + orow), D.mod));   // next source row
         }
     }
-    if (M.in) {
-        // the moments of the z rows this thread wrote, in a second pass (the
-        // 20 sums are not live beside the gather's registers)
-        MomAcc mom;
-        BW_ITEMS(item, D.n1) {
-            const uint32_t d = __ldg(D.m1 + static_cast<uint32_t>(item));
-            const int ych = T.ych[static_cast<int>(d >> 26)];
-            const int nz = T.koff[ych + 1] - T.koff[ych];
-            const long long zfirst = static_cast<long long>(D.x_cols) + (d & kLow26);
-            for (int q = 0; q < nz; ++q) {
-                const long long orow = cyc::op_col(D.drop0, D.drop1, zfirst + q);
-                if (orow >= 0) mom.add(M, orow, reinterpret_cast<const int4*>(out)[orow], D.mod);
-            }
-        }
-        mom.finish(M, D.mod);
-    }
 }
 
 // m-subset S': its x rows out_x(S', a) = -dc * (D_m^t t_adj)(S', a), compact
@@ -492,7 +405,7 @@ template <bool SMALL, bool STREAM>
 __global__ void __launch_bounds__(kThreads) sub_dm_transpose_kernel(SubsetDev D, const uint4* __restrict__ t_adj,
                                                                     const int32_t* __restrict__ dc,
                                                                     int32_t* __restrict__ out,
-                                                                    uint4* __restrict__ next_xs, MomentSink M) {
+                                                                    uint4* __restrict__ next_xs) {
     extern __shared__ int32_t sm[];
     const Tables T = stage(D, D.blob_t, sm);
     BW_ITEMS(item, D.n0) {
@@ -516,21 +429,6 @@ __global__ void __launch_bounds__(kThreads) sub_dm_transpose_kernel(SubsetDev D,
             if (next_xs) nxt[q] = scale4(o, __ldg(dc + orow), D.mod);
         }
         if (next_xs) st_block(next_xs, s, nxt[0], nxt[1]);   // next application's source block
-    }
-    if (M.in) {
-        // the moments of the x rows this thread wrote, in a second pass
-        MomAcc mom;
-        BW_ITEMS(item, D.n0) {
-            const uint32_t d = __ldg(D.m0 + static_cast<uint32_t>(item));
-            const int xch = static_cast<int>(d >> 26);
-            const int nx = T.a0off[xch + 1] - T.a0off[xch];
-            const long long xrow = d & kLow26;
-            for (int q = 0; q < nx; ++q) {
-                const long long orow = cyc::op_col(D.drop0, D.drop1, xrow + q);
-                if (orow >= 0) mom.add(M, orow, reinterpret_cast<const int4*>(out)[orow], D.mod);
-            }
-        }
-        mom.finish(M, D.mod);
     }
 }
 
@@ -786,7 +684,6 @@ void CyclicCtx::setup_subset_path() {
     BW_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
     stream_tables = table_bytes > static_cast<size_t>(l2) / 2;
     if (const char* env = std::getenv("BW_CYCLIC_PDL")) pdl = std::string(env) != "0";
-    if (const char* env = std::getenv("BW_CYCLIC_FUSED_MOMENTS")) fused_moments = std::string(env) != "0";
     // BW_CYCLIC_STREAM_TABLES=1 / =0 forces the evict-first (or the cached)
     // table reads at any size, so that small sectors run either instantiation.
     if (const char* env = std::getenv("BW_CYCLIC_STREAM_TABLES")) {
@@ -854,20 +751,17 @@ void CyclicCtx::subset_precondition16() {
     ++launches;
 }
 
-void CyclicCtx::subset_backward16(const int32_t* dc, int32_t* out, bool next_source, const MomentSink* moments) {
+void CyclicCtx::subset_backward16(const int32_t* dc, int32_t* out, bool next_source) {
     const size_t smem = static_cast<size_t>(S.blob_words) * 4;
-    BW_REQUIRE(!moments || S.n_extra == 0, "internal: fused moments need every output row in the two kernels");
-    MomentSink M = moments ? *moments : MomentSink{};
-    if (moments) M.ctas = grid_for(S.n1) + grid_for(S.n0);
     // next_source (apply_square, dc = the column preconditioner): the kernels
     // also write the next application's source from `out`
     uint4* nxs = next_source ? d_xs16 : nullptr;
     int32_t* nzs = next_source ? d_zs : nullptr;
 #define BW_LAUNCH(A, B)                                                                                       \
     launch_pdl(sub_d2_transpose_adjoint_kernel<A, B>, grid_for(S.n1), smem, S,                               \
-               static_cast<const uint4*>(d_u2_16), dc, d_t16, out, nzs, M);                                   \
+               static_cast<const uint4*>(d_u2_16), dc, d_t16, out, nzs);                                      \
     launch_pdl(sub_dm_transpose_kernel<A, B>, grid_for(S.n0), smem, S, static_cast<const uint4*>(d_t16), dc, \
-               out, nxs, M)
+               out, nxs)
     BW_SUBSET_DISPATCH(BW_LAUNCH);
 #undef BW_LAUNCH
     BW_CHECK_LAUNCH();
