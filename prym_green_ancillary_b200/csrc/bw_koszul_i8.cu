@@ -172,9 +172,8 @@ __host__ __device__ __forceinline__ long long plane_offset(long long blk, int u,
     return blk * (static_cast<long long>(NB) * dim) + static_cast<long long>(j >> 4) * dim * 16 + u * 16 + (j & 15);
 }
 
-// 544 threads x 112 registers leave room in the SM's 64K registers (one CTA per SM).
 template <int NB>
-__global__ void __maxnreg__(112) i8_gather_gemm_kernel(I8Dir P) {
+__global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int BT = 128 / NB;        // output blocks per tile
     constexpr int HG = NB / 16;         // 16-byte column groups per block row
@@ -472,9 +471,8 @@ constexpr int kHyMmaWarp = kCpWarps + 1;
 constexpr int kHyEpi0 = kCpWarps + 2;
 constexpr int kHyThreads = (kCpWarps + 2 + kEpilogueWarps) * 32;
 
-// 576 threads x 104 registers leave room in the SM's 64K registers (one CTA per SM).
 template <int NB>
-__global__ void __maxnreg__(104)
+__global__ void __launch_bounds__(kHyThreads, 1)
     i8_gather_hybrid_kernel(const __grid_constant__ CUtensorMap map_lo, const __grid_constant__ CUtensorMap map_hi,
                             I8Dir P) {
     extern __shared__ __align__(1024) uint8_t smem[];
