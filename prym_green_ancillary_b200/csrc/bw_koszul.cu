@@ -168,17 +168,29 @@ __global__ void __launch_bounds__(256) project_kernel(
 
     int32_t acc[4] = {0, 0, 0, 0};
     if (slice < slices) {
-        int cnt = 0;
-        for (long long row = static_cast<long long>(blockIdx.x) * slices + slice; row < rows;
-             row += static_cast<long long>(gridDim.x) * slices) {
+        // four rows a pass, their loads in flight together; eight products of
+        // balanced residues beside a partially reduced value stay inside int32
+        const long long stride = static_cast<long long>(gridDim.x) * slices;
+        long long row = static_cast<long long>(blockIdx.x) * slices + slice;
+        for (; row + 3 * stride < rows; row += 4 * stride) {
+            int32_t xv[4];
+            int4 w[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                xv[q] = __ldg(X + (row + q * stride) * m + x);
+                w[q] = __ldg(reinterpret_cast<const int4*>(W + (row + q * stride) * NB) + jg);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                acc[0] += xv[q] * w[q].x; acc[1] += xv[q] * w[q].y; acc[2] += xv[q] * w[q].z; acc[3] += xv[q] * w[q].w;
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a) acc[a] = reduce_partial(acc[a], mod);
+        }
+        for (; row < rows; row += stride) {
             const int32_t xv = __ldg(X + row * m + x);
             const int4 w = __ldg(reinterpret_cast<const int4*>(W + row * NB) + jg);
             acc[0] += xv * w.x; acc[1] += xv * w.y; acc[2] += xv * w.z; acc[3] += xv * w.w;
-            if (++cnt == 8) {
-                cnt = 0;
-#pragma unroll
-                for (int a = 0; a < 4; ++a) acc[a] = reduce_partial(acc[a], mod);
-            }
         }
 #pragma unroll
         for (int a = 0; a < 4; ++a) acc[a] = reduce_balanced(acc[a], mod);
