@@ -273,12 +273,15 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                 for (int k = 0; k < TPW; ++k) {
                     const int t = group + k * GROUPS;
                     if (t >= BT) break;
-                    // one K' row: a 16-byte copy per limb and column group from the +plane or
-                    // -plane of the neighbour block, or a zero-filling one (source size 0:
-                    // nothing is read) for an absent generator, so the warp does not diverge
-                    auto copy_row = [&](int w, int il, uint32_t e) {
+                    for (int w0 = sub * 32; w0 < rows; w0 += RPW * 32) {
+                        const int w = w0 + lane;
+                        const int il = il_of_row[min(w, rows - 1)];
+                        const uint32_t e = __shfl_sync(0xffffffffu, incr[k], s * P.gi + il);
+                        if (w >= rows) continue;
                         const int b = w - il * P.inner;
                         uint8_t* dst0 = slotA + static_cast<size_t>(t * HG) * KS * 16 + static_cast<size_t>(w) * 16;
+                        // one code path for every lane: an absent generator's rows are zero-filled by
+                        // the copy itself (source size 0: nothing is read), so the warp does not diverge
                         const bool present = e != kAbsent;
                         const long long nbr = present ? static_cast<long long>(e & 0x7FFFFFFFu) : 0;
                         // the -plane of a limb lies in_neg_off bytes after its +plane
@@ -292,15 +295,6 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                                                          static_cast<size_t>(h) * KS * 16,
                                                      P.in[limb] + negoff + (nbr * HG + h) * block_bytes + b * 16,
                                                      nbytes);
-                    };
-                    // two rows a lane per pass: their address chains overlap
-                    for (int w0 = sub * 32; w0 < rows; w0 += 2 * RPW * 32) {
-                        const int wa = w0 + lane, wb = w0 + RPW * 32 + lane;
-                        const int ila = il_of_row[min(wa, rows - 1)], ilb = il_of_row[min(wb, rows - 1)];
-                        const uint32_t ea = __shfl_sync(0xffffffffu, incr[k], s * P.gi + ila);
-                        const uint32_t eb = __shfl_sync(0xffffffffu, incr[k], s * P.gi + ilb);
-                        if (wa < rows) copy_row(wa, ila, ea);
-                        if (wb < rows) copy_row(wb, ilb, eb);
                     }
                 }
                 tc::cp_async_arrive_noinc(&full[slot]);   // when this thread's copies have landed
@@ -575,7 +569,13 @@ __global__ void __launch_bounds__(kHyThreads, 1)
                     const bool last = s == P.stages_per_tile - 1;
                     const int rows = (last ? P.groups - s * P.gs : P.gs) * 4 * P.inner_pad;
                     uint8_t* col0 = sA + static_cast<size_t>(slot) * P.slot_bytes + static_cast<size_t>(t * HG) * KS * 16;
-                    auto copy_row = [&](int w, int il, uint32_t e) {
+                    for (int w0 = sub * 32; w0 < rows; w0 += wpb * 32) {
+                        const int w = w0 + lane;
+                        const int il = il_of_row[min(w, rows - 1)];
+                        const int gen = s * P.gi + (il == 255 ? 0 : il);
+                        const uint32_t e = __shfl_sync(0xffffffffu, incr, min(gen, 31));
+                        // padding rows and generators past r: their B rows are zero, nothing to copy
+                        if (w >= rows || il == 255 || gen >= P.r) continue;
                         const int u = w - il * P.inner_pad;
                         const bool present = e != kAbsent;
                         const long long nbr = present ? static_cast<long long>(e & 0x7FFFFFFFu) : 0;
@@ -590,17 +590,6 @@ __global__ void __launch_bounds__(kHyThreads, 1)
                                 tc::cp_async16_zfill(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
                                                          static_cast<size_t>(h) * KS * 16,
                                                      P.in[limb] + negoff + (nbr * HG + h) * block_bytes + u * 16, nbytes);
-                    };
-                    // two rows a lane per pass: their address chains overlap
-                    for (int w0 = sub * 32; w0 < rows; w0 += 2 * wpb * 32) {
-                        const int wa = w0 + lane, wb = w0 + wpb * 32 + lane;
-                        const int ila = il_of_row[min(wa, rows - 1)], ilb = il_of_row[min(wb, rows - 1)];
-                        const int gena = s * P.gi + (ila == 255 ? 0 : ila), genb = s * P.gi + (ilb == 255 ? 0 : ilb);
-                        const uint32_t ea = __shfl_sync(0xffffffffu, incr, min(gena, 31));
-                        const uint32_t eb = __shfl_sync(0xffffffffu, incr, min(genb, 31));
-                        // padding rows and generators past r: their B rows are zero, nothing to copy
-                        if (wa < rows && ila != 255 && gena < P.r) copy_row(wa, ila, ea);
-                        if (wb < rows && ilb != 255 && genb < P.r) copy_row(wb, ilb, eb);
                     }
                 }
                 tc::cp_async_arrive_noinc(&full[slot]);   // when this thread's copies have landed
