@@ -521,7 +521,6 @@ template int16_t* KoszulCtx::alloc<int16_t>(uint64_t);
 template int* KoszulCtx::alloc<int>(uint64_t);
 template uint32_t* KoszulCtx::alloc<uint32_t>(uint64_t);
 template int4* KoszulCtx::alloc<int4>(uint64_t);
-template uint8_t* KoszulCtx::alloc<uint8_t>(uint64_t);
 
 void KoszulCtx::release(void* p) {
     auto it = std::find(allocations.begin(), allocations.end(), p);

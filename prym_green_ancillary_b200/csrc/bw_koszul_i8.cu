@@ -48,7 +48,6 @@
 // copies and MMAs are drained and TMEM is freed.
 #include "bw_koszul.cuh"
 #include "tc_sm100.cuh"
-#include "tile_groups.hpp"
 
 #include <cuda.h>   // CUtensorMap and cuTensorMapEncodeTiled's types (the function is reached through the runtime)
 
@@ -57,7 +56,6 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
-#include <memory>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -107,16 +105,6 @@ struct I8Dir {
     int32_t row_oob;             // a plane row past the input tensor (2 * input blocks * HG): zero-filled
     int t_tma;                   // hybrid producer: output blocks of a tile gathered by TMA (the rest by cp.async)
     uint32_t tx_full, tx_last;   // bytes a full / the last stage of a tile receives
-    // grouped tiles (i8_gather_gemm_kernel<NB, true>): a tile's blocks share most of their generators, and
-    // its K runs over the union of them only.  `inc` is then [tile * BT + t][g], the entry of the tile's
-    // g-th union generator for its t-th block (kAbsent past the union and for an empty position).
-    const int32_t* tile_blk;     // [n_tiles * BT]: output block of each tile position, or -1
-    const uint8_t* tile_gens;    // [n_tiles][32]: the tile's union generators, ascending
-    const uint8_t* tile_ngen;    // [n_tiles]: size of the union
-    long long n_tiles;
-    int cpg;                     // 16-row K chunks of a generator (inner_pad / 16)
-    uint32_t chunk_bytes;        // bytes of one K chunk of B (N x 16)
-    uint32_t zero_chunk;         // offset of an all-zero K chunk of B
 };
 
 // Position in a ring of pipeline slots: slot index and the parity of its
@@ -184,16 +172,7 @@ __host__ __device__ __forceinline__ long long plane_offset(long long blk, int u,
     return blk * (static_cast<long long>(NB) * dim) + static_cast<long long>(j >> 4) * dim * 16 + u * 16 + (j & 15);
 }
 
-// Byte g (< 32) of a 32-byte list held in eight registers.
-__device__ __forceinline__ uint32_t pick_byte(const uint32_t (&w)[8], int g) {
-    uint32_t v = w[0];
-#pragma unroll
-    for (int q = 1; q < 8; ++q)
-        if ((g >> 2) == q) v = w[q];
-    return (v >> (8 * (g & 3))) & 0xFFu;
-}
-
-template <int NB, bool GROUPED>
+template <int NB>
 __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int BT = 128 / NB;        // output blocks per tile
@@ -211,8 +190,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
     uint8_t* il_of_row = reinterpret_cast<uint8_t*>(tmem_slot + 4);   // K' row of a slot -> generator slot
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const long long n_tiles = GROUPED ? P.n_tiles : (P.n_blk + BT - 1) / BT;
-    const long long n_pos = GROUPED ? P.n_tiles * BT : P.n_blk;   // rows of the incidence table
+    const long long n_tiles = (P.n_blk + BT - 1) / BT;
 
     // B operand: global -> shared (generic stores, made visible to the tensor core below)
     for (uint32_t off = threadIdx.x * 16; off < P.b_bytes; off += blockDim.x * 16)
@@ -263,28 +241,20 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
 #pragma unroll
             for (int k = 0; k < TPW; ++k) {
                 const int t = group + k * GROUPS;
-                const long long pos = tile * BT + t;
-                dst[k] = (tile < n_tiles && t < BT && pos < n_pos && lane < P.r) ? __ldg(P.inc + pos * P.r + lane)
-                                                                                : kAbsent;
+                const long long blk = tile * BT + t;
+                dst[k] = (tile < n_tiles && t < BT && blk < P.n_blk && lane < P.r) ? __ldg(P.inc + blk * P.r + lane)
+                                                                                  : kAbsent;
             }
-        };
-        // generators in a tile's K: all r, or (grouped tiles) the size of the tile's union
-        auto load_ngen = [&](long long tile) {
-            return (GROUPED && tile < n_tiles) ? static_cast<int>(__ldg(P.tile_ngen + tile)) : P.r;
         };
         SlotRing ring(P.slots);
         bool ok = true;
         uint32_t incr[TPW], incn[TPW];
         load_inc(blockIdx.x, incn);
-        int ngen_n = load_ngen(blockIdx.x);
         for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
 #pragma unroll
             for (int k = 0; k < TPW; ++k) incr[k] = incn[k];
-            const int ngen = ngen_n;
             load_inc(tile + gridDim.x, incn);
-            ngen_n = load_ngen(tile + gridDim.x);
-            const int stages = GROUPED ? (ngen + P.gi - 1) / P.gi : P.stages_per_tile;
-            for (int s = 0; s < stages; ++s, ring.next()) {
+            for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
                 const int slot = ring.slot;
                 const uint32_t ph = ring.phase;
                 int got = 1;
@@ -296,7 +266,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                     break;
                 }
                 // failure tests: the first stage of CTA 0 is never filled, so its consumer's wait runs out
-                const int g_s = min(P.gi, ngen - s * P.gi);
+                const int g_s = min(P.gi, P.r - s * P.gi);
                 const int rows = g_s * P.inner;             // K' rows filled in this stage
                 uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
 #pragma unroll
@@ -309,10 +279,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                         const uint32_t e = __shfl_sync(0xffffffffu, incr[k], s * P.gi + il);
                         if (w >= rows) continue;
                         const int b = w - il * P.inner;
-                        // grouped tiles: a generator spans inner_pad rows (whole K chunks); the rows past
-                        // inner are not written (B is zero there)
-                        const int row = GROUPED ? w + il * (P.inner_pad - P.inner) : w;
-                        uint8_t* dst0 = slotA + static_cast<size_t>(t * HG) * KS * 16 + static_cast<size_t>(row) * 16;
+                        uint8_t* dst0 = slotA + static_cast<size_t>(t * HG) * KS * 16 + static_cast<size_t>(w) * 16;
                         // one code path for every lane: an absent generator's rows are zero-filled by
                         // the copy itself (source size 0: nothing is read), so the warp does not diverge
                         const bool present = e != kAbsent;
@@ -346,21 +313,10 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
             for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++tcount) {
                 const int buf = static_cast<int>(tcount & 1);
                 const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
-                // grouped tiles: the tile's union generators (one byte each) and their count
-                uint32_t gw[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                int ngen = P.r;
-                if constexpr (GROUPED) {
-                    const uint4* gp = reinterpret_cast<const uint4*>(P.tile_gens + tile * 32);
-                    const uint4 g0 = __ldg(gp), g1 = __ldg(gp + 1);
-                    gw[0] = g0.x; gw[1] = g0.y; gw[2] = g0.z; gw[3] = g0.w;
-                    gw[4] = g1.x; gw[5] = g1.y; gw[6] = g1.z; gw[7] = g1.w;
-                    ngen = __ldg(P.tile_ngen + tile);
-                }
-                const int stages = GROUPED ? (ngen + P.gi - 1) / P.gi : P.stages_per_tile;
                 if (!tc::mbar_wait(&accempty[buf], aph ^ 1u, abort, P.err, tc::ERR_WAIT_ACCUM_FREE, P.wait_limit)) break;
                 tc::tc_fence_after();
                 const uint32_t dbase = tmem + static_cast<uint32_t>(buf * 2 * N);
-                for (int s = 0; s < stages; ++s, ring.next()) {
+                for (int s = 0; s < P.stages_per_tile; ++s, ring.next()) {
                     const int slot = ring.slot;
                     const uint32_t ph = ring.phase;
                     // failure tests: CTA 0 waits for its first stage on a barrier that
@@ -374,40 +330,6 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                     }
                     tc::fence_proxy_async_smem();
                     tc::tc_fence_after();
-                    if constexpr (GROUPED) {
-                        // K chunk c of the stage belongs to union generator s * gi + c / cpg; its rows of
-                        // B sit at that generator's chunk of the resident maps.  A K-step pairs two
-                        // chunks (the descriptor's K-direction stride LBO is their distance, always
-                        // positive: generators ascend), the second an all-zero chunk past the stage's end.
-                        const int g_s = min(P.gi, ngen - s * P.gi);
-                        const int nch = g_s * P.cpg;
-                        int g = s * P.gi, loc = 0;
-                        auto next_chunk = [&]() {
-                            const uint32_t addr = sB0 + (pick_byte(gw, g) * static_cast<uint32_t>(P.cpg) +
-                                                         static_cast<uint32_t>(loc)) * P.chunk_bytes;
-                            if (++loc == P.cpg) {
-                                loc = 0;
-                                ++g;
-                            }
-                            return addr;
-                        };
-                        const uint32_t a_slot = sA0 + static_cast<uint32_t>(slot) * P.slot_bytes;
-                        for (int ks = 0; 2 * ks < nch; ++ks) {
-                            const uint32_t b0 = next_chunk();
-                            const uint32_t b1 = (2 * ks + 1 < nch) ? next_chunk() : sB0 + P.zero_chunk;
-                            const uint64_t bd = tc::smem_desc(b0, b1 - b0, 128u);
-#pragma unroll
-                            for (int limb = 0; limb < 2; ++limb) {
-                                const uint64_t ad =
-                                    tc::smem_desc(a_slot + static_cast<uint32_t>(limb) * P.limb_bytes + ks * 512u, 128u,
-                                                  static_cast<uint32_t>(KS) * 16u);
-                                tc::mma_i8(dbase + static_cast<uint32_t>(limb * N), ad, bd, idesc,
-                                           (s > 0 || ks > 0) ? 1u : 0u);
-                            }
-                        }
-                        tc::mma_commit(&empty[slot]);
-                        continue;
-                    }
                     const int ks_n = (s == P.stages_per_tile - 1) ? P.ks_last : P.ks_full;
                     for (int limb = 0; limb < 2; ++limb) {
                         const uint32_t a_base = sA0 + static_cast<uint32_t>(slot) * P.slot_bytes +
@@ -447,8 +369,8 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++tcount) {
             const int buf = static_cast<int>(tcount & 1);
             const uint32_t aph = static_cast<uint32_t>((tcount >> 1) & 1);
-            const long long blk = GROUPED ? static_cast<long long>(__ldg(P.tile_blk + tile * BT + t)) : tile * BT + t;
-            const bool valid = GROUPED ? blk >= 0 : blk < P.n_blk;
+            const long long blk = tile * BT + t;
+            const bool valid = blk < P.n_blk;
             // prefetch the diagonal entries of this warp's first chunk before waiting for the accumulator
             int32_t dg[16];
             auto load_diag = [&](int c) {
@@ -1178,17 +1100,8 @@ struct KoszulCtx::I8State {
         uint32_t* inc = nullptr;
         int4* rows4 = nullptr;     // TMA gather rows per group of four generators
         bool gather4 = false;      // hybrid producer (TMA gathers beside cp.async warps), else cp.async only
-        bool grouped = false;      // grouped tiles (cp.async producer, K over each tile's union of generators)
-        // grouped tiles: compact incidence [tile * BT + t][g], tile positions, union lists
-        uint32_t* ginc = nullptr;
-        int32_t* tile_blk = nullptr;
-        uint8_t* tile_gens = nullptr;
-        uint8_t* tile_ngen = nullptr;
-        long long n_tiles = 0;
-        double mean_union = 0;
         size_t smem = 0;
         unsigned grid = 0;
-        unsigned grid_grouped = 0;
     } fwd, bwd;
     // Y_a, Y_b, Z: lo, hi, -lo, -hi; each -plane directly follows its +plane in
     // memory, so that one tensor map covers both signs of a limb
@@ -1215,7 +1128,6 @@ struct TuneKey {
 };
 struct TuneChoice {
     bool gather4 = false;   // the hybrid producer
-    bool grouped = false;   // grouped tiles
     int gps = 0;            // generators per stage
     int t_tma = 0;          // hybrid: blocks of a tile gathered by TMA
     double ms = 0;
@@ -1362,118 +1274,6 @@ bool plan_direction(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int out
     return true;
 }
 
-// Plans one direction with grouped tiles (i8_gather_gemm_kernel<NB, true>):
-// `gps` generators a stage, each padded to whole 16-row K chunks (inner_pad =
-// inner rounded up to 16; its pad rows are never written, B is zero there).
-// B holds every generator's chunks side by side, [generator][chunk][N][16],
-// plus one all-zero chunk at the end; a K-step's descriptor picks its two
-// chunks by address.  Returns false when the maps and stages do not fit.
-bool plan_direction_grouped(KoszulCtx& c, KoszulCtx::I8State::Dir& D, int inner, int outer, bool transpose_maps,
-                            int gps) {
-    I8Dir& P = D.p;
-    P.r = c.r;
-    P.inner = inner;
-    P.outer = outer;
-    P.half = (outer + 15) / 16 * 16;
-    const int N = 2 * P.half;
-    BW_REQUIRE(N <= 256, "INT8 form: output dimension above 128 is not supported");
-    const size_t extra = (2 * 8 + 2 * 2 + 1) * 8 + 16 + kMaxRowTable;
-    if (gps < 1 || gps > c.r) return false;
-    P.inner_pad = (inner + 15) / 16 * 16;
-    P.cpg = P.inner_pad / 16;
-    P.chunk_bytes = static_cast<uint32_t>(N) * 16;
-    P.gi = gps;
-    P.ks_full = (gps * P.cpg + 1) / 2;
-    P.ks_last = P.ks_full;
-    P.stages_per_tile = (c.r + gps - 1) / gps;   // an upper bound; each tile runs ceil(union / gps) stages
-    const int KS = P.ks_full * 32;
-    if (KS > kMaxRowTable) return false;
-    P.zero_chunk = static_cast<uint32_t>(c.r * P.cpg) * P.chunk_bytes;
-    P.b_bytes = P.zero_chunk + P.chunk_bytes;
-    P.limb_bytes = static_cast<uint32_t>(8 * KS * 16);
-    P.slot_bytes = 2 * P.limb_bytes;
-    int slots = 8;
-    while (slots > 1 && P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra > static_cast<size_t>(kMaxSmem))
-        --slots;
-    if (P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra > static_cast<size_t>(kMaxSmem)) return false;
-    // a K-step's LBO (the distance of its two chunks) must fit the descriptor's 14-bit field of 16-byte units
-    BW_REQUIRE(P.b_bytes < (1u << 18), "internal: grouped B operand above the descriptor's reach");
-    P.slots = slots;
-    D.smem = P.b_bytes + static_cast<size_t>(slots) * P.slot_bytes + extra;
-    D.gather4 = false;
-    D.grouped = true;
-    P.t_tma = 0;
-    P.mod = c.mod;
-    P.c1 = to_balanced(255u % c.p, c.mod);
-    P.c2 = to_balanced(static_cast<uint32_t>((255ull * 255ull) % c.p), c.mod);
-
-    std::vector<int8_t> B(P.b_bytes, 0);
-    for (int i = 0; i < c.r; ++i)
-        for (int lc = 0; lc < P.cpg; ++lc)
-            for (int kk = 0; kk < 16; ++kk) {
-                const int u = lc * 16 + kk;
-                if (u >= inner) continue;   // pad rows of the generator's last chunk stay zero
-                for (int n = 0; n < N; ++n) {
-                    const int o = n % P.half;
-                    if (o >= outer) continue;
-                    const uint32_t raw = transpose_maps
-                                             ? c.maps_canonical[(static_cast<size_t>(i) * c.co + u) * c.ci + o]
-                                             : c.maps_canonical[(static_cast<size_t>(i) * c.co + o) * c.ci + u];
-                    int8_t lo, hi;
-                    split_limbs(to_balanced(raw % c.p, c.mod), lo, hi);
-                    const size_t off = static_cast<size_t>(i * P.cpg + lc) * P.chunk_bytes + (n / 8) * 128 +
-                                       (n % 8) * 16 + kk;
-                    B[off] = n < P.half ? lo : hi;
-                }
-            }
-    D.b_tiles = c.alloc<int8_t>(P.b_bytes);
-    BW_CUDA(cudaMemcpyAsync(D.b_tiles, B.data(), B.size(), cudaMemcpyHostToDevice, c.own_stream));
-    BW_CUDA(cudaStreamSynchronize(c.own_stream));
-    P.b_tiles = D.b_tiles;
-    P.tile_blk = D.tile_blk;
-    P.tile_gens = D.tile_gens;
-    P.tile_ngen = D.tile_ngen;
-    P.n_tiles = D.n_tiles;
-    return true;
-}
-
-// Tile groups per operator shape, shared by every context of the process
-// (the grouping depends only on r, k, the direction and the tile's blocks).
-std::mutex g_group_mutex;
-std::map<std::tuple<int, int, int, int>, std::shared_ptr<const TileGroups>> g_group_cache;
-
-std::shared_ptr<const TileGroups> tile_groups_for(const std::vector<uint32_t>& inc, uint64_t n_blk, int r, int k,
-                                                  int dir, int bt) {
-    const auto key = std::make_tuple(r, k, dir, bt);
-    {
-        std::lock_guard<std::mutex> lock(g_group_mutex);
-        const auto it = g_group_cache.find(key);
-        if (it != g_group_cache.end()) return it->second;
-    }
-    std::vector<uint32_t> present(n_blk, 0);
-    for (uint64_t b = 0; b < n_blk; ++b)
-        for (int i = 0; i < r; ++i)
-            if (inc[b * r + i] != kAbsent) present[b] |= 1u << i;
-    auto G = std::make_shared<const TileGroups>(group_tiles(present, r, bt));
-    // every block exactly once, and inside its tile's union
-    std::vector<uint8_t> seen(n_blk, 0);
-    for (uint64_t t = 0; t < G->n_tiles(); ++t) {
-        uint32_t u = 0;
-        for (int g = 0; g < G->ngen[t]; ++g) u |= 1u << G->gens[t * 32 + g];
-        for (int q = 0; q < bt; ++q) {
-            const int32_t b = G->blk[t * bt + q];
-            if (b < 0) continue;
-            BW_REQUIRE(static_cast<uint64_t>(b) < n_blk && !seen[b] && (present[b] & ~u) == 0,
-                       "internal: tile grouping is not a partition of the blocks");
-            seen[b] = 1;
-        }
-    }
-    for (uint64_t b = 0; b < n_blk; ++b) BW_REQUIRE(seen[b], "internal: tile grouping misses a block");
-    std::lock_guard<std::mutex> lock(g_group_mutex);
-    g_group_cache[key] = G;
-    return G;
-}
-
 // Rows of the TMA gathers: for output block blk and group g (generators
 // 4g..4g+3), the plane row of each generator's neighbour run at h = 0:
 // neg * n_blk_in * HG + nbr * HG, or one past the last row (zero-filled) for an
@@ -1581,16 +1381,12 @@ void plan_projection(KoszulCtx& c, KoszulCtx::I8State& S) {
 
 template <int NB>
 void launch_i8(KoszulCtx& c, KoszulCtx::I8State::Dir& D, const CUtensorMap* maps, cudaStream_t st) {
-    BW_REQUIRE(D.p.inc != nullptr && (!D.gather4 || D.p.rows4 != nullptr) && D.p.b_tiles != nullptr &&
-                   (!D.grouped || (D.p.tile_blk != nullptr && D.p.tile_gens != nullptr && D.p.tile_ngen != nullptr &&
-                                   D.p.inc == D.ginc)),
+    BW_REQUIRE(D.p.inc != nullptr && (!D.gather4 || D.p.rows4 != nullptr) && D.p.b_tiles != nullptr,
                "internal: INT8 gather tables missing for the chosen producer");
-    if (D.grouped)
-        i8_gather_gemm_kernel<NB, true><<<D.grid_grouped, kI8Threads, D.smem, st>>>(D.p);
-    else if (D.gather4)
+    if (D.gather4)
         i8_gather_hybrid_kernel<NB><<<D.grid, kHyThreads, D.smem, st>>>(maps[0], maps[1], D.p);
     else
-        i8_gather_gemm_kernel<NB, false><<<D.grid, kI8Threads, D.smem, st>>>(D.p);
+        i8_gather_gemm_kernel<NB><<<D.grid, kI8Threads, D.smem, st>>>(D.p);
     BW_CHECK_LAUNCH();
     ++c.launches;
 }
@@ -1667,51 +1463,6 @@ void KoszulCtx::i8_setup() {
     S.bwd.rows4 = upload_rows(bwd, n_s, n_t);
     S.fwd.inc = upload_inc(fwd);
     S.bwd.inc = upload_inc(bwd);
-    // Producers the autotuner may choose from: BW_I8_PRODUCER=cpasync, =hybrid
-    // or =grouped restricts it to one (tests and measurements of one form).
-    bool allow_g4 = true, allow_cp = true, allow_gr = true, tune = true;
-    if (const char* e = std::getenv("BW_I8_PRODUCER")) {
-        const std::string v(e);
-        if (v == "cpasync" || v == "hybrid" || v == "grouped") {
-            allow_cp = v == "cpasync";
-            allow_g4 = v == "hybrid";
-            allow_gr = v == "grouped";
-        }
-    }
-    if (const char* e = std::getenv("BW_I8_TUNE")) tune = std::string(e) != "0";
-    const int bt = 128 / nbi;
-    // Grouped tiles: the partition of each direction's output blocks, the
-    // compact incidence rows of its tile positions and the union lists.
-    auto upload_groups = [&](I8State::Dir& D, const std::vector<uint32_t>& inc, uint64_t n_blk, int dir) {
-        const auto G = tile_groups_for(inc, n_blk, r, k, dir, bt);
-        const uint64_t nt = G->n_tiles();
-        std::vector<uint32_t> ginc(nt * bt * r, kAbsent);
-        for (uint64_t t = 0; t < nt; ++t)
-            for (int q = 0; q < bt; ++q) {
-                const int32_t b = G->blk[t * bt + q];
-                if (b < 0) continue;
-                for (int g = 0; g < G->ngen[t]; ++g)
-                    ginc[(t * bt + q) * r + g] = inc[static_cast<uint64_t>(b) * r + G->gens[t * 32 + g]];
-            }
-        auto up = [&](const auto& v) {
-            using T = typename std::decay_t<decltype(v)>::value_type;
-            T* d = alloc<T>(v.size());
-            BW_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, own_stream));
-            return d;
-        };
-        D.ginc = up(ginc);
-        D.tile_blk = up(G->blk);
-        D.tile_gens = up(G->gens);
-        D.tile_ngen = up(G->ngen);
-        BW_CUDA(cudaStreamSynchronize(own_stream));
-        D.n_tiles = static_cast<long long>(nt);
-        D.mean_union = G->mean_union();
-        D.grid_grouped = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(nt, sms)));
-    };
-    if (allow_gr) {
-        upload_groups(S.fwd, fwd, n_t, 0);
-        upload_groups(S.bwd, bwd, n_s, 1);
-    }
     for (int b = 0; b < 3; ++b) {
         const uint64_t n_blk = b < 2 ? n_s : n_t;
         const int dim = b < 2 ? ci : co;
@@ -1731,14 +1482,14 @@ void KoszulCtx::i8_setup() {
     int hold = 0;
     if (const char* e = std::getenv("BW_TEST_HOLD_FIRST_STAGE")) hold = (*e && std::string(e) != "0") ? 1 : 0;
     S.proj.wait_limit = wait_limit;
-    int cap_g = 0, cap_4 = 0, cap_gr = 0;
+    int cap_g = 0, cap_4 = 0;
     dispatch_i8_nb(nbi, [&](auto NBc) {
-        cap_g = allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value, false>, device);
-        cap_gr = allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value, true>, device);
+        cap_g = allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value>, device);
         cap_4 = allow_dynamic_smem(i8_gather_hybrid_kernel<decltype(NBc)::value>, device);
         const int cap_p = allow_dynamic_smem(i8_project_tc_kernel<decltype(NBc)::value>, device);
         BW_REQUIRE(static_cast<int>(S.proj_smem) <= cap_p, "INT8 form: shared-memory plan above the device limit");
     });
+    const int bt = 128 / nbi;
     S.fwd.p.n_blk = static_cast<long long>(n_t);
     S.bwd.p.n_blk = static_cast<long long>(n_s);
     S.fwd.p.row_oob = static_cast<int32_t>(2 * n_s * hg);   // the forward gathers Y (source blocks)
@@ -1753,74 +1504,67 @@ void KoszulCtx::i8_setup() {
     // shape for the life of the process.  BW_I8_TUNE=0 takes the fill
     // heuristic instead; BW_I8_PRODUCER=cpasync or =hybrid restricts the
     // producer.
+    bool allow_g4 = true, allow_cp = true, tune = true;
+    if (const char* e = std::getenv("BW_I8_PRODUCER")) {
+        allow_g4 = std::string(e) != "cpasync";
+        allow_cp = std::string(e) != "hybrid";
+    }
+    if (const char* e = std::getenv("BW_I8_TUNE")) tune = std::string(e) != "0";
     std::string text;
     for (int dir = 0; dir < 2; ++dir) {
         I8State::Dir& D = dir == 0 ? S.fwd : S.bwd;
         const int inner = dir == 0 ? ci : co, outer = dir == 0 ? co : ci;
         const int in_buf = dir == 0 ? I8_YA : I8_Z, out_buf = dir == 0 ? I8_Z : I8_YB;
-        auto plan = [&](bool g4, int gps, int t_tma, bool grouped) {
+        auto plan = [&](bool g4, int gps, int t_tma) {
             if (D.b_tiles) release(D.b_tiles);
             D.b_tiles = nullptr;
-            if (grouped) {
-                if (!plan_direction_grouped(*this, D, inner, outer, dir == 1, gps)) return false;
-                if (static_cast<int>(D.smem) > cap_gr) return false;
-            } else {
-                if (!plan_direction(*this, D, inner, outer, dir == 1, g4, gps)) return false;
-                if (static_cast<int>(D.smem) > (g4 ? cap_4 : cap_g)) return false;
-                D.grouped = false;
-            }
+            if (!plan_direction(*this, D, inner, outer, dir == 1, g4, gps)) return false;
+            if (static_cast<int>(D.smem) > (g4 ? cap_4 : cap_g)) return false;
             D.p.t_tma = g4 ? t_tma : 0;
             D.p.err = S.err;
             D.p.wait_limit = wait_limit;
             D.p.hold_first_stage = 0;
-            D.p.inc = grouped ? D.ginc : D.inc;
+            D.p.inc = D.inc;
             D.p.rows4 = D.rows4;
             return true;
         };
-        const TuneKey key{r, k, inner, outer, nbi, dir, sms,
-                          (allow_g4 ? 1 : 0) | (allow_cp ? 2 : 0) | (allow_gr ? 4 : 0)};
+        const TuneKey key{r, k, inner, outer, nbi, dir, sms, (allow_g4 ? 1 : 0) | (allow_cp ? 2 : 0)};
         TuneChoice choice{};
         bool have = tune && tune_lookup(key, choice);
         std::string tried;
         if (!have && tune) {
             // candidates: the cp.async producer with its heuristic stage; the
             // hybrid producer with 1..3 groups of four generators a stage and a
-            // quarter, half or three quarters of a tile's blocks gathered by TMA;
-            // grouped tiles with 2..8 generators a stage
+            // quarter, half or three quarters of a tile's blocks gathered by TMA
             struct Cand {
                 bool g4;
                 int gps, t_tma;
-                bool grouped;
             };
             std::vector<Cand> cands;
             if (allow_cp) {
                 // the fill heuristic's stage, and fewer or more generators a stage
                 // (smaller stages leave room for more pipeline slots)
-                cands.push_back({false, 0, 0, false});
+                cands.push_back({false, 0, 0});
                 for (int g : {4, 6, 8, 12})
-                    if (g < r) cands.push_back({false, g, 0, false});
+                    if (g < r) cands.push_back({false, g, 0});
             }
             if (allow_g4)
                 for (int gs = 1; gs <= std::min(3, (r + 3) / 4); ++gs)
-                    for (int qt = 1; qt <= 3; ++qt) cands.push_back({true, 4 * gs, qt * bt / 4, false});
-            if (allow_gr)
-                for (int g = 2; g <= std::min(8, r); ++g) cands.push_back({false, g, 0, true});
+                    for (int qt = 1; qt <= 3; ++qt) cands.push_back({true, 4 * gs, qt * bt / 4});
             double best = 1e30;
             for (const Cand& cand : cands) {
-                if (!plan(cand.g4, cand.gps, cand.t_tma, cand.grouped)) continue;
+                if (!plan(cand.g4, cand.gps, cand.t_tma)) continue;
                 const double ms = i8_time_direction(dir == 0, in_buf, out_buf);
                 char buf[96];
                 if (cand.g4)
                     std::snprintf(buf, sizeof buf, "%shybrid stage=%d tma=%d/%d: %.4f ms", tried.empty() ? "" : ", ",
                                   D.p.gi, cand.t_tma, bt, ms);
-                else if (cand.grouped)
-                    std::snprintf(buf, sizeof buf, "%sgrouped stage=%d: %.4f ms", tried.empty() ? "" : ", ", D.p.gi, ms);
                 else
                     std::snprintf(buf, sizeof buf, "%scp.async stage=%d: %.4f ms", tried.empty() ? "" : ", ", D.p.gi, ms);
                 tried += buf;
                 if (ms < best) {
                     best = ms;
-                    choice = TuneChoice{cand.g4, cand.grouped, D.p.gi, cand.t_tma, ms};
+                    choice = TuneChoice{cand.g4, D.p.gi, cand.t_tma, ms};
                 }
             }
             BW_REQUIRE(best < 1e30, "INT8 form: no stage plan fits in shared memory");
@@ -1828,17 +1572,11 @@ void KoszulCtx::i8_setup() {
             have = true;
         }
         bool ok = false;
-        if (have) ok = plan(choice.gather4, choice.gps, choice.t_tma, choice.grouped);
-        if (!ok) ok = (allow_cp && plan(false, 0, 0, false)) || (allow_g4 && plan(true, 0, bt / 2, false));
-        // grouped tiles without the tuner: two stages a tile at the mean union, fewer generators if that does not fit
-        for (int g = std::min(r, static_cast<int>(D.mean_union + 1) / 2 + 1); !ok && allow_gr && g >= 1; --g)
-            ok = plan(false, g, 0, true);
+        if (have) ok = plan(choice.gather4, choice.gps, choice.t_tma);
+        if (!ok) ok = (allow_cp && plan(false, 0, 0)) || (allow_g4 && plan(true, 0, bt / 2));
         BW_REQUIRE(ok, "INT8 form: maps too large for shared memory");
         char buf[192];
-        if (D.grouped)
-            std::snprintf(buf, sizeof buf, "%s: grouped tiles (union %.2f of %d generators) stage=%d generators, %d slots, "
-                          "%zu B shared", dir == 0 ? "d" : "d^T", D.mean_union, r, D.p.gi, D.p.slots, D.smem);
-        else if (D.gather4)
+        if (D.gather4)
             std::snprintf(buf, sizeof buf, "%s: hybrid (TMA gathers for %d of %d blocks) stage=%d generators, %d slots, "
                           "%zu B shared", dir == 0 ? "d" : "d^T", D.p.t_tma, bt, D.p.gi, D.p.slots, D.smem);
         else
@@ -1847,32 +1585,15 @@ void KoszulCtx::i8_setup() {
         text += (text.empty() ? "" : "; ") + std::string(buf);
         if (!tried.empty()) text += " (tuned: " + tried + ")";
     }
-    // tables the chosen plans do not read are freed: the TMA rows unless the
-    // hybrid producer was chosen (it reads both the rows and the incidence
-    // words); the grouped tables unless grouped tiles were; the rank-order
-    // incidence words when they were
+    // the TMA rows are freed when the cp.async producer alone was chosen (the
+    // hybrid producer reads both tables)
     for (I8State::Dir* D : {&S.fwd, &S.bwd}) {
-        if (!D->gather4 && D->rows4) {
+        if (!D->gather4) {
             release(D->rows4);
             D->rows4 = nullptr;
         }
-        if (D->grouped) {
-            release(D->inc);
-            D->inc = nullptr;
-        } else {
-            for (void* t : {static_cast<void*>(D->ginc), static_cast<void*>(D->tile_blk),
-                            static_cast<void*>(D->tile_gens), static_cast<void*>(D->tile_ngen)})
-                if (t) release(t);
-            D->ginc = nullptr;
-            D->tile_blk = nullptr;
-            D->tile_gens = nullptr;
-            D->tile_ngen = nullptr;
-        }
-        D->p.inc = D->grouped ? D->ginc : D->inc;
+        D->p.inc = D->inc;
         D->p.rows4 = D->rows4;
-        D->p.tile_blk = D->tile_blk;
-        D->p.tile_gens = D->tile_gens;
-        D->p.tile_ngen = D->tile_ngen;
         D->p.hold_first_stage = hold;
     }
     char pbuf[160];

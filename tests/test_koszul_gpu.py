@@ -23,11 +23,10 @@ pytestmark = pytest.mark.gpu
 GOLDEN = np.load(Path(__file__).parent / "golden" / "koszul_golden.npz")
 CASES = sorted({k.split("/")[0] for k in GOLDEN.files})
 FORMS = ["plain", "int8"]
-# The INT8 form's stage producers (the set-up autotuner picks one per shape;
-# BW_I8_PRODUCER restricts the choice): cp.async warps alone over tiles of
-# consecutive blocks, TMA gathers beside them, or cp.async warps over grouped
-# tiles whose K covers only the union of the tile's generators.
-PRODUCER_FORMS = ["plain", "int8:cpasync", "int8:hybrid", "int8:grouped"]
+# The INT8 form's two stage producers (the set-up autotuner picks one per
+# shape; BW_I8_PRODUCER restricts the choice): cp.async warps alone, or TMA
+# gathers beside them.
+PRODUCER_FORMS = ["plain", "int8:cpasync", "int8:hybrid"]
 
 
 @pytest.fixture
@@ -93,7 +92,6 @@ def test_operators_match_oracle(dims, producer_form):
     with _engine(shape, maps, diag, form) as eng:
         if producer:
             assert ("hybrid" in eng.plan) == (producer == "hybrid"), eng.plan
-            assert ("grouped" in eng.plan) == (producer == "grouped"), eng.plan
         y = torch.from_numpy(Y.view(np.int32)).to(dev)
         z = torch.from_numpy(Z.view(np.int32)).to(dev)
         out_z = torch.empty((shape.n_tgt, shape.nb), dtype=torch.int32, device=dev)
@@ -197,31 +195,6 @@ def test_full_size_apply_and_session(cfg, producer_form):
         torch.cuda.synchronize()
         np.testing.assert_array_equal(seq.cpu().numpy().view(np.uint32), np.stack(want))
         assert torch.equal(y_end, cur)
-
-
-@pytest.mark.parametrize("cfg", [
-    ("config2", 19, 9, 20, 28, 32003, 16, 16),
-    ("config5", 23, 11, 32, 40, 32003, 32, 32),
-])
-def test_grouped_tiles_equal_rank_order_tiles_at_full_size(cfg, monkeypatch):
-    """Grouped tiles cover every output block exactly once: one application of
-    S at the full config-2 and config-5 sizes equals, over every row, the one
-    computed with tiles of consecutive blocks (itself checked against the row
-    oracle above)."""
-    name, r, k, ci, co, p, nb, m = cfg
-    shape = oracle.KoszulShape(r, k, ci, co, p, nb, m)
-    dev = torch.device("cuda", 0)
-    maps, diag, x, y = _device_problem(shape, 77, dev)
-    outs = {}
-    for producer in ("cpasync", "grouped"):
-        monkeypatch.setenv("BW_I8_PRODUCER", producer)
-        with _engine(shape, maps, diag, "int8") as eng:
-            assert ("grouped" in eng.plan) == (producer == "grouped"), eng.plan
-            out = torch.empty_like(y)
-            eng.apply(y, out)
-            torch.cuda.synchronize()
-            outs[producer] = out
-    assert torch.equal(outs["cpasync"], outs["grouped"])
 
 
 @pytest.mark.parametrize("form", FORMS)
