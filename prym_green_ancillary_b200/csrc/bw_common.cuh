@@ -87,6 +87,7 @@ struct Mod {
     int32_t p;
     int32_t half;       // (p-1)/2
     int32_t barrett;    // floor(2^32 / p)
+    uint32_t shift;     // half + K p with K p the largest multiple of p below 2^31 (reduce_balanced_fast)
 };
 
 inline Mod make_mod(uint32_t p) {
@@ -94,6 +95,7 @@ inline Mod make_mod(uint32_t p) {
     m.p = static_cast<int32_t>(p);
     m.half = static_cast<int32_t>((p - 1) / 2);
     m.barrett = static_cast<int32_t>((uint64_t{1} << 32) / p);
+    m.shift = static_cast<uint32_t>(m.half) + static_cast<uint32_t>(((uint32_t{1} << 31) - 1) / p * p);
     return m;
 }
 
@@ -118,6 +120,32 @@ __host__ __device__ __forceinline__ int32_t reduce_balanced(int32_t x, const Mod
     if (r >= m.p) r -= m.p;             // [0, p)
     if (r > m.half) r -= m.p;           // balanced
     return r;
+}
+
+__host__ __device__ __forceinline__ uint32_t mulhi_u32(uint32_t a, uint32_t b) {
+#if defined(__CUDA_ARCH__)
+    return __umulhi(a, b);
+#else
+    return static_cast<uint32_t>((static_cast<uint64_t>(a) * b) >> 32);
+#endif
+}
+
+// Exact balanced representative of x for |x| <= 2^31 - 2p, with one Barrett
+// step and one correction.  y = x + half + K p lies in [0, 2^32); q =
+// floor(y * barrett / 2^32) is floor(y / p) or one below, so s = y - q p is in
+// [0, 2p) and s - half is congruent to x; one subtraction of p brings it into
+// [-half, half].
+__host__ __device__ __forceinline__ int32_t reduce_balanced_fast(int32_t x, const Mod& m) {
+    const uint32_t y = static_cast<uint32_t>(x) + m.shift;
+    const uint32_t q = mulhi_u32(y, static_cast<uint32_t>(m.barrett));
+    const int32_t s = static_cast<int32_t>(y - q * static_cast<uint32_t>(m.p));
+    return s - (s >= m.p ? m.p + m.half : m.half);
+}
+
+// Bytewise negation of four signed bytes in [-127, 127] (SWAR: 0x80 - the low
+// seven bits never borrows across a byte; the sign bit is then fixed up).
+__host__ __device__ __forceinline__ uint32_t neg_bytes4(uint32_t w) {
+    return (0x80808080u - (w & 0x7F7F7F7Fu)) ^ (~w & 0x80808080u);
 }
 
 __host__ __device__ __forceinline__ int32_t to_balanced(uint32_t canonical, const Mod& m) {

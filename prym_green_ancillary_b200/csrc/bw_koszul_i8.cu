@@ -131,6 +131,18 @@ __device__ __forceinline__ int32_t combine(int32_t ll, int32_t lhhl, int32_t hh,
     return reduce_balanced(a + c1 * b + c2 * c, mod);
 }
 
+// The gather-GEMM epilogue's value of one output, balanced: ll + 255 (lh + hl)
+// + 255^2 hh, times the diagonal entry dg when scaling (d^T).  The sum before
+// the last reduction stays below 1.11e9 in magnitude: |ll| <= 1024 * 127^2
+// (at most 1024 K rows), 255 * |lh + hl reduced| < 255 * 2p and
+// |c2 * hh reduced| < 16383 * 2p; the scaled product is below 2p * (p - 1) / 2.
+// Both are within reduce_balanced_fast's range.
+__device__ __forceinline__ int32_t epilogue_value(int32_t ll, int32_t lhhl, int32_t hh, const Mod& mod, int32_t c2,
+                                                  bool scale, int32_t dg) {
+    const int32_t t = ll + 255 * reduce_partial(lhhl, mod) + c2 * reduce_partial(hh, mod);
+    return reduce_balanced_fast(scale ? reduce_partial(t, mod) * dg : t, mod);
+}
+
 __host__ __device__ __forceinline__ void split_limbs(int32_t v, int8_t& lo, int8_t& hi) {
     // v in [-16383, 16383]: q = floor((v + 127) / 255), lo = v - 255 q in [-127, 127]
     const int32_t q = static_cast<int32_t>(static_cast<uint32_t>(v + 127 + 255 * 128) / 255u) - 128;
@@ -392,23 +404,37 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
             for (int c = half_id; c < chunks; c += EPQ) {
                 const int o0 = c * 16;
                 if (c != half_id) load_diag(c);
-                int32_t ll[16], lh[16], hl[16], hh[16];
-                tc::tmem_ld16(col0 + o0, ll);
-                tc::tmem_ld16(col0 + P.half + o0, lh);
-                tc::tmem_ld16(col0 + N + o0, hl);
-                tc::tmem_ld16(col0 + N + P.half + o0, hh);
-                tc::tmem_ld_wait();
                 // this lane's 16 outputs (o0..o0+15 of its column j) as limb bytes; columns o >= outer
                 // hold zeros (zero rows of the maps, zero diagonal entries) and are not stored
                 uint32_t lw[4] = {0, 0, 0, 0}, hw[4] = {0, 0, 0, 0};
+                // Eight columns at a time (the four partials of eight outputs live together), and only
+                // the groups of four columns that reach below outer need arithmetic (the rest stay zero).
+                const int live = P.outer - o0;
+                const bool scale = P.diag != nullptr;
 #pragma unroll
-                for (int oo = 0; oo < 16; ++oo) {
-                    int32_t v = combine(ll[oo], lh[oo] + hl[oo], hh[oo], P.mod, P.c1, P.c2);
-                    if (P.diag) v = reduce_balanced(v * dg[oo], P.mod);
-                    int8_t lo, hi;
-                    split_limbs(v, lo, hi);
-                    lw[oo >> 2] |= static_cast<uint32_t>(static_cast<uint8_t>(lo)) << (8 * (oo & 3));
-                    hw[oo >> 2] |= static_cast<uint32_t>(static_cast<uint8_t>(hi)) << (8 * (oo & 3));
+                for (int h8 = 0; h8 < 2; ++h8) {
+                    if (h8 * 8 >= live) break;
+                    int32_t ll[8], lh[8], hl[8], hh[8];
+                    const uint32_t cb = col0 + static_cast<uint32_t>(o0 + h8 * 8);
+                    tc::tmem_ld8(cb, ll);
+                    tc::tmem_ld8(cb + P.half, lh);
+                    tc::tmem_ld8(cb + N, hl);
+                    tc::tmem_ld8(cb + N + P.half, hh);
+                    tc::tmem_ld_wait();
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        if (h8 * 8 + q * 4 >= live) break;
+#pragma unroll
+                        for (int oi = 0; oi < 4; ++oi) {
+                            const int oo = q * 4 + oi;
+                            const int32_t v = epilogue_value(ll[oo], lh[oo] + hl[oo], hh[oo], P.mod, P.c2, scale,
+                                                             dg[h8 * 8 + oo]);
+                            int8_t lo, hi;
+                            split_limbs(v, lo, hi);
+                            lw[h8 * 2 + q] |= static_cast<uint32_t>(static_cast<uint8_t>(lo)) << (8 * oi);
+                            hw[h8 * 2 + q] |= static_cast<uint32_t>(static_cast<uint8_t>(hi)) << (8 * oi);
+                        }
+                    }
                 }
                 // transposed, lane L of the half-warp holds output row o0 + L: 16 bytes, one per j
                 transpose16(lw, lane);
@@ -418,10 +444,10 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                     const uint32_t off = h_off + static_cast<uint32_t>(o) * 16u;
                     *reinterpret_cast<uint4*>(o_lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
                     *reinterpret_cast<uint4*>(o_hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                    *reinterpret_cast<uint4*>(o_nlo + off) = make_uint4(__vsub4(0u, lw[0]), __vsub4(0u, lw[1]),
-                                                                        __vsub4(0u, lw[2]), __vsub4(0u, lw[3]));
-                    *reinterpret_cast<uint4*>(o_nhi + off) = make_uint4(__vsub4(0u, hw[0]), __vsub4(0u, hw[1]),
-                                                                        __vsub4(0u, hw[2]), __vsub4(0u, hw[3]));
+                    *reinterpret_cast<uint4*>(o_nlo + off) =
+                        make_uint4(neg_bytes4(lw[0]), neg_bytes4(lw[1]), neg_bytes4(lw[2]), neg_bytes4(lw[3]));
+                    *reinterpret_cast<uint4*>(o_nhi + off) =
+                        make_uint4(neg_bytes4(hw[0]), neg_bytes4(hw[1]), neg_bytes4(hw[2]), neg_bytes4(hw[3]));
                 }
             }
             tc::tc_fence_before();
@@ -748,21 +774,35 @@ __global__ void __launch_bounds__(kHyThreads, 1)
             for (int c = half_id; c < chunks; c += EPQ) {
                 const int o0 = c * 16;
                 if (c != half_id) load_diag(c);
-                int32_t ll[16], lh[16], hl[16], hh[16];
-                tc::tmem_ld16(col0 + o0, ll);
-                tc::tmem_ld16(col0 + P.half + o0, lh);
-                tc::tmem_ld16(col0 + N + o0, hl);
-                tc::tmem_ld16(col0 + N + P.half + o0, hh);
-                tc::tmem_ld_wait();
                 uint32_t lw[4] = {0, 0, 0, 0}, hw[4] = {0, 0, 0, 0};
+                // Eight columns at a time (the four partials of eight outputs live together), and only
+                // the groups of four columns that reach below outer need arithmetic (the rest stay zero).
+                const int live = P.outer - o0;
+                const bool scale = P.diag != nullptr;
 #pragma unroll
-                for (int oo = 0; oo < 16; ++oo) {
-                    int32_t v = combine(ll[oo], lh[oo] + hl[oo], hh[oo], P.mod, P.c1, P.c2);
-                    if (P.diag) v = reduce_balanced(v * dg[oo], P.mod);
-                    int8_t lo, hi;
-                    split_limbs(v, lo, hi);
-                    lw[oo >> 2] |= static_cast<uint32_t>(static_cast<uint8_t>(lo)) << (8 * (oo & 3));
-                    hw[oo >> 2] |= static_cast<uint32_t>(static_cast<uint8_t>(hi)) << (8 * (oo & 3));
+                for (int h8 = 0; h8 < 2; ++h8) {
+                    if (h8 * 8 >= live) break;
+                    int32_t ll[8], lh[8], hl[8], hh[8];
+                    const uint32_t cb = col0 + static_cast<uint32_t>(o0 + h8 * 8);
+                    tc::tmem_ld8(cb, ll);
+                    tc::tmem_ld8(cb + P.half, lh);
+                    tc::tmem_ld8(cb + N, hl);
+                    tc::tmem_ld8(cb + N + P.half, hh);
+                    tc::tmem_ld_wait();
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        if (h8 * 8 + q * 4 >= live) break;
+#pragma unroll
+                        for (int oi = 0; oi < 4; ++oi) {
+                            const int oo = q * 4 + oi;
+                            const int32_t v = epilogue_value(ll[oo], lh[oo] + hl[oo], hh[oo], P.mod, P.c2, scale,
+                                                             dg[h8 * 8 + oo]);
+                            int8_t lo, hi;
+                            split_limbs(v, lo, hi);
+                            lw[h8 * 2 + q] |= static_cast<uint32_t>(static_cast<uint8_t>(lo)) << (8 * oi);
+                            hw[h8 * 2 + q] |= static_cast<uint32_t>(static_cast<uint8_t>(hi)) << (8 * oi);
+                        }
+                    }
                 }
                 transpose16(lw, lane);
                 transpose16(hw, lane);
@@ -771,10 +811,10 @@ __global__ void __launch_bounds__(kHyThreads, 1)
                     const uint32_t off = h_off + static_cast<uint32_t>(o) * 16u;
                     *reinterpret_cast<uint4*>(o_lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
                     *reinterpret_cast<uint4*>(o_hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                    *reinterpret_cast<uint4*>(o_nlo + off) = make_uint4(__vsub4(0u, lw[0]), __vsub4(0u, lw[1]),
-                                                                        __vsub4(0u, lw[2]), __vsub4(0u, lw[3]));
-                    *reinterpret_cast<uint4*>(o_nhi + off) = make_uint4(__vsub4(0u, hw[0]), __vsub4(0u, hw[1]),
-                                                                        __vsub4(0u, hw[2]), __vsub4(0u, hw[3]));
+                    *reinterpret_cast<uint4*>(o_nlo + off) =
+                        make_uint4(neg_bytes4(lw[0]), neg_bytes4(lw[1]), neg_bytes4(lw[2]), neg_bytes4(lw[3]));
+                    *reinterpret_cast<uint4*>(o_nhi + off) =
+                        make_uint4(neg_bytes4(hw[0]), neg_bytes4(hw[1]), neg_bytes4(hw[2]), neg_bytes4(hw[3]));
                 }
             }
             tc::tc_fence_before();
