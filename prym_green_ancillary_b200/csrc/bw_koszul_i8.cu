@@ -232,14 +232,14 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t block_bytes = static_cast<uint32_t>(P.inner) * 16;
 
     if (warp < kProducerWarps) {
         // ------------------------------------------------------------ producers
         // Warp w stages the output blocks t = w % GROUPS, + GROUPS, ... of each tile.  Lane
-        // i holds the incidence entry of generator i for those blocks (read by
-        // shuffle; the next tile's entries are loaded one tile ahead), and the
-        // warp's lanes walk the K' rows of every (limb, block, column group):
+        // i holds, for those blocks, where generator i's neighbour run starts: its offset
+        // from the limb's +plane in 16-byte units, the -plane's offset added for a negative
+        // sign, or kAbsent (read by shuffle; the next tile's entries are loaded one tile
+        // ahead).  The warp's lanes walk the K' rows of every (limb, block, column group):
         // a 16-byte cp.async from the +plane or -plane of the neighbour block,
         // or a zero-filling one (source size 0) for an absent generator.  Each
         // thread arrives on the stage barrier once, through
@@ -249,15 +249,19 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         constexpr int GROUPS = kProducerWarps / RPW;                     // distinct block positions
         constexpr int TPW = (BT + GROUPS - 1) / GROUPS;                  // blocks per producer warp
         const int group = warp % GROUPS, sub = warp / GROUPS;
+        const uint32_t neg16 = static_cast<uint32_t>(P.in_neg_off >> 4);
+        const uint32_t run16 = static_cast<uint32_t>(HG * P.inner);   // 16-byte rows of one neighbour block
         auto load_inc = [&](long long tile, uint32_t (&dst)[TPW]) {
 #pragma unroll
             for (int k = 0; k < TPW; ++k) {
                 const int t = group + k * GROUPS;
                 const long long blk = tile * BT + t;
-                dst[k] = (tile < n_tiles && t < BT && blk < P.n_blk && lane < P.r) ? __ldg(P.inc + blk * P.r + lane)
-                                                                                  : kAbsent;
+                const uint32_t e = (tile < n_tiles && t < BT && blk < P.n_blk && lane < P.r)
+                                       ? __ldg(P.inc + blk * P.r + lane) : kAbsent;
+                dst[k] = e == kAbsent ? kAbsent : ((e >> 31) ? neg16 : 0u) + (e & 0x7FFFFFFFu) * run16;
             }
         };
+        const uint32_t sA_u32 = tc::smem_u32(sA);
         SlotRing ring(P.slots);
         bool ok = true;
         uint32_t incr[TPW], incn[TPW];
@@ -280,7 +284,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                 // failure tests: the first stage of CTA 0 is never filled, so its consumer's wait runs out
                 const int g_s = min(P.gi, P.r - s * P.gi);
                 const int rows = g_s * P.inner;             // K' rows filled in this stage
-                uint8_t* slotA = sA + static_cast<size_t>(slot) * P.slot_bytes;
+                const uint32_t slotA = sA_u32 + static_cast<uint32_t>(slot) * P.slot_bytes;
 #pragma unroll
                 for (int k = 0; k < TPW; ++k) {
                     const int t = group + k * GROUPS;
@@ -288,24 +292,22 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                     for (int w0 = sub * 32; w0 < rows; w0 += RPW * 32) {
                         const int w = w0 + lane;
                         const int il = il_of_row[min(w, rows - 1)];
-                        const uint32_t e = __shfl_sync(0xffffffffu, incr[k], s * P.gi + il);
+                        const uint32_t o16 = __shfl_sync(0xffffffffu, incr[k], s * P.gi + il);
                         if (w >= rows) continue;
                         const int b = w - il * P.inner;
-                        uint8_t* dst0 = slotA + static_cast<size_t>(t * HG) * KS * 16 + static_cast<size_t>(w) * 16;
+                        const uint32_t dst0 = slotA + static_cast<uint32_t>(t * HG * KS + w) * 16u;
                         // one code path for every lane: an absent generator's rows are zero-filled by
                         // the copy itself (source size 0: nothing is read), so the warp does not diverge
-                        const bool present = e != kAbsent;
-                        const long long nbr = present ? static_cast<long long>(e & 0x7FFFFFFFu) : 0;
-                        // the -plane of a limb lies in_neg_off bytes after its +plane
-                        const long long negoff = (present && (e >> 31)) ? P.in_neg_off : 0;
+                        const bool present = o16 != kAbsent;
+                        const uint32_t src16 = (present ? o16 : 0u) + static_cast<uint32_t>(b);
                         const uint32_t nbytes = present ? 16u : 0u;
 #pragma unroll
                         for (int limb = 0; limb < 2; ++limb)
 #pragma unroll
                             for (int h = 0; h < HG; ++h)
-                                tc::cp_async16_zfill(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
-                                                         static_cast<size_t>(h) * KS * 16,
-                                                     P.in[limb] + negoff + (nbr * HG + h) * block_bytes + b * 16,
+                                tc::cp_async16_zfill(dst0 + static_cast<uint32_t>(limb) * P.limb_bytes +
+                                                         static_cast<uint32_t>(h * KS * 16),
+                                                     P.in[limb] + static_cast<size_t>(src16 + h * P.inner) * 16u,
                                                      nbytes);
                     }
                 }
@@ -556,7 +558,6 @@ __global__ void __launch_bounds__(kHyThreads, 1)
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t block_bytes = static_cast<uint32_t>(P.inner) * 16;
 
     if (warp < kCpWarps) {
         // ------------------------------------------------------------ cp.async producers
@@ -569,11 +570,17 @@ __global__ void __launch_bounds__(kHyThreads, 1)
         const int wpb = n_cp > 0 ? kCpWarps / n_cp : 1;
         const bool active = n_cp > 0 && warp < n_cp * wpb;
         const int t = active ? P.t_tma + warp / wpb : 0, sub = active ? warp % wpb : 0;
+        // lane i: where generator i's neighbour run starts (16-byte units from the limb's +plane,
+        // the -plane's offset added for a negative sign), or kAbsent
+        const uint32_t neg16 = static_cast<uint32_t>(P.in_neg_off >> 4);
+        const uint32_t run16 = static_cast<uint32_t>(HG * P.inner);
         auto load_inc = [&](long long tile) -> uint32_t {
             const long long blk = tile * BT + t;
-            return (active && tile < n_tiles && blk < P.n_blk && lane < P.r) ? __ldg(P.inc + blk * P.r + lane)
-                                                                              : kAbsent;
+            const uint32_t e = (active && tile < n_tiles && blk < P.n_blk && lane < P.r)
+                                   ? __ldg(P.inc + blk * P.r + lane) : kAbsent;
+            return e == kAbsent ? kAbsent : ((e >> 31) ? neg16 : 0u) + (e & 0x7FFFFFFFu) * run16;
         };
+        const uint32_t sA_u32 = tc::smem_u32(sA);
         SlotRing ring(P.slots);
         bool ok = true;
         uint32_t incn = load_inc(blockIdx.x);
@@ -594,28 +601,28 @@ __global__ void __launch_bounds__(kHyThreads, 1)
                 if (active) {
                     const bool last = s == P.stages_per_tile - 1;
                     const int rows = (last ? P.groups - s * P.gs : P.gs) * 4 * P.inner_pad;
-                    uint8_t* col0 = sA + static_cast<size_t>(slot) * P.slot_bytes + static_cast<size_t>(t * HG) * KS * 16;
+                    const uint32_t col0 = sA_u32 + static_cast<uint32_t>(slot) * P.slot_bytes +
+                                          static_cast<uint32_t>(t * HG * KS) * 16u;
                     for (int w0 = sub * 32; w0 < rows; w0 += wpb * 32) {
                         const int w = w0 + lane;
                         const int il = il_of_row[min(w, rows - 1)];
                         const int gen = s * P.gi + (il == 255 ? 0 : il);
-                        const uint32_t e = __shfl_sync(0xffffffffu, incr, min(gen, 31));
+                        const uint32_t o16 = __shfl_sync(0xffffffffu, incr, min(gen, 31));
                         // padding rows and generators past r: their B rows are zero, nothing to copy
                         if (w >= rows || il == 255 || gen >= P.r) continue;
                         const int u = w - il * P.inner_pad;
-                        const bool present = e != kAbsent;
-                        const long long nbr = present ? static_cast<long long>(e & 0x7FFFFFFFu) : 0;
-                        // the -plane of a limb lies in_neg_off bytes after its +plane
-                        const long long negoff = (present && (e >> 31)) ? P.in_neg_off : 0;
+                        const bool present = o16 != kAbsent;
+                        const uint32_t src16 = (present ? o16 : 0u) + static_cast<uint32_t>(u);
                         const uint32_t nbytes = present ? 16u : 0u;
-                        uint8_t* dst0 = col0 + static_cast<size_t>(w) * 16;
+                        const uint32_t dst0 = col0 + static_cast<uint32_t>(w) * 16u;
 #pragma unroll
                         for (int limb = 0; limb < 2; ++limb)
 #pragma unroll
                             for (int h = 0; h < HG; ++h)
-                                tc::cp_async16_zfill(dst0 + static_cast<size_t>(limb) * P.limb_bytes +
-                                                         static_cast<size_t>(h) * KS * 16,
-                                                     P.in[limb] + negoff + (nbr * HG + h) * block_bytes + u * 16, nbytes);
+                                tc::cp_async16_zfill(dst0 + static_cast<uint32_t>(limb) * P.limb_bytes +
+                                                         static_cast<uint32_t>(h * KS * 16),
+                                                     P.in[limb] + static_cast<size_t>(src16 + h * P.inner) * 16u,
+                                                     nbytes);
                     }
                 }
                 tc::cp_async_arrive_noinc(&full[slot]);   // when this thread's copies have landed
@@ -1474,6 +1481,8 @@ void KoszulCtx::i8_setup() {
     // each limb's -plane directly after its +plane (one tensor map covers both signs)
     for (int b = 0; b < 3; ++b) {
         const uint64_t plane = (b < 2 ? n_src : n_tgt) * nbi;
+        // the gather producers address a +plane and its -plane in 16-byte units below 2^32 - 1
+        BW_REQUIRE(2 * plane / 16 < 0xFFFFFFFFull, "INT8 form: limb planes above the 16-byte offset range");
         for (int limb = 0; limb < 2; ++limb) {
             int8_t* pair = alloc<int8_t>(2 * plane);
             S.planes[b][limb] = pair;

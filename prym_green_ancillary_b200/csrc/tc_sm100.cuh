@@ -117,6 +117,11 @@ __device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, uin
                  : "memory");
 }
 
+// The same with the destination given as a shared-memory address.
+__device__ __forceinline__ void cp_async16_zfill(uint32_t dst_smem, const void* src, uint32_t src_size) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst_smem), "l"(src), "r"(src_size) : "memory");
+}
+
 // Arrive on `bar` once every cp.async issued so far by this thread has landed
 // (the arrival is one of the barrier's expected arrivals).
 __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
