@@ -107,6 +107,12 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def peak_source(kind):
+    """Where the roofline's HBM denominator came from."""
+    return ("measured copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured"
+            else "fallback 6650 GB/s (no MEASURED_PEAKS.json)")
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
 
@@ -501,7 +507,7 @@ def run_batch(args):
             "roofline": {"bound": "hbm", "kernel": "batch step (all sectors' kernels, one graph per 16 steps)",
                          "achieved": step_bytes / (step_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak, "traffic": None,
-                         "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+                         "peak_source": peak_source(peak_kind)},
             "cpu_baseline": cpu,
             "e2e": {"value": world * K * n_sec / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
@@ -586,7 +592,7 @@ def run_paper(args):
             "roofline": {"bound": "hbm", "kernel": "apply of S + moments (one CUDA graph per round)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": paper_traffic(args.workload),
-                         "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+                         "peak_source": peak_source(peak_kind)},
             "cpu_baseline": cpu,
             "e2e": {"value": world * K / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": cols * 4 * 4 / K,
                     "d2h_bytes_per_step": (seq.nbytes + cur.nbytes) / K,
@@ -808,8 +814,7 @@ def run_engine(args):
             "kernel_ms": dict(zip(names, kern_ms)),
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"
-                         if peak_kind == "measured" else "fallback 6650 GB/s"},
+                         "peak_source": peak_source(peak_kind)},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "calls": len(e2e_calls),
