@@ -320,6 +320,9 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_i8(128, N, true, false);
             const uint32_t sA0 = tc::smem_u32(sA), sB0 = tc::smem_u32(sB);
+            const uint32_t a_hi = tc::desc_hi(static_cast<uint32_t>(KS) * 16u), b_hi = tc::desc_hi(256u);
+            const uint32_t b_kstep = static_cast<uint32_t>(N) * 32u;   // bytes of B per K-step
+            const uint32_t a_limb = P.limb_bytes >> 4;                 // hi limb of A, in descriptor units
             long long tcount = 0;
             SlotRing ring(P.slots);
             bool ok = true;
@@ -345,16 +348,18 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
                     tc::fence_proxy_async_smem();
                     tc::tc_fence_after();
                     const int ks_n = (s == P.stages_per_tile - 1) ? P.ks_last : P.ks_full;
-                    for (int limb = 0; limb < 2; ++limb) {
-                        const uint32_t a_base = sA0 + static_cast<uint32_t>(slot) * P.slot_bytes +
-                                                static_cast<uint32_t>(limb) * P.limb_bytes;
-                        for (int ks = 0; ks < ks_n; ++ks) {
-                            const uint64_t ad = tc::smem_desc(a_base + ks * 512u, 128u, static_cast<uint32_t>(KS) * 16u);
-                            const uint32_t gks = static_cast<uint32_t>(s * P.ks_full + ks);
-                            const uint64_t bd = tc::smem_desc(sB0 + gks * static_cast<uint32_t>(N) * 32u, 128u, 256u);
-                            tc::mma_i8(dbase + static_cast<uint32_t>(limb * N), ad, bd, idesc,
-                                       (s > 0 || ks > 0) ? 1u : 0u);
-                        }
+                    // descriptors advance by adding to their low words: A by one K-step (32 rows of
+                    // 16 bytes), B by one K-step of the maps (N x 32 bytes); the two limbs of the
+                    // input go to the tile's two accumulators
+                    const uint32_t a_lo = tc::desc_lo(sA0 + static_cast<uint32_t>(slot) * P.slot_bytes, 128u);
+                    const uint32_t b_lo = tc::desc_lo(sB0 + static_cast<uint32_t>(s * P.ks_full) * b_kstep, 128u);
+#pragma unroll 2
+                    for (int ks = 0; ks < ks_n; ++ks) {
+                        const uint64_t bd = tc::desc_make(b_lo + static_cast<uint32_t>(ks) * (b_kstep >> 4), b_hi);
+                        const uint32_t acc = (s > 0 || ks > 0) ? 1u : 0u;
+                        const uint32_t a_k = a_lo + static_cast<uint32_t>(ks) * (512u >> 4);
+                        tc::mma_i8(dbase, tc::desc_make(a_k, a_hi), bd, idesc, acc);
+                        tc::mma_i8(dbase + static_cast<uint32_t>(N), tc::desc_make(a_k + a_limb, a_hi), bd, idesc, acc);
                     }
                     tc::mma_commit(&empty[slot]);
                 }
@@ -696,6 +701,9 @@ __global__ void __launch_bounds__(kHyThreads, 1)
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_i8(128, N, true, false);
             const uint32_t sA0 = tc::smem_u32(sA), sB0 = tc::smem_u32(sB);
+            const uint32_t a_hi = tc::desc_hi(static_cast<uint32_t>(KS) * 16u), b_hi = tc::desc_hi(256u);
+            const uint32_t b_kstep = static_cast<uint32_t>(N) * 32u;   // bytes of B per K-step
+            const uint32_t a_limb = P.limb_bytes >> 4;                 // hi limb of A, in descriptor units
             long long tcount = 0;
             SlotRing ring(P.slots);
             bool ok = true;
@@ -722,16 +730,18 @@ __global__ void __launch_bounds__(kHyThreads, 1)
                     tc::fence_proxy_async_smem();
                     tc::tc_fence_after();
                     const int ks_n = (s == P.stages_per_tile - 1) ? P.ks_last : P.ks_full;
-                    for (int limb = 0; limb < 2; ++limb) {
-                        const uint32_t a_base = sA0 + static_cast<uint32_t>(slot) * P.slot_bytes +
-                                                static_cast<uint32_t>(limb) * P.limb_bytes;
-                        for (int ks = 0; ks < ks_n; ++ks) {
-                            const uint64_t ad = tc::smem_desc(a_base + ks * 512u, 128u, static_cast<uint32_t>(KS) * 16u);
-                            const uint32_t gks = static_cast<uint32_t>(s * P.ks_full + ks);
-                            const uint64_t bd = tc::smem_desc(sB0 + gks * static_cast<uint32_t>(N) * 32u, 128u, 256u);
-                            tc::mma_i8(dbase + static_cast<uint32_t>(limb * N), ad, bd, idesc,
-                                       (s > 0 || ks > 0) ? 1u : 0u);
-                        }
+                    // descriptors advance by adding to their low words: A by one K-step (32 rows of
+                    // 16 bytes), B by one K-step of the maps (N x 32 bytes); the two limbs of the
+                    // input go to the tile's two accumulators
+                    const uint32_t a_lo = tc::desc_lo(sA0 + static_cast<uint32_t>(slot) * P.slot_bytes, 128u);
+                    const uint32_t b_lo = tc::desc_lo(sB0 + static_cast<uint32_t>(s * P.ks_full) * b_kstep, 128u);
+#pragma unroll 2
+                    for (int ks = 0; ks < ks_n; ++ks) {
+                        const uint64_t bd = tc::desc_make(b_lo + static_cast<uint32_t>(ks) * (b_kstep >> 4), b_hi);
+                        const uint32_t acc = (s > 0 || ks > 0) ? 1u : 0u;
+                        const uint32_t a_k = a_lo + static_cast<uint32_t>(ks) * (512u >> 4);
+                        tc::mma_i8(dbase, tc::desc_make(a_k, a_hi), bd, idesc, acc);
+                        tc::mma_i8(dbase + static_cast<uint32_t>(N), tc::desc_make(a_k + a_limb, a_hi), bd, idesc, acc);
                     }
                     tc::mma_commit(&empty[slot]);
                 }
