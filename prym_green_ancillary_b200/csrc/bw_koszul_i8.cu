@@ -1457,7 +1457,8 @@ void KoszulCtx::i8_destroy() {
 
 void KoszulCtx::i8_setup() {
     BW_REQUIRE(nbi == 16 || nbi == 32, "INT8 form: internal block width must be 16 or 32");
-    BW_REQUIRE(ci <= 128 && co <= 128, "INT8 form: dim_in and dim_out must be at most 128");
+    // two double-buffered accumulators of 2 N <= 256 columns each fill the 512 TMEM columns
+    BW_REQUIRE(ci <= 64 && co <= 64, "INT8 form: dim_in and dim_out must be at most 64");
     BW_REQUIRE(static_cast<long long>(r) * std::max(ci, co) <= 1024, "INT8 form: r * dim above 1024 (int32 bound)");
     BW_REQUIRE(r <= 32, "INT8 form: at most 32 generators (one per lane)");
     int major = 0;

@@ -234,3 +234,15 @@ def test_contexts_of_different_shapes_coexist(form):
     finally:
         for *_, eng in engines:
             eng.close()
+
+
+def test_int8_form_refuses_dims_beyond_its_accumulators():
+    """The INT8 form keeps two double-buffered accumulators of 2 N TMEM columns
+    (N = 2 x dim rounded up to 16): dims above 64 would need more than the 512
+    columns an SM has, so such contexts are refused with status 3."""
+    from prym_green_ancillary_b200 import EngineError
+    shape = oracle.KoszulShape(3, 2, 65, 4, 32003, 16, 16)
+    maps, diag, X, Y = oracle.seeded_problem(shape, 5)
+    with pytest.raises(EngineError) as err:
+        _engine(shape, maps, diag, "int8")
+    assert err.value.status == 3 and "at most 64" in str(err.value)
