@@ -18,6 +18,12 @@
 #include "bw_koszul.cuh"
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
 #include <cstring>
 #include <vector>
 
@@ -27,23 +33,27 @@ namespace bw {
 
 namespace {
 
-__device__ __forceinline__ void mac4x4(int32_t (&acc)[4][4], const int4& a, const int4& y) {
-    acc[0][0] += a.x * y.x; acc[0][1] += a.x * y.y; acc[0][2] += a.x * y.z; acc[0][3] += a.x * y.w;
-    acc[1][0] += a.y * y.x; acc[1][1] += a.y * y.y; acc[1][2] += a.y * y.z; acc[1][3] += a.y * y.w;
-    acc[2][0] += a.z * y.x; acc[2][1] += a.z * y.y; acc[2][2] += a.z * y.z; acc[2][3] += a.z * y.w;
-    acc[3][0] += a.w * y.x; acc[3][1] += a.w * y.y; acc[3][2] += a.w * y.z; acc[3][3] += a.w * y.w;
+// acc[o0 + a][j] += coef[a] * y[j] for the four coefficients of one int4
+template <int TO>
+__device__ __forceinline__ void mac4(int32_t (&acc)[TO][4], int o0, const int4& a, const int4& y) {
+    acc[o0][0] += a.x * y.x; acc[o0][1] += a.x * y.y; acc[o0][2] += a.x * y.z; acc[o0][3] += a.x * y.w;
+    acc[o0 + 1][0] += a.y * y.x; acc[o0 + 1][1] += a.y * y.y; acc[o0 + 1][2] += a.y * y.z; acc[o0 + 1][3] += a.y * y.w;
+    acc[o0 + 2][0] += a.z * y.x; acc[o0 + 2][1] += a.z * y.y; acc[o0 + 2][2] += a.z * y.z; acc[o0 + 2][3] += a.z * y.w;
+    acc[o0 + 3][0] += a.w * y.x; acc[o0 + 3][1] += a.w * y.y; acc[o0 + 3][2] += a.w * y.z; acc[o0 + 3][3] += a.w * y.w;
 }
 
-__device__ __forceinline__ void reduce4x4(int32_t (&acc)[4][4], const Mod& mod) {
+template <int TO>
+__device__ __forceinline__ void reduce_tile(int32_t (&acc)[TO][4], const Mod& mod) {
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < TO; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b] = reduce_partial(acc[a][b], mod);
 }
 
-__device__ __forceinline__ void negate4x4(int32_t (&acc)[4][4]) {
+template <int TO>
+__device__ __forceinline__ void negate_tile(int32_t (&acc)[TO][4]) {
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < TO; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b] = -acc[a][b];
 }
@@ -55,25 +65,29 @@ __device__ __forceinline__ void negate4x4(int32_t (&acc)[4][4]) {
 // d   : blk = T, o = c (dim_out), u = b (dim_in),  coef = M^T  (i x b x c)
 // d^T : blk = S, o = b (dim_in),  u = c (dim_out), coef = M    (i x c x b)
 //
-// A thread owns a 4 (o) x 4 (j) register tile of one output block; the
-// coefficient tiles of all r maps sit in shared memory ([i][u][o4], o padded
-// to a multiple of 4 with zeros), the gathered input rows stream from L2 as
-// 16-byte loads.  Sums of 8 balanced products stay inside int32 next to a
-// partially reduced value, so the accumulator is reduced every 8 u-steps.
-template <int NB>
+// A thread owns a TO (o) x 4 (j) register tile of one output block (TO = 4 or
+// 8: an 8-row tile does twice the multiply-adds per gathered 16-byte row); the
+// coefficient tiles of all r maps sit in shared memory ([i][u][o], rows of
+// `ostride` = outer rounded up to 8, zero-padded), the gathered input rows
+// stream from L2 as 16-byte loads.  Sums of 8 balanced products stay inside
+// int32 next to a partially reduced value, so the accumulator is reduced every
+// 8 u-steps.
+template <int NB, int TO>
 __global__ void __launch_bounds__(256) gather_mac_kernel(
     const int32_t* __restrict__ in, int32_t* __restrict__ out,
     const uint32_t* __restrict__ inc, const int32_t* __restrict__ coef,
     const int32_t* __restrict__ diag,   // nullptr: no scaling
-    long long n_blk, int width, int r, int inner, int outer, int outer4, Mod mod) {
+    long long n_blk, int width, int r, int inner, int outer, int ostride, Mod mod) {
     extern __shared__ int4 smem_raw[];
     int32_t* sm = reinterpret_cast<int32_t*>(smem_raw);
-    const int total = r * inner * outer4;
+    const int total = r * inner * ostride;
     for (int e = threadIdx.x; e < total; e += blockDim.x) sm[e] = coef[e];
     __syncthreads();
 
     constexpr int JG = NB / 4;
-    const int OG = outer4 / 4;
+    constexpr int TQ = TO / 4;                     // int4 coefficient loads per u-step
+    const int OG = (outer + TO - 1) / TO;
+    const int OS4 = ostride / 4;
     const int tpb = OG * JG;                       // threads per output block
     const int bpc = blockDim.x / tpb;              // output blocks per CTA pass
     const int local = threadIdx.x / tpb;
@@ -85,9 +99,9 @@ __global__ void __launch_bounds__(256) gather_mac_kernel(
     const int4* sm4 = reinterpret_cast<const int4*>(sm);
     for (long long blk = static_cast<long long>(blockIdx.x) * bpc + local; blk < n_blk;
          blk += static_cast<long long>(gridDim.x) * bpc) {
-        int32_t acc[4][4];
+        int32_t acc[TO][4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < TO; ++a)
 #pragma unroll
             for (int b = 0; b < 4; ++b) acc[a][b] = 0;
         bool neg_state = false;
@@ -103,11 +117,11 @@ __global__ void __launch_bounds__(256) gather_mac_kernel(
             const int i = static_cast<int>((e >> 26) & 31u);
             const long long s = static_cast<long long>(e & 0x3FFFFFFu);
             if (neg != neg_state) {
-                negate4x4(acc);
+                negate_tile<TO>(acc);
                 neg_state = neg;
             }
             const int4* irow = reinterpret_cast<const int4*>(in + s * inner * NB) + jg;
-            const int4* crow = sm4 + static_cast<size_t>(i) * inner * OG + og;
+            const int4* crow = sm4 + static_cast<size_t>(i) * inner * OS4 + og * TQ;
             for (int u0 = 0; u0 < inner; u0 += 8) {
                 int4 y[8];
 #pragma unroll
@@ -116,16 +130,16 @@ __global__ void __launch_bounds__(256) gather_mac_kernel(
 #pragma unroll
                 for (int uu = 0; uu < 8; ++uu) {
                     if (u0 + uu >= inner) break;
-                    const int4 a = crow[(u0 + uu) * OG];
-                    mac4x4(acc, a, y[uu]);
+#pragma unroll
+                    for (int t = 0; t < TQ; ++t) mac4<TO>(acc, 4 * t, crow[(u0 + uu) * OS4 + t], y[uu]);
                 }
-                reduce4x4(acc, mod);
+                reduce_tile<TO>(acc, mod);
             }
         }
-        if (neg_state) negate4x4(acc);
-        const int o0 = og * 4;
+        if (neg_state) negate_tile<TO>(acc);
+        const int o0 = og * TO;
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
+        for (int a = 0; a < TO; ++a) {
             const int o = o0 + a;
             if (o >= outer) break;
             const long long row = blk * outer + o;
@@ -270,13 +284,13 @@ void KoszulCtx::launch_to_canonical(const int32_t* in, uint32_t* out, uint64_t c
 
 namespace {
 
-template <int NB>
+template <int NB, int TO>
 void launch_gather(KoszulCtx& c, const int32_t* in, int32_t* out, const uint32_t* inc, const int32_t* coef,
-                   const int32_t* diag, uint64_t n_blk, int width, int inner, int outer, int outer4,
+                   const int32_t* diag, uint64_t n_blk, int width, int inner, int outer, int ostride,
                    cudaStream_t st) {
-    const size_t smem = static_cast<size_t>(c.r) * inner * outer4 * sizeof(int32_t);
-    auto kern = gather_mac_kernel<NB>;
-    const int tpb = (outer4 / 4) * (NB / 4);
+    const size_t smem = static_cast<size_t>(c.r) * inner * ostride * sizeof(int32_t);
+    auto kern = gather_mac_kernel<NB, TO>;
+    const int tpb = (outer + TO - 1) / TO * (NB / 4);
     BW_REQUIRE(tpb <= 256, "dimension too large for the plain gather kernel (dim/4 * n/4 > 256)");
     const int bpc = 256 / tpb;
     BW_REQUIRE(static_cast<int>(smem) <= allow_dynamic_smem(kern, c.device),
@@ -287,7 +301,7 @@ void launch_gather(KoszulCtx& c, const int32_t* in, int32_t* out, const uint32_t
     const uint64_t groups = (n_blk + bpc - 1) / bpc;
     const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(groups, static_cast<uint64_t>(c.sms) * occ));
     kern<<<grid, 256, smem, st>>>(in, out, inc, coef, diag, static_cast<long long>(n_blk), width, c.r,
-                                  inner, outer, outer4, c.mod);
+                                  inner, outer, ostride, c.mod);
     BW_CHECK_LAUNCH();
     ++c.launches;
 }
@@ -315,14 +329,22 @@ void dispatch_nb(int nb, F&& f) {
 
 void KoszulCtx::plain_forward(const int32_t* y, int32_t* z, cudaStream_t st) {
     dispatch_nb(nb, [&](auto NBc) {
-        launch_gather<decltype(NBc)::value>(*this, y, z, d_fwd, d_coef_fwd, nullptr, n_t, r - k + 1, ci, co, co4, st);
+        constexpr int NB = decltype(NBc)::value;
+        if (tile_fwd == 8)
+            launch_gather<NB, 8>(*this, y, z, d_fwd, d_coef_fwd, nullptr, n_t, r - k + 1, ci, co, co8, st);
+        else
+            launch_gather<NB, 4>(*this, y, z, d_fwd, d_coef_fwd, nullptr, n_t, r - k + 1, ci, co, co8, st);
     });
 }
 
 void KoszulCtx::plain_transpose(const int32_t* z, int32_t* w, bool scale, cudaStream_t st) {
     dispatch_nb(nb, [&](auto NBc) {
-        launch_gather<decltype(NBc)::value>(*this, z, w, d_bwd, d_coef_bwd, scale ? d_diag : nullptr, n_s, k, co,
-                                            ci, ci4, st);
+        constexpr int NB = decltype(NBc)::value;
+        const int32_t* dg = scale ? d_diag : nullptr;
+        if (tile_bwd == 8)
+            launch_gather<NB, 8>(*this, z, w, d_bwd, d_coef_bwd, dg, n_s, k, co, ci, ci8, st);
+        else
+            launch_gather<NB, 4>(*this, z, w, d_bwd, d_coef_bwd, dg, n_s, k, co, ci, ci8, st);
     });
 }
 
@@ -440,8 +462,8 @@ KoszulCtx* KoszulCtx::create(const bw_koszul_desc& d, int dev) {
     c->k = static_cast<int>(d.k);
     c->ci = static_cast<int>(d.dim_in);
     c->co = static_cast<int>(d.dim_out);
-    c->ci4 = (c->ci + 3) / 4 * 4;
-    c->co4 = (c->co + 3) / 4 * 4;
+    c->ci8 = (c->ci + 7) / 8 * 8;
+    c->co8 = (c->co + 7) / 8 * 8;
     c->nb = static_cast<int>(d.block_width);
     c->nbi = d.form == BW_FORM_INT8 ? (c->nb <= 16 ? 16 : 32) : c->nb;
     c->m = static_cast<int>(d.proj_width);
@@ -455,22 +477,22 @@ KoszulCtx* KoszulCtx::create(const bw_koszul_desc& d, int dev) {
     BW_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
     BW_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
 
-    const size_t smem_fwd = static_cast<size_t>(c->r) * c->ci * c->co4 * sizeof(int32_t);
-    const size_t smem_bwd = static_cast<size_t>(c->r) * c->co * c->ci4 * sizeof(int32_t);
+    const size_t smem_fwd = static_cast<size_t>(c->r) * c->ci * c->co8 * sizeof(int32_t);
+    const size_t smem_bwd = static_cast<size_t>(c->r) * c->co * c->ci8 * sizeof(int32_t);
     BW_REQUIRE(smem_fwd <= 200 * 1024 && smem_bwd <= 200 * 1024,
                "maps too large for shared memory staging (r * dim_in * dim_out * 4 > 200 KiB)");
 
-    // Coefficient tiles (balanced): forward uses M^T [i][b][c4], transpose M [i][c][b4].
-    std::vector<int32_t> coef_fwd(static_cast<size_t>(c->r) * c->ci * c->co4, 0);
-    std::vector<int32_t> coef_bwd(static_cast<size_t>(c->r) * c->co * c->ci4, 0);
+    // Coefficient tiles (balanced): forward uses M^T [i][b][c8], transpose M [i][c][b8] (rows zero-padded to 8).
+    std::vector<int32_t> coef_fwd(static_cast<size_t>(c->r) * c->ci * c->co8, 0);
+    std::vector<int32_t> coef_bwd(static_cast<size_t>(c->r) * c->co * c->ci8, 0);
     c->maps_canonical.assign(d.maps, d.maps + static_cast<size_t>(c->r) * c->co * c->ci);
     for (int i = 0; i < c->r; ++i)
         for (int cc = 0; cc < c->co; ++cc)
             for (int b = 0; b < c->ci; ++b) {
                 const uint32_t v = d.maps[(static_cast<size_t>(i) * c->co + cc) * c->ci + b] % c->p;
                 const int32_t bal = to_balanced(v, c->mod);
-                coef_fwd[(static_cast<size_t>(i) * c->ci + b) * c->co4 + cc] = bal;
-                coef_bwd[(static_cast<size_t>(i) * c->co + cc) * c->ci4 + b] = bal;
+                coef_fwd[(static_cast<size_t>(i) * c->ci + b) * c->co8 + cc] = bal;
+                coef_bwd[(static_cast<size_t>(i) * c->co + cc) * c->ci8 + b] = bal;
             }
     std::vector<uint32_t> fwd, bwd;
     build_tables(c->r, c->k, fwd, bwd);
@@ -512,8 +534,82 @@ KoszulCtx* KoszulCtx::create(const bw_koszul_desc& d, int dev) {
     BW_CUDA(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int), st));
     BW_CUDA(cudaMemsetAsync(c->d_seq_index, 0, sizeof(unsigned long long), st));
     if (c->form == BW_FORM_INT8) c->i8_setup();
+    if (c->form == BW_FORM_PLAIN) c->plain_setup();
     BW_CUDA(cudaStreamSynchronize(st));
     return c.release();
+}
+
+namespace {
+// Plain tile heights chosen per operator shape and device, shared by every
+// context of the process.
+std::mutex g_plain_mutex;
+std::map<std::tuple<int, int, int, int, int, int>, std::pair<int, int>> g_plain_tiles;
+}  // namespace
+
+// The plain gathers hold a 4- or 8-row output tile per thread (8 rows: twice
+// the multiply-adds per gathered row, more registers, and the rows padded to
+// a multiple of 8).  Each direction's height is timed at set-up on the
+// context's own buffers (one warm-up and two launches; the kernels' work does
+// not depend on the values) and the faster kept; BW_PLAIN_TILE=4 or =8 forces
+// one height.
+void KoszulCtx::plain_setup() {
+    int forced = 0;
+    if (const char* e = std::getenv("BW_PLAIN_TILE")) forced = std::atoi(e);
+    if (forced == 4 || forced == 8) {
+        tile_fwd = tile_bwd = forced;
+        plain_plan = "plain: " + std::to_string(forced) + " output rows a thread (forced)";
+        return;
+    }
+    const auto key = std::make_tuple(r, k, ci, co, nb, sms);
+    {
+        std::lock_guard<std::mutex> lock(g_plain_mutex);
+        const auto it = g_plain_tiles.find(key);
+        if (it != g_plain_tiles.end()) {
+            tile_fwd = it->second.first;
+            tile_bwd = it->second.second;
+            plain_plan = "plain: d " + std::to_string(tile_fwd) + ", d^T " + std::to_string(tile_bwd) +
+                         " output rows a thread (tuned earlier in this process)";
+            return;
+        }
+    }
+    cudaStream_t st = own_stream;
+    BW_CUDA(cudaMemsetAsync(d_ya, 0, n_src * nb * sizeof(int32_t), st));
+    BW_CUDA(cudaMemsetAsync(d_z, 0, n_tgt * nb * sizeof(int32_t), st));
+    cudaEvent_t e0, e1;
+    BW_CUDA(cudaEventCreate(&e0));
+    BW_CUDA(cudaEventCreate(&e1));
+    auto time_it = [&](bool fwd, int tile) {
+        (fwd ? tile_fwd : tile_bwd) = tile;
+        auto run = [&] {
+            if (fwd)
+                plain_forward(d_ya, d_z, st);
+            else
+                plain_transpose(d_z, d_yb, true, st);
+        };
+        run();
+        BW_CUDA(cudaEventRecord(e0, st));
+        run();
+        run();
+        BW_CUDA(cudaEventRecord(e1, st));
+        BW_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        BW_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms / 2;
+    };
+    char buf[256];
+    const float f4 = time_it(true, 4), f8 = time_it(true, 8);
+    const float b4 = time_it(false, 4), b8 = time_it(false, 8);
+    BW_CUDA(cudaEventDestroy(e0));
+    BW_CUDA(cudaEventDestroy(e1));
+    tile_fwd = f8 < f4 ? 8 : 4;
+    tile_bwd = b8 < b4 ? 8 : 4;
+    std::snprintf(buf, sizeof buf,
+                  "plain: d %d, d^T %d output rows a thread (tuned: d 4 rows %.4f ms, 8 rows %.4f ms; d^T 4 rows %.4f "
+                  "ms, 8 rows %.4f ms)",
+                  tile_fwd, tile_bwd, f4, f8, b4, b8);
+    plain_plan = buf;
+    std::lock_guard<std::mutex> lock(g_plain_mutex);
+    g_plain_tiles[key] = {tile_fwd, tile_bwd};
 }
 
 template int8_t* KoszulCtx::alloc<int8_t>(uint64_t);
@@ -799,9 +895,7 @@ extern "C" int bw_koszul_plan(const bw_koszul* ctx, char* buf, size_t cap) {
     return guarded([&] {
         BW_ARG(ctx && buf && cap > 0, "bw_koszul_plan: null argument");
         const KoszulCtx& c = *ctx->impl;
-        const std::string text = c.form == BW_FORM_INT8 ? c.i8_plan_text()
-                                                        : std::string("plain: one CTA per 16 output rows, maps in "
-                                                                      "shared memory");
+        const std::string text = c.form == BW_FORM_INT8 ? c.i8_plan_text() : c.plain_plan;
         BW_ARG(text.size() < cap, "bw_koszul_plan: buffer too small");
         std::memcpy(buf, text.c_str(), text.size() + 1);
     });

@@ -13,7 +13,9 @@ namespace bw {
 struct KoszulCtx {
     // shape
     int device = 0, sms = 0;
-    int r = 0, k = 0, ci = 0, co = 0, ci4 = 0, co4 = 0, nb = 0, m = 0;
+    int r = 0, k = 0, ci = 0, co = 0, ci8 = 0, co8 = 0, nb = 0, m = 0;
+    // plain form: output rows per thread of the d and d^T gathers (4 or 8)
+    int tile_fwd = 4, tile_bwd = 4;
     int nbi = 0;   // block width inside the INT8 form (nb, or 16 for nb = 4 / 8: zero columns appended)
     uint32_t p = 0, form = BW_FORM_PLAIN;
     Mod mod{};
@@ -79,6 +81,8 @@ struct KoszulCtx {
     void ensure_host_staging(uint64_t nlen);
 
     // INT8-limb form
+    void plain_setup();            // chooses the plain gathers' tile heights (tile_fwd, tile_bwd)
+    std::string plain_plan;        // the choice and its timings
     void i8_setup();
     void i8_destroy();
     void i8_forward(const int32_t* y, int32_t* z, cudaStream_t st);

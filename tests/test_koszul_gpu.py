@@ -25,17 +25,20 @@ CASES = sorted({k.split("/")[0] for k in GOLDEN.files})
 FORMS = ["plain", "int8"]
 # The INT8 form's two stage producers (the set-up autotuner picks one per
 # shape; BW_I8_PRODUCER restricts the choice): cp.async warps alone, or TMA
-# gathers beside them.
-PRODUCER_FORMS = ["plain", "int8:cpasync", "int8:hybrid"]
+# gathers beside them.  The plain form's two tile heights (4 or 8 output rows
+# a thread; timed at set-up, BW_PLAIN_TILE forces one).
+PRODUCER_FORMS = ["plain:tile4", "plain:tile8", "int8:cpasync", "int8:hybrid"]
 
 
 @pytest.fixture
 def producer_form(request, monkeypatch):
     form, _, producer = request.param.partition(":")
-    if producer:
+    monkeypatch.delenv("BW_I8_PRODUCER", raising=False)
+    monkeypatch.delenv("BW_PLAIN_TILE", raising=False)
+    if form == "int8":
         monkeypatch.setenv("BW_I8_PRODUCER", producer)
     else:
-        monkeypatch.delenv("BW_I8_PRODUCER", raising=False)
+        monkeypatch.setenv("BW_PLAIN_TILE", producer[len("tile"):])
     return form, producer
 
 
@@ -90,8 +93,10 @@ def test_operators_match_oracle(dims, producer_form):
     Z = rng.integers(0, shape.p, (shape.n_tgt, shape.nb), dtype=np.uint32)
     dev = torch.device("cuda", 0)
     with _engine(shape, maps, diag, form) as eng:
-        if producer:
+        if form == "int8":
             assert ("hybrid" in eng.plan) == (producer == "hybrid"), eng.plan
+        else:
+            assert eng.plan.startswith("plain: %s output rows" % producer[len("tile"):]), eng.plan
         y = torch.from_numpy(Y.view(np.int32)).to(dev)
         z = torch.from_numpy(Z.view(np.int32)).to(dev)
         out_z = torch.empty((shape.n_tgt, shape.nb), dtype=torch.int32, device=dev)
