@@ -29,18 +29,20 @@
 // of the traffic through one L2 slice).
 // The epilogue writes all four planes of its output.
 //
-// Warp roles (persistent, one CTA per SM):
-//   warps 0-7   producers: each owns an eighth of the tile's output blocks (or,
+// Warp roles (persistent, one CTA per SM; PW = 8 or 16 producer warps, chosen
+// per direction by the set-up autotuner):
+//   warps 0..PW-1  producers: each owns one of the tile's output blocks (or,
 //               with fewer blocks per tile than producer warps, a share of one
 //               block's rows) and keeps their incidence rows in registers (one
 //               generator per lane); every thread arrives on the stage barrier
 //               through cp.async.mbarrier.arrive.noinc when its copies have
 //               landed;
-//   warp 8      allocates TMEM and issues tcgen05.mma / tcgen05.commit (after a
+//   warp PW     allocates TMEM and issues tcgen05.mma / tcgen05.commit (after a
 //               proxy fence: the stage was written through the generic proxy);
-//   warps 9-16  epilogue, two warps per TMEM lane quadrant: tcgen05.ld the four
-//               partials, recombine, reduce mod p, scale by D (d^T only), split
-//               into limbs, transpose 16 x 16 bytes per half-warp and store one
+//   the rest    epilogue (eight warps with PW = 8, four with PW = 16), one or two
+//               warps per TMEM lane quadrant: tcgen05.ld the four partials,
+//               recombine, reduce mod p, scale by D (d^T only), split into
+//               limbs, transpose 16 x 16 bytes per half-warp and store one
 //               16-byte plane row per lane.
 // Stages are tracked with mbarriers; accumulators are double-buffered in TMEM.
 // Every wait is bounded and polls only a shared-memory give-up flag: on a
@@ -66,11 +68,20 @@ namespace bw {
 namespace {
 
 constexpr uint32_t kAbsent = 0xFFFFFFFFu;
-constexpr int kProducerWarps = 8;
-constexpr int kMmaWarp = kProducerWarps;
-constexpr int kEpilogueWarp0 = kProducerWarps + 1;
-constexpr int kEpilogueWarps = 8;                 // per TMEM lane quadrant: kEpilogueWarps / 4
-constexpr int kI8Threads = (kProducerWarps + 1 + kEpilogueWarps) * 32;
+constexpr int kEpilogueWarps = 8;                 // hybrid kernel; per TMEM lane quadrant: kEpilogueWarps / 4
+
+// Warp roles of the cp.async gather kernel with PW producer warps: PW = 8
+// (eight epilogue warps, 17 in all) or PW = 16 (four epilogue warps, 21 in
+// all; more copy streams for the same register budget of 96 a thread).
+template <int PW>
+struct GatherWarps {
+    static_assert(PW == 8 || PW == 16, "8 or 16 producer warps");
+    static constexpr int producers = PW;
+    static constexpr int mma = PW;                        // allocates TMEM, issues the MMAs
+    static constexpr int epilogue0 = PW + 1;
+    static constexpr int epilogue = PW == 16 ? 4 : 8;     // per TMEM lane quadrant: epilogue / 4
+    static constexpr int threads = (PW + 1 + epilogue) * 32;
+};
 constexpr int kMaxSmem = 227 * 1024;
 constexpr int kMaxRowTable = 2048;    // bytes of the K'-row -> generator table
 
@@ -184,8 +195,11 @@ __host__ __device__ __forceinline__ long long plane_offset(long long blk, int u,
     return blk * (static_cast<long long>(NB) * dim) + static_cast<long long>(j >> 4) * dim * 16 + u * 16 + (j & 15);
 }
 
-template <int NB>
-__global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) {
+template <int NB, int PW>
+__global__ void __launch_bounds__(GatherWarps<PW>::threads, 1) i8_gather_gemm_kernel(I8Dir P) {
+    using W = GatherWarps<PW>;
+    constexpr int kProducerWarps = W::producers, kMmaWarp = W::mma, kEpilogueWarp0 = W::epilogue0;
+    constexpr int kGatherEpilogueWarps = W::epilogue;
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int BT = 128 / NB;        // output blocks per tile
     constexpr int HG = NB / 16;         // 16-byte column groups per block row
@@ -215,7 +229,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         }
         for (int b = 0; b < 2; ++b) {
             tc::mbar_init(&accfull[b], 1);
-            tc::mbar_init(&accempty[b], kEpilogueWarps * 32);
+            tc::mbar_init(&accempty[b], kGatherEpilogueWarps * 32);
         }
         tc::mbar_init(drained, 1);
         tc::fence_mbar_init();
@@ -377,7 +391,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) i8_gather_gemm_kernel(I8Dir P) 
         // Warps 9..16: warp & 3 is the TMEM lane quadrant it may read; the two
         // warps of a quadrant split the 16-column output chunks between them.
         const int q = warp & 3;
-        constexpr int EPQ = kEpilogueWarps / 4;                 // epilogue warps per quadrant
+        constexpr int EPQ = kGatherEpilogueWarps / 4;          // epilogue warps per quadrant
         const int half_id = (warp - kEpilogueWarp0) >> 2;      // this warp's part of the chunks
         const int m = q * 32 + lane;               // tile row = (block t, column j)
         const int t = m / NB, j = m % NB;
@@ -1157,6 +1171,7 @@ struct KoszulCtx::I8State {
         uint32_t* inc = nullptr;
         int4* rows4 = nullptr;     // TMA gather rows per group of four generators
         bool gather4 = false;      // hybrid producer (TMA gathers beside cp.async warps), else cp.async only
+        int pw = 8;                // cp.async producer warps (8 or 16)
         size_t smem = 0;
         unsigned grid = 0;
     } fwd, bwd;
@@ -1185,6 +1200,7 @@ struct TuneKey {
 };
 struct TuneChoice {
     bool gather4 = false;   // the hybrid producer
+    int pw = 8;             // cp.async producer warps
     int gps = 0;            // generators per stage
     int t_tma = 0;          // hybrid: blocks of a tile gathered by TMA
     double ms = 0;
@@ -1442,8 +1458,10 @@ void launch_i8(KoszulCtx& c, KoszulCtx::I8State::Dir& D, const CUtensorMap* maps
                "internal: INT8 gather tables missing for the chosen producer");
     if (D.gather4)
         i8_gather_hybrid_kernel<NB><<<D.grid, kHyThreads, D.smem, st>>>(maps[0], maps[1], D.p);
+    else if (D.pw == 16)
+        i8_gather_gemm_kernel<NB, 16><<<D.grid, GatherWarps<16>::threads, D.smem, st>>>(D.p);
     else
-        i8_gather_gemm_kernel<NB><<<D.grid, kI8Threads, D.smem, st>>>(D.p);
+        i8_gather_gemm_kernel<NB, 8><<<D.grid, GatherWarps<8>::threads, D.smem, st>>>(D.p);
     BW_CHECK_LAUNCH();
     ++c.launches;
 }
@@ -1544,7 +1562,8 @@ void KoszulCtx::i8_setup() {
     S.proj.wait_limit = wait_limit;
     int cap_g = 0, cap_4 = 0;
     dispatch_i8_nb(nbi, [&](auto NBc) {
-        cap_g = allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value>, device);
+        cap_g = std::min(allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value, 8>, device),
+                         allow_dynamic_smem(i8_gather_gemm_kernel<decltype(NBc)::value, 16>, device));
         cap_4 = allow_dynamic_smem(i8_gather_hybrid_kernel<decltype(NBc)::value>, device);
         const int cap_p = allow_dynamic_smem(i8_project_tc_kernel<decltype(NBc)::value>, device);
         BW_REQUIRE(static_cast<int>(S.proj_smem) <= cap_p, "INT8 form: shared-memory plan above the device limit");
@@ -1570,16 +1589,23 @@ void KoszulCtx::i8_setup() {
         allow_cp = std::string(e) != "hybrid";
     }
     if (const char* e = std::getenv("BW_I8_TUNE")) tune = std::string(e) != "0";
+    // BW_I8_PRODUCER_WARPS=8 or =16 restricts the cp.async producer's warp count
+    std::vector<int> pws{8, 16};
+    if (const char* e = std::getenv("BW_I8_PRODUCER_WARPS")) {
+        const int v = std::atoi(e);
+        if (v == 8 || v == 16) pws = {v};
+    }
     std::string text;
     for (int dir = 0; dir < 2; ++dir) {
         I8State::Dir& D = dir == 0 ? S.fwd : S.bwd;
         const int inner = dir == 0 ? ci : co, outer = dir == 0 ? co : ci;
         const int in_buf = dir == 0 ? I8_YA : I8_Z, out_buf = dir == 0 ? I8_Z : I8_YB;
-        auto plan = [&](bool g4, int gps, int t_tma) {
+        auto plan = [&](bool g4, int gps, int t_tma, int pw) {
             if (D.b_tiles) release(D.b_tiles);
             D.b_tiles = nullptr;
             if (!plan_direction(*this, D, inner, outer, dir == 1, g4, gps)) return false;
             if (static_cast<int>(D.smem) > (g4 ? cap_4 : cap_g)) return false;
+            D.pw = g4 ? 8 : pw;
             D.p.t_tma = g4 ? t_tma : 0;
             D.p.err = S.err;
             D.p.wait_limit = wait_limit;
@@ -1588,7 +1614,8 @@ void KoszulCtx::i8_setup() {
             D.p.rows4 = D.rows4;
             return true;
         };
-        const TuneKey key{r, k, inner, outer, nbi, dir, sms, (allow_g4 ? 1 : 0) | (allow_cp ? 2 : 0)};
+        const TuneKey key{r, k, inner, outer, nbi, dir, sms,
+                          (allow_g4 ? 1 : 0) | (allow_cp ? 2 : 0) | (pws.size() == 1 ? pws[0] * 4 : 0)};
         TuneChoice choice{};
         bool have = tune && tune_lookup(key, choice);
         std::string tried;
@@ -1598,33 +1625,37 @@ void KoszulCtx::i8_setup() {
             // quarter, half or three quarters of a tile's blocks gathered by TMA
             struct Cand {
                 bool g4;
-                int gps, t_tma;
+                int gps, t_tma, pw;
             };
             std::vector<Cand> cands;
             if (allow_cp) {
                 // the fill heuristic's stage, and fewer or more generators a stage
-                // (smaller stages leave room for more pipeline slots)
-                cands.push_back({false, 0, 0});
-                for (int g : {4, 6, 8, 12})
-                    if (g < r) cands.push_back({false, g, 0});
+                // (smaller stages leave room for more pipeline slots), each with 8
+                // and with 16 producer warps
+                for (int pw : pws) {
+                    cands.push_back({false, 0, 0, pw});
+                    for (int g : {4, 6, 8, 12})
+                        if (g < r) cands.push_back({false, g, 0, pw});
+                }
             }
             if (allow_g4)
                 for (int gs = 1; gs <= std::min(3, (r + 3) / 4); ++gs)
-                    for (int qt = 1; qt <= 3; ++qt) cands.push_back({true, 4 * gs, qt * bt / 4});
+                    for (int qt = 1; qt <= 3; ++qt) cands.push_back({true, 4 * gs, qt * bt / 4, 8});
             double best = 1e30;
             for (const Cand& cand : cands) {
-                if (!plan(cand.g4, cand.gps, cand.t_tma)) continue;
+                if (!plan(cand.g4, cand.gps, cand.t_tma, cand.pw)) continue;
                 const double ms = i8_time_direction(dir == 0, in_buf, out_buf);
                 char buf[96];
                 if (cand.g4)
                     std::snprintf(buf, sizeof buf, "%shybrid stage=%d tma=%d/%d: %.4f ms", tried.empty() ? "" : ", ",
                                   D.p.gi, cand.t_tma, bt, ms);
                 else
-                    std::snprintf(buf, sizeof buf, "%scp.async stage=%d: %.4f ms", tried.empty() ? "" : ", ", D.p.gi, ms);
+                    std::snprintf(buf, sizeof buf, "%scp.async stage=%d warps=%d: %.4f ms", tried.empty() ? "" : ", ",
+                                  D.p.gi, cand.pw, ms);
                 tried += buf;
                 if (ms < best) {
                     best = ms;
-                    choice = TuneChoice{cand.g4, D.p.gi, cand.t_tma, ms};
+                    choice = TuneChoice{cand.g4, cand.pw, D.p.gi, cand.t_tma, ms};
                 }
             }
             BW_REQUIRE(best < 1e30, "INT8 form: no stage plan fits in shared memory");
@@ -1632,16 +1663,16 @@ void KoszulCtx::i8_setup() {
             have = true;
         }
         bool ok = false;
-        if (have) ok = plan(choice.gather4, choice.gps, choice.t_tma);
-        if (!ok) ok = (allow_cp && plan(false, 0, 0)) || (allow_g4 && plan(true, 0, bt / 2));
+        if (have) ok = plan(choice.gather4, choice.gps, choice.t_tma, choice.pw);
+        if (!ok) ok = (allow_cp && plan(false, 0, 0, pws[0])) || (allow_g4 && plan(true, 0, bt / 2, 8));
         BW_REQUIRE(ok, "INT8 form: maps too large for shared memory");
         char buf[192];
         if (D.gather4)
             std::snprintf(buf, sizeof buf, "%s: hybrid (TMA gathers for %d of %d blocks) stage=%d generators, %d slots, "
                           "%zu B shared", dir == 0 ? "d" : "d^T", D.p.t_tma, bt, D.p.gi, D.p.slots, D.smem);
         else
-            std::snprintf(buf, sizeof buf, "%s: cp.async stage=%d generators, %d slots, %zu B shared",
-                          dir == 0 ? "d" : "d^T", D.p.gi, D.p.slots, D.smem);
+            std::snprintf(buf, sizeof buf, "%s: cp.async stage=%d generators, %d producer warps, %d slots, %zu B shared",
+                          dir == 0 ? "d" : "d^T", D.p.gi, D.pw, D.p.slots, D.smem);
         text += (text.empty() ? "" : "; ") + std::string(buf);
         if (!tried.empty()) text += " (tuned: " + tried + ")";
     }

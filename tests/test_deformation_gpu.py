@@ -143,20 +143,25 @@ def test_deformation_eliminated_operator_matches_cyclic(tmp_path):
     assert texts[0] == texts[1]
 
 
+@pytest.mark.parametrize("op", ["augmented", "replacement"])
 @pytest.mark.parametrize("sector", [0, 1])
-def test_augmented_recovery_matches_reference(sector, tmp_path):
+def test_deformation_recovery_matches_reference(op, sector, tmp_path):
+    """The recovery program on each deformation variant: the same null-vector
+    files and report as the reference's cuprym_deformation_kernel_vectors, from
+    the same sequence files and the same generator."""
     _need_reference("cuprym_deformation_kernel_vectors")
     p = 661
     inst = GOLDEN / "g12_p661.json"
-    *_, dense_path, _, _ = _inputs(tmp_path, inst, sector, "augmented", 303 + sector)
+    *_, dense_path, _, drop_path = _inputs(tmp_path, inst, sector, op, 303 + sector)
+    drop_args = ["--drop-columns", drop_path] if drop_path else []
     seq_dir = tmp_path / "seq"
-    res = _run([BIN / "cuprym_deformation", inst, "--operator", "augmented", "--sector", sector, "--out", seq_dir,
-                *RECIPE, "--dense-file", dense_path])
+    res = _run([BIN / "cuprym_deformation", inst, "--operator", op, "--sector", sector, "--out", seq_dir,
+                *RECIPE, "--dense-file", dense_path, *drop_args])
     assert res.returncode == 0, res.stderr
-    with CyclicEngine(inst, sector, op="augmented", dense_file=dense_path) as eng:
+    with CyclicEngine(inst, sector, op=op, dense_file=dense_path, drop_columns=drop_path) as eng:
         S = square_matrix(eng, p)
     gen = kernel_generator(S, p)
-    stem = f"augmented-sector{sector:02d}-v4-rowmix-r2-s10001"
+    stem = f"{op}-sector{sector:02d}-v4-rowmix-r2-s10001"
     outs = {}
     for name, exe in (("ours", BIN / "cuprym_deformation_kernel_vectors"),
                       (("ref", REF / "cuprym_deformation_kernel_vectors"))):
@@ -166,8 +171,8 @@ def test_augmented_recovery_matches_reference(sector, tmp_path):
             shutil.copy(seq_dir / (stem + suffix), d / (stem + suffix))
         write_generator(d / (stem + "_generators.txt"), gen, p)
         wdm = d / (stem + ".wdm.zst")
-        res = _run([exe, inst, "-f", wdm, "--operator", "augmented", "--sector", sector, "-d", 0,
-                    "--dense-file", dense_path])
+        res = _run([exe, inst, "-f", wdm, "--operator", op, "--sector", sector, "-d", 0,
+                    "--dense-file", dense_path, *drop_args])
         outs[name] = (res.returncode, res.stderr, wdm)
     (rc_o, err_o, w_o), (rc_r, err_r, w_r) = outs["ours"], outs["ref"]
     assert rc_o == rc_r, (err_o, err_r)

@@ -23,20 +23,25 @@ pytestmark = pytest.mark.gpu
 GOLDEN = np.load(Path(__file__).parent / "golden" / "koszul_golden.npz")
 CASES = sorted({k.split("/")[0] for k in GOLDEN.files})
 FORMS = ["plain", "int8"]
-# The INT8 form's two stage producers (the set-up autotuner picks one per
-# shape; BW_I8_PRODUCER restricts the choice): cp.async warps alone, or TMA
-# gathers beside them.  The plain form's two tile heights (4 or 8 output rows
-# a thread; timed at set-up, BW_PLAIN_TILE forces one).
-PRODUCER_FORMS = ["plain:tile4", "plain:tile8", "int8:cpasync", "int8:hybrid"]
+# The INT8 form's stage producers (the set-up autotuner picks one per shape;
+# BW_I8_PRODUCER restricts the choice): cp.async warps alone (8 or 16 of them,
+# BW_I8_PRODUCER_WARPS), or TMA gathers beside them.  The plain form's two
+# tile heights (4 or 8 output rows a thread; timed at set-up, BW_PLAIN_TILE
+# forces one).
+PRODUCER_FORMS = ["plain:tile4", "plain:tile8", "int8:cpasync8", "int8:cpasync16", "int8:hybrid"]
 
 
 @pytest.fixture
 def producer_form(request, monkeypatch):
     form, _, producer = request.param.partition(":")
-    monkeypatch.delenv("BW_I8_PRODUCER", raising=False)
-    monkeypatch.delenv("BW_PLAIN_TILE", raising=False)
+    for var in ("BW_I8_PRODUCER", "BW_I8_PRODUCER_WARPS", "BW_PLAIN_TILE"):
+        monkeypatch.delenv(var, raising=False)
     if form == "int8":
-        monkeypatch.setenv("BW_I8_PRODUCER", producer)
+        if producer.startswith("cpasync"):
+            monkeypatch.setenv("BW_I8_PRODUCER", "cpasync")
+            monkeypatch.setenv("BW_I8_PRODUCER_WARPS", producer[len("cpasync"):])
+        else:
+            monkeypatch.setenv("BW_I8_PRODUCER", producer)
     else:
         monkeypatch.setenv("BW_PLAIN_TILE", producer[len("tile"):])
     return form, producer
@@ -95,6 +100,8 @@ def test_operators_match_oracle(dims, producer_form):
     with _engine(shape, maps, diag, form) as eng:
         if form == "int8":
             assert ("hybrid" in eng.plan) == (producer == "hybrid"), eng.plan
+            if producer.startswith("cpasync"):
+                assert "%s producer warps" % producer[len("cpasync"):] in eng.plan, eng.plan
         else:
             assert eng.plan.startswith("plain: %s output rows" % producer[len("tile"):]), eng.plan
         y = torch.from_numpy(Y.view(np.int32)).to(dev)

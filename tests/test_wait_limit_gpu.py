@@ -29,12 +29,16 @@ def _forward(eng, Y, shape, dev):
     return z.cpu().numpy().view(np.uint32)
 
 
-@pytest.mark.parametrize("producer", ["cpasync", "hybrid"])
+@pytest.mark.parametrize("producer", ["cpasync8", "cpasync16", "hybrid"])
 def test_wait_that_runs_out_returns_status_2_and_context_stays_usable(producer, monkeypatch):
-    """Both stage producers: the cp.async warps alone, and TMA gathers beside them."""
+    """Every stage producer: the cp.async warps alone (8 or 16 of them), and
+    TMA gathers beside them."""
     shape = oracle.KoszulShape(*SHAPE)
     maps, diag, X, Y = oracle.seeded_problem(shape, 41)
     dev = torch.device("cuda", 0)
+    if producer.startswith("cpasync"):
+        monkeypatch.setenv("BW_I8_PRODUCER_WARPS", producer[len("cpasync"):])
+        producer = "cpasync"
     monkeypatch.setenv("BW_I8_PRODUCER", producer)
     monkeypatch.setenv("BW_TEST_WAIT_LIMIT", "100000")
     monkeypatch.setenv("BW_TEST_HOLD_FIRST_STAGE", "1")
@@ -46,6 +50,7 @@ def test_wait_that_runs_out_returns_status_2_and_context_stays_usable(producer, 
         assert "gave up waiting (ERR_WAIT_" in str(err.value)
     monkeypatch.delenv("BW_TEST_WAIT_LIMIT")
     monkeypatch.delenv("BW_TEST_HOLD_FIRST_STAGE")
+    monkeypatch.delenv("BW_I8_PRODUCER_WARPS", raising=False)
     # the CUDA context is intact: a fresh engine on the same device is exact
     with KoszulEngine(*SHAPE, maps=maps, diag=diag, form="int8") as eng:
         np.testing.assert_array_equal(_forward(eng, Y, shape, dev), oracle.forward(shape, maps, Y))
