@@ -388,8 +388,9 @@ __global__ void __launch_bounds__(GatherWarps<PW>::threads, 1) i8_gather_gemm_ke
         __syncwarp();
     } else {
         // ------------------------------------------------------------ epilogue
-        // Warps 9..16: warp & 3 is the TMEM lane quadrant it may read; the two
-        // warps of a quadrant split the 16-column output chunks between them.
+        // Warps PW+1 on: warp & 3 is the TMEM lane quadrant a warp may read; the
+        // warps of a quadrant (two with PW = 8, one with PW = 16) split the
+        // 16-column output chunks between them.
         const int q = warp & 3;
         constexpr int EPQ = kGatherEpilogueWarps / 4;          // epilogue warps per quadrant
         const int half_id = (warp - kEpilogueWarp0) >> 2;      // this warp's part of the chunks
