@@ -352,16 +352,6 @@ void KoszulCtx::project(const int32_t* w, cudaStream_t st) {
     dispatch_nb(nb, [&](auto NBc) { launch_project<decltype(NBc)::value>(*this, w, st); });
 }
 
-void KoszulCtx::forward(const int32_t* y, int32_t* z, cudaStream_t st) {
-    if (form == BW_FORM_INT8) i8_forward(y, z, st);
-    else plain_forward(y, z, st);
-}
-
-void KoszulCtx::transpose(const int32_t* z, int32_t* w, bool scale, cudaStream_t st) {
-    if (form == BW_FORM_INT8) i8_transpose(z, w, scale, st);
-    else plain_transpose(z, w, scale, st);
-}
-
 // One step: cur -> other, append a_i.
 void KoszulCtx::step_once(cudaStream_t st) {
     if (form == BW_FORM_INT8) {
@@ -370,8 +360,8 @@ void KoszulCtx::step_once(cudaStream_t st) {
     }
     int32_t* src = cur_is_a ? d_ya : d_yb;
     int32_t* dst = cur_is_a ? d_yb : d_ya;
-    forward(src, d_z, st);
-    transpose(d_z, dst, true, st);
+    plain_forward(src, d_z, st);
+    plain_transpose(d_z, dst, true, st);
     project(dst, st);
     cur_is_a = !cur_is_a;
 }
@@ -786,7 +776,7 @@ extern "C" int bw_koszul_forward(bw_koszul* ctx, const uint32_t* d_y, uint32_t* 
             return;
         }
         c.launch_to_balanced(d_y, c.d_ya, c.n_src * c.nb, st);
-        c.forward(c.d_ya, c.d_z, st);
+        c.plain_forward(c.d_ya, c.d_z, st);
         c.launch_to_canonical(c.d_z, d_z, c.n_tgt * c.nb, st);
     });
 }
@@ -809,7 +799,7 @@ extern "C" int bw_koszul_transpose(bw_koszul* ctx, const uint32_t* d_z, uint32_t
             return;
         }
         c.launch_to_balanced(d_z, c.d_z, c.n_tgt * c.nb, st);
-        c.transpose(c.d_z, c.d_ya, scale_by_diag != 0, st);
+        c.plain_transpose(c.d_z, c.d_ya, scale_by_diag != 0, st);
         c.launch_to_canonical(c.d_ya, d_w, c.n_src * c.nb, st);
     });
 }
@@ -832,8 +822,8 @@ extern "C" int bw_koszul_apply(bw_koszul* ctx, const uint32_t* d_y, uint32_t* d_
             return;
         }
         c.launch_to_balanced(d_y, c.d_ya, c.n_src * c.nb, st);
-        c.forward(c.d_ya, c.d_z, st);
-        c.transpose(c.d_z, c.d_yb, true, st);
+        c.plain_forward(c.d_ya, c.d_z, st);
+        c.plain_transpose(c.d_z, c.d_yb, true, st);
         c.launch_to_canonical(c.d_yb, d_out, c.n_src * c.nb, st);
     });
 }
@@ -925,9 +915,9 @@ extern "C" int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* m
             } else {
                 int32_t* src = c.cur_is_a ? c.d_ya : c.d_yb;
                 int32_t* dst = c.cur_is_a ? c.d_yb : c.d_ya;
-                c.forward(src, c.d_z, st);
+                c.plain_forward(src, c.d_z, st);
                 BW_CUDA(cudaEventRecord(ev[4 * s + 1], st));
-                c.transpose(c.d_z, dst, true, st);
+                c.plain_transpose(c.d_z, dst, true, st);
                 BW_CUDA(cudaEventRecord(ev[4 * s + 2], st));
                 c.project(dst, st);
             }

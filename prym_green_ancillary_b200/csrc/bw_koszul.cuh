@@ -68,8 +68,6 @@ struct KoszulCtx {
 
     void plain_forward(const int32_t* y, int32_t* z, cudaStream_t st);
     void plain_transpose(const int32_t* z, int32_t* w, bool scale, cudaStream_t st);
-    void forward(const int32_t* y, int32_t* z, cudaStream_t st);
-    void transpose(const int32_t* z, int32_t* w, bool scale, cudaStream_t st);
     void project(const int32_t* w, cudaStream_t st);
     void step_once(cudaStream_t st);
 
@@ -85,8 +83,6 @@ struct KoszulCtx {
     std::string plain_plan;        // the choice and its timings
     void i8_setup();
     void i8_destroy();
-    void i8_forward(const int32_t* y, int32_t* z, cudaStream_t st);
-    void i8_transpose(const int32_t* z, int32_t* w, bool scale, cudaStream_t st);
     uint64_t i8_kernels_per_step() const;
     enum { I8_YA = 0, I8_YB = 1, I8_Z = 2 };   // limb-plane block arrays
     void i8_run(bool forward_dir, int in_buf, int out_buf, bool scale, cudaStream_t st);

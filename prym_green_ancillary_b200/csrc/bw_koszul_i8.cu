@@ -1806,11 +1806,4 @@ void KoszulCtx::i8_step_once(cudaStream_t st) {
     cur_is_a = !cur_is_a;
 }
 
-void KoszulCtx::i8_forward(const int32_t*, int32_t*, cudaStream_t) {
-    throw Error("internal: the INT8 form runs on limb planes", 3);
-}
-void KoszulCtx::i8_transpose(const int32_t*, int32_t*, bool, cudaStream_t) {
-    throw Error("internal: the INT8 form runs on limb planes", 3);
-}
-
 }  // namespace bw
