@@ -102,8 +102,14 @@ def algorithmic(sh):
 def measured_peaks():
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
-        d = json.loads(path.read_text())
-        return float(d["hbm_gbs"]), "measured"
+        try:
+            v = json.loads(path.read_text())["hbm_gbs"]
+            if isinstance(v, dict):   # a record of several figures: its value
+                v = v.get("value", v.get("gbs"))
+            if v is not None and float(v) > 0:
+                return float(v), "measured"
+        except (ValueError, KeyError, TypeError):
+            pass   # unreadable: the fallback below, named in peak_source
     return 6650.0, "fallback"
 
 
