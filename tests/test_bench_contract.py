@@ -44,3 +44,27 @@ def test_reference_arm_line_follows_the_contract(workload):
 def test_reference_arm_prints_nothing_on_other_ranks():
     env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
     assert _run(["--impl", "reference", "--steps", "3", "--warmup", "3"], env=env).strip() == ""
+
+
+def test_algorithmic_work_per_step():
+    """The roofline numerators: bytes 2 (N_src + N_tgt) n 4 per step (each side's
+    block read and written once), and the multiply-adds of d, D d^T and the
+    projection, at the two synthetic sizes the bench reports."""
+    c2 = bench.algorithmic(bench.shape_of("config2"))
+    assert c2["step_bytes"] == 2 * (1847560 + 2116296) * 16 * 4            # 0.507 GB
+    assert abs(c2["step_bytes"] / 1e9 - 0.507) < 0.001
+    assert c2["macs"] == 2 * 75582 * 11 * 28 * 20 * 16 + 1847560 * 16 * 16
+    c5 = bench.algorithmic(bench.shape_of("config5"))
+    assert c5["step_bytes"] == 2 * (43266496 + 45762640) * 32 * 4          # 22.79 GB
+    assert abs(c5["step_bytes"] / 1e9 - 22.79) < 0.01
+    assert c5["macs"] == 2 * 1144066 * 13 * 40 * 32 * 32 + 43266496 * 32 * 32
+
+
+def test_peak_file_falls_back_when_unreadable(tmp_path, monkeypatch):
+    """A missing or malformed peaks file gives the stated fallback, never an error."""
+    monkeypatch.setattr(bench, "ROOT", tmp_path)
+    assert bench.measured_peaks() == (6650.0, "fallback")
+    (tmp_path / "MEASURED_PEAKS.json").write_text("{not json")
+    assert bench.measured_peaks() == (6650.0, "fallback")
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6457.4, "bf16_tflops": 1590}))
+    assert bench.measured_peaks() == (6457.4, "measured")
