@@ -74,8 +74,8 @@ typedef struct bw_koszul bw_koszul;
 typedef struct bw_koszul_desc {
     uint32_t r;           /* generators (exterior rank), 2..31 */
     uint32_t k;           /* source exterior degree, 1..r */
-    uint32_t dim_in;      /* dim R_q   (columns of each M_i) */
-    uint32_t dim_out;     /* dim R_q+1 (rows of each M_i) */
+    uint32_t dim_in;      /* dim R_q   (columns of each M_i); at most 64 in the INT8 form */
+    uint32_t dim_out;     /* dim R_q+1 (rows of each M_i); at most 64 in the INT8 form */
     uint32_t prime;       /* odd prime < 2^15 */
     uint32_t block_width; /* n: columns of Y (4, 8, 16 or 32) */
     uint32_t proj_width;  /* m: columns of X (4, 8, 16 or 32) */
@@ -141,10 +141,11 @@ BW_API int bw_koszul_seq_step_timed(bw_koszul* ctx, uint64_t steps, float* ms_ou
 BW_API uint64_t bw_koszul_launch_count(const bw_koszul* ctx);
 
 /* The context's kernel plan as text: for the INT8 form, each direction's
- * producer (TMA gathers or cp.async warps), generators per stage, pipeline
- * slots and shared memory, with the set-up autotuner's timing of every
- * candidate when it ran (a shape already tuned in this process reuses the
- * choice), and the projection's stage.  No reference counterpart (the
+ * producer (TMA gathers or 8 or 16 cp.async warps), generators per stage,
+ * pipeline slots and shared memory, with the set-up autotuner's timing of
+ * every candidate when it ran (a shape already tuned in this process reuses
+ * the choice), and the projection's stage; for the plain form, the output
+ * rows a thread of each direction's gathers (4 or 8, timed the same way).  No reference counterpart (the
  * reference has one fixed kernel configuration per block width,
  * cuda/cyclic_cuda_helpers.h:552-631). */
 BW_API int bw_koszul_plan(const bw_koszul* ctx, char* buf, size_t cap);
